@@ -1,0 +1,323 @@
+"""Benchmark of the KAMI block-GEMM hot path on B200.
+
+Workload (default): FP16 block GEMM with FP32 accumulation, M = N = K = 128,
+one problem per CTA, batch = 4 x SM count (592 on a 148-SM B200), the
+reference's in-register repeat method with NUM_ITER = 1000 (every CTA
+multiplies its resident A and B 1000 times; FLOPs = 2*M*N*K*batch*NUM_ITER,
+block_gemm_1d_half_mma.cu:255-258).  Inputs: uniform[-1, 1] rounded to
+FP16, seed 0, synthetic.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One JSON line on rank 0.  `value` is device time of the GEMM launches only
+(inputs resident in HBM; the 256 MiB L2 flush between steps is outside the
+timed events); `e2e` is the same metric through the public C-ABI call with
+the inputs copied from pinned host memory and C copied back inside the timed
+region.  With --gpus N > 1 every rank runs its own replica (weak scaling);
+the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=128)
+    ap.add_argument("--num-iter", type=int, default=1000)
+    ap.add_argument("--variant", default="auto", choices=["auto", "mma_sync", "tcgen05"])
+    ap.add_argument("--partition", default="auto", choices=["auto", "1d", "2d", "3d"])
+    ap.add_argument("--cpu-seconds", type=float, default=10.0, help="bounded CPU-baseline sample length")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("bf16_tflops"), d.get("hbm_gbs"), "measured"
+    return 1590.0, 6650.0, "fallback"
+
+
+def ncu_traffic(kernel_key: str):
+    """DRAM bytes per launch from the committed ncu summary (profiles/*.md,
+    a line `traffic_bytes_per_launch[<key>]: <int>`), else None."""
+    d = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(d):
+        return None
+    tag = f"traffic_bytes_per_launch[{kernel_key}]:"
+    for fn in sorted(os.listdir(d)):
+        if fn.endswith((".md", ".txt")):
+            for ln in open(os.path.join(d, fn)):
+                if ln.strip().startswith(tag):
+                    try:
+                        return int(ln.split(":", 1)[1].strip())
+                    except ValueError:
+                        return None
+    return None
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle (restated reference check loop), bounded sample
+# ---------------------------------------------------------------------------
+def cpu_sample(M, N, K, seconds):
+    import oracle
+    rng = np.random.default_rng(0)
+    A1 = rng.uniform(-1, 1, (1, M, K)).astype(np.float16)
+    B1 = rng.uniform(-1, 1, (1, N, K)).astype(np.float16)
+    t0 = time.perf_counter()
+    oracle.gemm(A1, B1)
+    t1 = time.perf_counter() - t0
+    cores = os.cpu_count() or 1
+    n = int(max(1, min(4096, seconds / max(t1, 1e-6) * cores * 0.7)))
+    A = rng.uniform(-1, 1, (n, M, K)).astype(np.float16)
+    B = rng.uniform(-1, 1, (n, N, K)).astype(np.float16)
+    t0 = time.perf_counter()
+    oracle.gemm(A, B)
+    dt = time.perf_counter() - t0
+    flops = 2.0 * M * N * K * n
+    return {"value": flops / dt / 1e12, "unit": "TFLOP/s", "cores": cores, "kind": "port",
+            "sample": f"{n} problems of {M}x{N}x{K} FP16 inputs, double accumulation (the reference's host "
+                      f"check loop, OpenMP over problems), {dt:.2f} s"}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's CPU path (the oracle restatement of
+    its host check GEMM) on the host cores, same metric and config."""
+    if rank != 0:
+        return
+    M = N = K = args.size
+    batch = 4 * 148
+    for _ in range(args.warmup):
+        cpu_sample(M, N, K, 1.0)
+    vals = []
+    t0 = time.perf_counter()
+    last = None
+    for _ in range(args.steps):
+        last = cpu_sample(M, N, K, max(1.0, args.cpu_seconds / max(args.steps, 1)))
+        vals.append(last["value"])
+    wall = time.perf_counter() - t0
+    v = statistics.median(vals)
+    cfg = {"workload": f"fp16 block GEMM {M}x{N}x{K}, fp32 accumulate, batch {batch}", "M": M, "N": N, "K": K,
+           "batch": batch, "num_iter": args.num_iter}
+    out = {"impl": "reference", "metric": "block-GEMM TFLOPS", "value": v, "unit": "TFLOP/s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall * 1e3 / args.steps,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f16", "data": "synthetic",
+           "config": cfg,
+           "cpu_baseline": {"value": v, "unit": "TFLOP/s", "cores": last["cores"], "kind": "port",
+                            "sample": last["sample"]},
+           "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# our implementation
+# ---------------------------------------------------------------------------
+def run_ours(args, rank, world):
+    import torch
+    import torch.distributed as dist
+    from kami_b200 import api
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    M = N = K = args.size
+    batch = 4 * sms
+    num_iter = args.num_iter
+    g = torch.Generator(device="cpu").manual_seed(0 + rank)
+    A_h = (torch.rand((batch, M, K), generator=g) * 2 - 1).half()
+    B_h = (torch.rand((batch, N, K), generator=g) * 2 - 1).half()
+    A = A_h.to(dev)
+    B = B_h.to(dev)
+    C = torch.empty((batch, M, N), dtype=torch.float32, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    plan = api.describe(M, N, K, batch, torch.float16, variant=args.variant, partition=args.partition)
+
+    def step():
+        api.gemm_batched(A, B, C, variant=args.variant, partition=args.partition, num_iter=num_iter)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    # correctness spot check of one problem against a double reference on the host
+    ref = (A_h[0].double() @ B_h[0].double().T) * num_iter
+    got = C[0].double().cpu()
+    rel = float((got - ref).norm() / ref.norm())
+
+    if world > 1:
+        dist.barrier()
+    sampler = ClockSampler(dev.index) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        times.append((e0, e1))
+    torch.cuda.synchronize()
+    ms = [a.elapsed_time(b) for a, b in times]
+    if world > 1:
+        dist.barrier()
+    # ---- end-to-end through the C ABI with host buffers ----
+    A_pin = A_h.pin_memory()
+    B_pin = B_h.pin_memory()
+    C_pin = torch.empty((batch, M, N), dtype=torch.float32).pin_memory()
+    A_e = torch.empty_like(A)
+    B_e = torch.empty_like(B)
+    e2e_ms = []
+    for i in range(args.warmup + args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        A_e.copy_(A_pin, non_blocking=True)
+        B_e.copy_(B_pin, non_blocking=True)
+        api.gemm_batched(A_e, B_e, C, variant=args.variant, partition=args.partition, num_iter=num_iter)
+        C_pin.copy_(C, non_blocking=True)
+        e1.record(stream)
+        e1.synchronize()
+        if i >= args.warmup:
+            e2e_ms.append(e0.elapsed_time(e1))
+    clocks = sampler.stop() if sampler else None
+
+    step_ms = sum(ms) / len(ms)
+    e2e_step = sum(e2e_ms) / len(e2e_ms)
+    if world > 1:
+        t = torch.tensor([step_ms, e2e_step], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        step_ms, e2e_step = float(t[0]), float(t[1])
+    flops_rank = 2.0 * M * N * K * batch * num_iter
+    value = flops_rank * world / (step_ms * 1e-3) / 1e12
+    e2e_value = flops_rank * world / (e2e_step * 1e-3) / 1e12
+    if rank != 0:
+        return
+    peak_tf, peak_bw, src = measured_peaks()
+    achieved = flops_rank / (min(ms) * 1e-3) / 1e12
+    roof = {"bound": "tensor", "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s",
+            "frac": achieved / peak_tf, "peak_source": f"{src} bf16 dense (burst)",
+            "traffic": ncu_traffic(f"gemm_{plan['variant']}_{M}"),
+            "algorithmic_bytes_per_launch": batch * (M * K * 2 + N * K * 2 + M * N * 4)}
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        cpu = cpu_sample(M, N, K, args.cpu_seconds)
+    out = {"metric": "block-GEMM TFLOPS", "value": value, "unit": "TFLOP/s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f16",
+           "data": "synthetic (uniform[-1,1] rounded to fp16, seed 0)",
+           "config": {"workload": f"fp16 block GEMM {M}x{N}x{K}, fp32 accumulate, batch {batch} "
+                                  f"(4 x {sms} SMs), NUM_ITER {num_iter} in-register repeats",
+                      "M": M, "N": N, "K": K, "batch": batch, "num_iter": num_iter,
+                      "variant": plan["variant"], "partition": plan["partition"], "P": plan["P"],
+                      "threads": plan["threads"], "l2": "256 MiB buffer written between timed steps",
+                      "parallelism": f"replicas x{world}"},
+           "roofline": roof, "cpu_baseline": cpu,
+           "e2e": {"value": e2e_value, "unit": "TFLOP/s",
+                   "h2d_bytes_per_step": int(A_h.numel() * 2 + B_h.numel() * 2),
+                   "d2h_bytes_per_step": int(C.numel() * 4)},
+           "gpu_launches": args.steps, "clocks": clocks, "check_rel_err": rel}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,144 @@
+/*
+ * kami.h -- C ABI of kami_b200, a B200-native (sm_100a) implementation of the
+ * KAMI block-GEMM / block-SpGEMM path.
+ *
+ * The reference (KAMI) has no library ABI: each benchmark program owns one
+ * __global__ kernel whose shape and partition are compile-time -D macros and
+ * whose launch is <<<batch, NUM_ALLOC_RANK_BLOCK*32, smem>>> on the default
+ * stream.  Every entry point below replaces one of those kernel launches
+ * (cited per function, paths inside the KAMI project) and keeps the
+ * reference's knobs as run-time arguments: precision, M/N/K, partition
+ * (1D/2D/3D), warp-rank count P (NUM_RANK_BLOCK), allocated warps
+ * (NUM_ALLOC_RANK_BLOCK) and in-register repeat count (NUM_ITER).
+ *
+ * Conventions
+ *   - Every function returns int: 0 (KAMI_OK) or a negative kami_status.
+ *     No C++ exception crosses this boundary.
+ *   - All pointers to matrix data are DEVICE pointers.  Index arrays
+ *     (row_ptr/col_idx) are device int32.  The caller allocates every device
+ *     buffer, as in the reference.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default
+ *     stream).  Calls are stream-ordered and do not synchronise the host,
+ *     except where a function says so.
+ *   - Leading dimensions (ld*) are row strides in elements; stride* are
+ *     per-problem strides in elements.
+ *   - Layouts: A is M x K row-major (KAMI_A_ROW_MK) or stored transposed
+ *     (K x M row-major, KAMI_A_COL_MK).  B is the reference's N x K
+ *     row-major operand (KAMI_B_REF_NK: h_B[j*K+k], batched_gemm_2d_double_
+ *     mma.cu:348) or K x N row-major (KAMI_B_ROW_KN).  C is M x N row-major.
+ */
+#ifndef KAMI_B200_H
+#define KAMI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum kami_status {
+    KAMI_OK = 0,
+    KAMI_ERR_INVALID_VALUE = -1, /* bad shape, null pointer, bad enum     */
+    KAMI_ERR_UNSUPPORTED = -2,   /* valid request with no kernel for it    */
+    KAMI_ERR_MISALIGNED = -3,    /* pointer / leading-dimension alignment  */
+    KAMI_ERR_WORKSPACE = -4,     /* workspace missing or too small         */
+    KAMI_ERR_CUDA = -5,          /* a CUDA runtime call failed             */
+    KAMI_ERR_TIMEOUT = -6,       /* a bounded device wait gave up          */
+    KAMI_ERR_INTERNAL = -7
+} kami_status_t;
+
+typedef enum kami_dtype {
+    KAMI_F16 = 0,
+    KAMI_BF16 = 1,
+    KAMI_F64 = 2,
+    KAMI_F32 = 3
+} kami_dtype_t;
+
+typedef enum kami_partition {
+    KAMI_PARTITION_AUTO = 0,
+    KAMI_PARTITION_1D = 1, /* warps split M; B slices broadcast per stage            */
+    KAMI_PARTITION_2D = 2, /* P x P warps; A along rows, B along columns (SUMMA)     */
+    KAMI_PARTITION_3D = 3  /* P x P x P warps; K split in depth, reduced on device   */
+} kami_partition_t;
+
+typedef enum kami_variant {
+    KAMI_VARIANT_AUTO = 0,
+    KAMI_VARIANT_MMA_SYNC = 1, /* warp mma.sync, register-resident operands        */
+    KAMI_VARIANT_TCGEN05 = 2   /* tcgen05.mma, TMA-staged operands, TMEM accumulators */
+} kami_variant_t;
+
+typedef enum kami_a_layout { KAMI_A_ROW_MK = 0, KAMI_A_COL_MK = 1 } kami_a_layout_t;
+typedef enum kami_b_layout { KAMI_B_REF_NK = 0, KAMI_B_ROW_KN = 1 } kami_b_layout_t;
+
+/* ------------------------------------------------------------------------ */
+/* Library                                                                  */
+/* ------------------------------------------------------------------------ */
+
+/* Human-readable text of the last error raised on the calling host thread. */
+const char *kami_last_error_string(void);
+
+/* Library version as MAJOR*10000 + MINOR*100 + PATCH. */
+int kami_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* Batched block GEMM                                                       */
+/* ------------------------------------------------------------------------ */
+
+/*
+ * C[b] = alpha * sum_{iter < num_iter} A[b] * op(B[b]) + beta * C[b],
+ * for b < batch, one problem per CTA (one CTA may also hold several small
+ * problems).  With num_iter > 1 the product is accumulated num_iter times in
+ * the accumulator -- the reference's in-register repeat methodology
+ * (NUM_ITER, block_gemm_1d_half_mma.cu:130), whose host check divides C by
+ * NUM_ITER.
+ *
+ * Replaces the launches of
+ *   block_gemm_{1d,2d,3d}_half_mma   (src/block_gemm/KAMI/{1d,2d,3d}/fp16/*.cu:61/64/61)
+ *   block_gemm_{1d,2d,3d}_double_mma (src/block_gemm/KAMI/{1d,2d,3d}/fp64/*.cu:55/61/62)
+ *   batched_gemm_{1d,2d,3d}_double_mma (src/batched_gemm/KAMI/{1d,2d,3d}/*.cu:59/65/64)
+ * whose signature is (const T *A, const T *B, T *C, T alpha, T beta).  The
+ * reference ignores alpha and beta; here they are applied.  The 3D partition
+ * reduces its P partial C slices on the device instead of writing a P-times
+ * larger C for a host reduction (batched_gemm_3d_double_mma.cu:361-373).
+ *
+ * in_type : KAMI_F16, KAMI_BF16 (FP32 accumulation) or KAMI_F64.
+ * out_type: KAMI_F32, KAMI_F16 or KAMI_BF16 for 16-bit inputs; KAMI_F64
+ *           for KAMI_F64 inputs.
+ * P       : ranks per partition dimension (NUM_RANK_BLOCK); 0 = choose.
+ * alloc_warps: warps launched per CTA (NUM_ALLOC_RANK_BLOCK); 0 = exactly
+ *           the warps the partition uses.  Extra warps exit at once.
+ * workspace / ws_bytes: device scratch; see kami_gemm_workspace_size (the
+ *           current kernels need none; pass NULL, 0).
+ */
+int kami_gemm_batched(kami_dtype_t in_type, kami_dtype_t out_type,
+                      kami_partition_t partition, kami_variant_t variant,
+                      int M, int N, int K, int P, int alloc_warps,
+                      int64_t batch,
+                      const void *A, int64_t lda, int64_t strideA, kami_a_layout_t a_layout,
+                      const void *B, int64_t ldb, int64_t strideB, kami_b_layout_t b_layout,
+                      void *C, int64_t ldc, int64_t strideC,
+                      double alpha, double beta, int num_iter,
+                      void *workspace, size_t ws_bytes, void *stream);
+
+/* Bytes of device workspace kami_gemm_batched needs for this request. */
+int kami_gemm_workspace_size(kami_dtype_t in_type, kami_partition_t partition,
+                             kami_variant_t variant, int M, int N, int K, int P,
+                             int64_t batch, size_t *bytes);
+
+/*
+ * Describe the kernel kami_gemm_batched would launch (after AUTO resolution):
+ * out[0] = variant, out[1] = partition, out[2] = P, out[3] = threads per
+ * CTA, out[4] = dynamic shared memory bytes, out[5] = problems per CTA,
+ * out[6] = CTAs in the grid.  Host-only; launches nothing.
+ */
+int kami_gemm_describe(kami_dtype_t in_type, kami_dtype_t out_type,
+                       kami_partition_t partition, kami_variant_t variant,
+                       int M, int N, int K, int P, int alloc_warps, int64_t batch,
+                       kami_a_layout_t a_layout, kami_b_layout_t b_layout, int out[8]);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KAMI_B200_H */

@@ -1,0 +1,71 @@
+"""Loader of libkami_b200.so (the C ABI declared in include/kami.h).
+
+The library is built in-tree by ``kami_b200.build``.  There is no fallback:
+when the library is missing or cannot be loaded, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libkami_b200.so")
+
+# enums of include/kami.h
+KAMI_OK = 0
+F16, BF16, F64, F32 = 0, 1, 2, 3
+PARTITION_AUTO, PARTITION_1D, PARTITION_2D, PARTITION_3D = 0, 1, 2, 3
+VARIANT_AUTO, VARIANT_MMA_SYNC, VARIANT_TCGEN05 = 0, 1, 2
+A_ROW_MK, A_COL_MK = 0, 1
+B_REF_NK, B_ROW_KN = 0, 1
+
+STATUS_NAMES = {
+    0: "KAMI_OK", -1: "KAMI_ERR_INVALID_VALUE", -2: "KAMI_ERR_UNSUPPORTED", -3: "KAMI_ERR_MISALIGNED",
+    -4: "KAMI_ERR_WORKSPACE", -5: "KAMI_ERR_CUDA", -6: "KAMI_ERR_TIMEOUT", -7: "KAMI_ERR_INTERNAL",
+}
+
+# every exported symbol, with ctypes signatures (kept in step with kami.h)
+_i = ctypes.c_int
+_i64 = ctypes.c_int64
+_sz = ctypes.c_size_t
+_vp = ctypes.c_void_p
+_d = ctypes.c_double
+SIGNATURES = {
+    "kami_last_error_string": ([], ctypes.c_char_p),
+    "kami_version": ([], _i),
+    "kami_gemm_batched": ([_i, _i, _i, _i, _i, _i, _i, _i, _i, _i64,
+                           _vp, _i64, _i64, _i,
+                           _vp, _i64, _i64, _i,
+                           _vp, _i64, _i64,
+                           _d, _d, _i, _vp, _sz, _vp], _i),
+    "kami_gemm_workspace_size": ([_i, _i, _i, _i, _i, _i, _i, _i64, ctypes.POINTER(_sz)], _i),
+    "kami_gemm_describe": ([_i, _i, _i, _i, _i, _i, _i, _i, _i, _i64, _i, _i, ctypes.POINTER(_i)], _i),
+}
+
+
+class KamiError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m kami_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (args, res) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != KAMI_OK:
+        raise KamiError(status, load().kami_last_error_string().decode())

@@ -1,0 +1,94 @@
+"""Python mirror of the C ABI (include/kami.h) over torch CUDA tensors.
+
+torch provides device memory and streams only; every computation runs in
+libkami_b200.so.  Argument meaning follows the reference kernels: A is the
+M x K operand, B is the reference's N x K operand (``b_layout="ref_nk"``,
+``h_B[j*K+k]`` in batched_gemm_2d_double_mma.cu:348) or K x N
+(``b_layout="row_kn"``); ``P`` is NUM_RANK_BLOCK, ``alloc_warps`` is
+NUM_ALLOC_RANK_BLOCK and ``num_iter`` is NUM_ITER.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from . import _lib
+from ._lib import check, load
+
+_DT = {torch.float16: _lib.F16, torch.bfloat16: _lib.BF16, torch.float64: _lib.F64, torch.float32: _lib.F32}
+_PART = {"auto": _lib.PARTITION_AUTO, "1d": _lib.PARTITION_1D, "2d": _lib.PARTITION_2D, "3d": _lib.PARTITION_3D}
+_VAR = {"auto": _lib.VARIANT_AUTO, "mma_sync": _lib.VARIANT_MMA_SYNC, "tcgen05": _lib.VARIANT_TCGEN05}
+_AL = {"row_mk": _lib.A_ROW_MK, "col_mk": _lib.A_COL_MK}
+_BL = {"ref_nk": _lib.B_REF_NK, "row_kn": _lib.B_ROW_KN}
+
+
+def _stream_ptr(stream) -> int:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return int(s.cuda_stream)
+
+
+def _as3(x: torch.Tensor) -> torch.Tensor:
+    return x.unsqueeze(0) if x.dim() == 2 else x
+
+
+def _check_inner(x: torch.Tensor, name: str):
+    if x.stride(-1) != 1:
+        raise ValueError(f"{name} must be contiguous in its last dimension")
+
+
+def gemm_batched(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = None, *,
+                 a_layout: str = "row_mk", b_layout: str = "ref_nk", partition: str = "auto",
+                 variant: str = "auto", P: int = 0, alloc_warps: int = 0, num_iter: int = 1,
+                 alpha: float = 1.0, beta: float = 0.0, out_dtype: torch.dtype | None = None,
+                 stream=None) -> torch.Tensor:
+    """C[b] = alpha * num_iter * A[b] op(B[b]) + beta * C[b] (kami_gemm_batched).
+
+    A: [batch, M, K] (row_mk) or [batch, K, M] (col_mk).
+    B: [batch, N, K] (ref_nk) or [batch, K, N] (row_kn).
+    Returns C [batch, M, N]: float32 for 16-bit inputs unless ``out_dtype``
+    (float16 / bfloat16) is given, float64 for float64 inputs."""
+    squeeze = A.dim() == 2
+    A3, B3 = _as3(A), _as3(B)
+    if A3.dtype != B3.dtype:
+        raise TypeError("A and B must have the same dtype")
+    if not (A3.is_cuda and B3.is_cuda):
+        raise ValueError("A and B must be CUDA tensors")
+    _check_inner(A3, "A")
+    _check_inner(B3, "B")
+    batch = A3.shape[0]
+    if a_layout == "row_mk":
+        M, K = A3.shape[1], A3.shape[2]
+    else:
+        K, M = A3.shape[1], A3.shape[2]
+    N = B3.shape[1] if b_layout == "ref_nk" else B3.shape[2]
+    if C is None:
+        odt = out_dtype or (torch.float64 if A3.dtype == torch.float64 else torch.float32)
+        C3 = torch.empty((batch, M, N), dtype=odt, device=A3.device)
+    else:
+        C3 = _as3(C)
+        _check_inner(C3, "C")
+    st = load().kami_gemm_batched(
+        _DT[A3.dtype], _DT[C3.dtype], _PART[partition], _VAR[variant], M, N, K, P, alloc_warps, batch,
+        A3.data_ptr(), A3.stride(1), A3.stride(0) if batch > 1 else 0, _AL[a_layout],
+        B3.data_ptr(), B3.stride(1), B3.stride(0) if batch > 1 else 0, _BL[b_layout],
+        C3.data_ptr(), C3.stride(1), C3.stride(0) if batch > 1 else 0,
+        float(alpha), float(beta), int(num_iter), None, 0, _stream_ptr(stream))
+    check(st)
+    if C is not None:
+        return C
+    return C3[0] if squeeze else C3
+
+
+def describe(M: int, N: int, K: int, batch: int, dtype=torch.float16, out_dtype=None, *, partition="auto",
+             variant="auto", P=0, alloc_warps=0, a_layout="row_mk", b_layout="ref_nk") -> dict:
+    """The kernel kami_gemm_batched would launch for this request."""
+    out = (ctypes.c_int * 8)()
+    odt = out_dtype or (torch.float64 if dtype == torch.float64 else torch.float32)
+    check(load().kami_gemm_describe(_DT[dtype], _DT[odt], _PART[partition], _VAR[variant], M, N, K, P,
+                                    alloc_warps, batch, _AL[a_layout], _BL[b_layout], out))
+    keys = ["variant", "partition", "P", "threads", "smem", "problems_per_cta", "grid"]
+    d = dict(zip(keys, list(out)[:7]))
+    d["variant"] = {1: "mma_sync", 2: "tcgen05"}[d["variant"]]
+    d["partition"] = {1: "1d", 2: "2d", 3: "3d"}[d["partition"]]
+    return d

@@ -1,0 +1,24 @@
+// tc05_gemm.cuh -- host interface of the tcgen05 (5th-generation tensor core)
+// block GEMM variant: operands staged in shared memory by TMA, accumulators
+// in tensor memory (TMEM).  Implemented in tc05_gemm.cu.
+#pragma once
+#include "kami_common.cuh"
+
+namespace kami {
+
+int fail(int code, const char *fmt, ...);
+int cuda_fail(cudaError_t e, const char *what);
+
+// True when AUTO should try the tcgen05 variant first for this request.
+bool tc05_prefer(int in_type, int partition, int M, int N, int K, int a_layout, int b_layout);
+
+// Resolve (without launching) the tcgen05 launch for a request.
+int tc05_plan(int in_type, int out_type, int partition, int P, int M, int N, int K, int64_t batch, int a_layout,
+              int b_layout, LaunchInfo *info);
+
+// Launch; returns KAMI_ERR_UNSUPPORTED (and launches nothing) when the
+// request is outside what the variant handles.
+int tc05_launch(const GemmArgs &g, int in_type, int partition, int P, void *workspace, size_t ws_bytes,
+                cudaStream_t stream);
+
+} // namespace kami

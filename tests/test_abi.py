@@ -1,0 +1,81 @@
+"""The C ABI library: it loads, exports every function include/kami.h
+declares, and validates arguments on the host (no GPU needed; nothing here
+launches a kernel)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from kami_b200 import _lib
+from kami_b200._lib import KamiError
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = set()
+    for fn in os.listdir(os.path.join(ROOT, "include")):
+        if fn.endswith(".h"):
+            txt = open(os.path.join(ROOT, "include", fn)).read()
+            txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+            names |= set(re.findall(r"\b(kami_[a-z0-9_]+)\s*\(", txt))
+    return sorted(names)
+
+
+def test_library_loads():
+    L = _lib.load()
+    assert L.kami_version() >= 100
+
+
+def test_every_declared_symbol_is_exported():
+    L = _lib.load()
+    names = declared_functions()
+    assert "kami_gemm_batched" in names
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    # and the Python signature table covers them all
+    assert set(names) <= set(_lib.SIGNATURES), set(names) - set(_lib.SIGNATURES)
+
+
+def _call(**kw):
+    a = dict(in_type=_lib.F16, out_type=_lib.F32, part=0, var=0, M=64, N=64, K=64, P=0, alloc=0, batch=1,
+             A=16, lda=64, sA=4096, al=0, B=16, ldb=64, sB=4096, bl=0, C=16, ldc=64, sC=4096,
+             alpha=1.0, beta=0.0, it=1)
+    a.update(kw)
+    return _lib.load().kami_gemm_batched(a["in_type"], a["out_type"], a["part"], a["var"], a["M"], a["N"], a["K"],
+                                         a["P"], a["alloc"], a["batch"], a["A"], a["lda"], a["sA"], a["al"],
+                                         a["B"], a["ldb"], a["sB"], a["bl"], a["C"], a["ldc"], a["sC"],
+                                         a["alpha"], a["beta"], a["it"], None, 0, None)
+
+
+@pytest.mark.parametrize("kw,status", [
+    (dict(batch=0), 0),
+    (dict(M=0), -1),
+    (dict(in_type=7), -1),
+    (dict(in_type=_lib.F64, out_type=_lib.F32), -2),
+    (dict(K=30, lda=30, ldb=30), -2),
+    (dict(A=None), -1),
+    (dict(A=18), -3),
+    (dict(lda=63), -1),
+    (dict(it=0), -1),
+    (dict(al=5), -1),
+])
+def test_host_validation(kw, status):
+    assert _call(**kw) == status
+    if status:
+        assert _lib.load().kami_last_error_string()
+
+
+def test_describe_is_host_only():
+    from kami_b200 import api
+    import torch
+    d = api.describe(128, 128, 128, 592, torch.float16, variant="mma_sync", partition="2d")
+    assert d["variant"] == "mma_sync" and d["partition"] == "2d" and d["P"] == 4
+    assert d["threads"] == 512 and d["grid"] == 592
+    d = api.describe(32, 32, 32, 1024, torch.float64, partition="2d", P=2)
+    assert d["threads"] == 128 and d["problems_per_cta"] == 1
+    d = api.describe(16, 16, 16, 1000, torch.float16, partition="1d", variant="mma_sync")
+    assert d["problems_per_cta"] == 4 and d["grid"] == 250
+    with pytest.raises(KamiError):
+        api.describe(200, 200, 200, 1, torch.float16, variant="mma_sync")
