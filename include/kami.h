@@ -81,6 +81,13 @@ const char *kami_last_error_string(void);
 /* Library version as MAJOR*10000 + MINOR*100 + PATCH. */
 int kami_version(void);
 
+/* Read and clear the device-side status word that kernels with bounded
+ * waits set when a wait gives up instead of hanging (no counterpart in the
+ * reference, whose kernels have no waits).  *code receives 0 when no wait
+ * timed out; the return value is KAMI_ERR_TIMEOUT when one did.  Synchronises
+ * with the device. */
+int kami_device_status(int *code);
+
 /* ------------------------------------------------------------------------ */
 /* Batched block GEMM                                                       */
 /* ------------------------------------------------------------------------ */

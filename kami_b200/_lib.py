@@ -33,6 +33,7 @@ _d = ctypes.c_double
 SIGNATURES = {
     "kami_last_error_string": ([], ctypes.c_char_p),
     "kami_version": ([], _i),
+    "kami_device_status": ([ctypes.POINTER(_i)], _i),
     "kami_gemm_batched": ([_i, _i, _i, _i, _i, _i, _i, _i, _i, _i64,
                            _vp, _i64, _i64, _i,
                            _vp, _i64, _i64, _i,

@@ -223,6 +223,18 @@ const char *kami_last_error_string(void) { return g_err; }
 
 int kami_version(void) { return 100; }
 
+int kami_device_status(int *code)
+{
+    if (!code)
+        return fail(KAMI_ERR_INVALID_VALUE, "code is NULL");
+    int st = tc05_read_error(code);
+    if (st)
+        return st;
+    if (*code)
+        return fail(KAMI_ERR_TIMEOUT, "a bounded device wait gave up (code %d)", *code);
+    return KAMI_OK;
+}
+
 int kami_gemm_workspace_size(kami_dtype_t in_type, kami_partition_t partition, kami_variant_t variant, int M, int N,
                              int K, int P, int64_t batch, size_t *bytes)
 {

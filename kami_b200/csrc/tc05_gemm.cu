@@ -1,18 +1,383 @@
-// tc05_gemm.cu -- tcgen05 block GEMM (placeholder until the kernel lands).
+// tc05_gemm.cu -- the tcgen05 variant of the block GEMM (FP16/BF16 inputs,
+// FP32 accumulation in tensor memory).
+//
+// One CTA (4 warps) per problem.  Thread 0 loads the whole problem -- A
+// (M x K) and B (N x K, the reference's operand) -- into shared memory with
+// TMA (128-byte swizzle, 64-element K boxes), then issues every
+// tcgen05.mma of the problem back to back into a TMEM accumulator
+// (M = 64 or 128 rows of TMEM lanes, N columns) and commits to an mbarrier;
+// all four warps read the accumulator back with tcgen05.ld and store C.
+// Several CTAs share an SM (shared memory and TMEM permitting), so one
+// CTA's loads and stores overlap another CTA's MMAs.
+//
+// The reference's partitions map onto how the MMAs are issued:
+//   1D  one M x N MMA per k-step (N <= 256);
+//   2D  N split into P column panels, P MMAs of M x N/P per k-step, each
+//       into its own accumulator columns;
+//   3D  K split into P depth slices, each accumulated in its own TMEM
+//       accumulator, the P partials summed on the device in the epilogue
+//       (the reference sums its 3D slices on the host,
+//       block_gemm_3d_half_mma.cu:291-300).
+// num_iter repeats the MMA chain on the resident operands, the reference's
+// in-register repeat (NUM_ITER, block_gemm_1d_half_mma.cu:130).
+//
+// Every mbarrier wait is bounded; on a timeout the kernel records an error
+// in g_tc05_error, waits (bounded) for its copies in flight, frees TMEM and
+// returns.
+#include <mutex>
+
+#include "kami_common.cuh"
 #include "tc05_gemm.cuh"
+#include "tc05_ptx.cuh"
 
 namespace kami {
 
-bool tc05_prefer(int, int, int, int, int, int, int) { return false; }
+__device__ int g_tc05_error = 0;
 
-int tc05_plan(int, int, int, int, int, int, int, int64_t, int, int, LaunchInfo *)
+struct Tc05Params
 {
-    return fail(KAMI_ERR_UNSUPPORTED, "tcgen05 variant not built");
+    GemmArgs g;
+    int bm;             // MMA M (64 or 128)
+    int bn;             // padded N (B box rows)
+    int nkb;            // 64-element K boxes
+    int ksteps;         // 16-element MMA k-steps
+    int part, P;
+    uint32_t idesc;     // instruction descriptor (N = bn, or bn / P for 2D)
+    uint32_t tmem_cols; // allocated TMEM columns (power of two >= 32)
+    uint64_t timeout_ns;
+};
+
+__device__ __forceinline__ void tc05_flag(int code) { atomicExch(&g_tc05_error, code); }
+
+template <bool BF16>
+__global__ void __launch_bounds__(128) tc05_block_kernel(const __grid_constant__ CUtensorMap tmA,
+                                                         const __grid_constant__ CUtensorMap tmB,
+                                                         const Tc05Params p)
+{
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    // 1024-byte alignment of the swizzle atoms
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int a_box = p.bm * 128, b_box = p.bn * 128;
+    uint8_t *sA = smem;
+    uint8_t *sB = sA + p.nkb * a_box;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sB + p.nkb * b_box); // [0] loads landed, [1] MMAs done
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2);
+    int *ok_slot = reinterpret_cast<int *>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int prob = blockIdx.x;
+    const GemmArgs &g = p.g;
+
+    if (threadIdx.x == 0)
+    {
+        tc::mbar_init(&bars[0], 1);
+        tc::mbar_init(&bars[1], 1);
+        tc::fence_mbar_init();
+        *ok_slot = 1;
+    }
+    __syncwarp();
+    if (warp == 0)
+    {
+        tc::tmem_alloc(tmem_slot, p.tmem_cols);
+        tc::tmem_relinquish();
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (threadIdx.x == 0)
+    {
+        const uint32_t bytes = (uint32_t)(p.nkb * (a_box + b_box));
+        tc::mbar_expect_tx(&bars[0], bytes);
+        for (int kb = 0; kb < p.nkb; ++kb)
+        {
+            tc::tma_load_3d(sA + kb * a_box, &tmA, &bars[0], kb * 64, 0, prob);
+            tc::tma_load_3d(sB + kb * b_box, &tmB, &bars[0], kb * 64, 0, prob);
+        }
+        if (!tc::mbar_wait_bounded(&bars[0], 0, p.timeout_ns))
+        {
+            tc05_flag(1);
+            *ok_slot = 0;
+            tc::mbar_wait_bounded(&bars[0], 0, p.timeout_ns); // copies still in flight
+            tc::mbar_arrive(&bars[1]);
+        }
+        else
+        {
+            tc::tc_fence_after();
+            const uint32_t a0 = tc::smem_u32(sA), b0 = tc::smem_u32(sB);
+            const int depth = p.part == 3 ? p.P : 1;
+            const int panels = p.part == 2 ? p.P : 1;
+            const int pn = p.bn / panels;
+            for (int it = 0; it < g.num_iter; ++it)
+            {
+                for (int d = 0; d < depth; ++d)
+                {
+                    const int k_lo = p.ksteps * d / depth, k_hi = p.ksteps * (d + 1) / depth;
+                    const uint32_t acc_col = (uint32_t)(d * p.bn);
+                    for (int ks = k_lo; ks < k_hi; ++ks)
+                    {
+                        const int kb = ks >> 2, kin = ks & 3;
+                        const uint64_t adesc = tc::desc_kmajor_sw128(a0 + kb * a_box + kin * 32);
+                        const uint32_t acc = (it > 0 || ks > k_lo) ? 1u : 0u;
+                        for (int q = 0; q < panels; ++q)
+                        {
+                            const uint64_t bdesc = tc::desc_kmajor_sw128(b0 + kb * b_box + q * pn * 128 + kin * 32);
+                            tc::mma_f16_ss(tmem + acc_col + q * pn, adesc, bdesc, p.idesc, acc);
+                        }
+                    }
+                }
+            }
+            tc::mma_commit(&bars[1]);
+        }
+    }
+    __syncwarp();
+
+    // ---- epilogue: TMEM -> registers -> C ----
+    const bool done = tc::mbar_wait_bounded(&bars[1], 0, p.timeout_ns);
+    __syncwarp(); // tcgen05.ld is .sync.aligned: the warp must be converged
+    tc::tc_fence_after();
+    if (!done)
+        tc05_flag(2);
+    const bool ok = done && *reinterpret_cast<volatile int *>(ok_slot);
+    if (ok)
+    {
+        const int row = p.bm == 128 ? warp * 32 + lane : warp * 16 + lane;
+        const bool row_ok = (p.bm == 128 || lane < 16) && row < g.M;
+        const uint32_t lane_addr = (uint32_t)(warp * 32) << 16;
+        const int depth = p.part == 3 ? p.P : 1;
+        const int osz = g.out_type == KAMI_F32 ? 4 : 2;
+        void *Cb = reinterpret_cast<char *>(g.C) + (int64_t)prob * g.sC * osz;
+        const bool fast = g.out_type == KAMI_F32 && g.alpha == 1.0 && g.beta == 0.0 && g.c_vec &&
+                          (g.ldc % 4 == 0) && (g.sC % 4 == 0) && ((reinterpret_cast<uintptr_t>(g.C) & 15) == 0);
+        for (int c0 = 0; c0 < p.bn; c0 += 16)
+        {
+            uint32_t v[16];
+            tc::tmem_ld16(tmem + lane_addr + c0, v);
+            tc::tmem_ld_wait();
+            float f[16];
+#pragma unroll
+            for (int e = 0; e < 16; ++e)
+                f[e] = __uint_as_float(v[e]);
+            for (int d = 1; d < depth; ++d)
+            {
+                uint32_t w[16];
+                tc::tmem_ld16(tmem + lane_addr + d * p.bn + c0, w);
+                tc::tmem_ld_wait();
+#pragma unroll
+                for (int e = 0; e < 16; ++e)
+                    f[e] += __uint_as_float(w[e]);
+            }
+            if (row_ok)
+            {
+                if (fast && c0 + 16 <= g.N)
+                {
+                    float4 *dst = reinterpret_cast<float4 *>(reinterpret_cast<float *>(Cb) + (int64_t)row * g.ldc + c0);
+#pragma unroll
+                    for (int e = 0; e < 4; ++e)
+                        dst[e] = make_float4(f[4 * e], f[4 * e + 1], f[4 * e + 2], f[4 * e + 3]);
+                }
+                else
+                {
+#pragma unroll
+                    for (int e = 0; e < 16; e += 2)
+                        store_pair<float>(g, Cb, row, c0 + e, f[e], f[e + 1]);
+                }
+            }
+        }
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == 0)
+    {
+        __syncwarp();
+        tc::tc_fence_after();
+        tc::tmem_dealloc(tmem, p.tmem_cols);
+    }
 }
 
-int tc05_launch(const GemmArgs &, int, int, int, void *, size_t, cudaStream_t)
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn()
 {
-    return fail(KAMI_ERR_UNSUPPORTED, "tcgen05 variant not built");
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(f);
+    });
+    return fn;
+}
+
+// 3D map {K, rows, batch} over a K-major operand, box {64, box_rows, 1},
+// 128-byte swizzle, zero fill out of bounds.
+static int make_map(CUtensorMap *map, bool bf16, const void *base, int K, int rows, int64_t batch, int64_t ld,
+                    int64_t stride, int box_rows)
+{
+    EncodeTiledFn fn = encode_fn();
+    if (!fn)
+        return fail(KAMI_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
+    cuuint64_t dims[3] = {(cuuint64_t)K, (cuuint64_t)rows, (cuuint64_t)batch};
+    const int64_t s2 = batch > 1 ? stride : (int64_t)rows * ld;
+    cuuint64_t strides[2] = {(cuuint64_t)(ld * 2), (cuuint64_t)(s2 * 2)};
+    cuuint32_t box[3] = {64, (cuuint32_t)box_rows, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = fn(map, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3,
+                    const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        return fail(KAMI_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled failed (%d) for K=%d rows=%d ld=%lld", (int)r, K,
+                    rows, (long long)ld);
+    return KAMI_OK;
+}
+
+struct Tc05Shape
+{
+    int bm, bn, nkb, ksteps, part, P;
+    uint32_t tmem_cols;
+    size_t smem;
+};
+
+static size_t smem_bytes(int bm, int bn, int nkb) { return (size_t)nkb * (bm + bn) * 128 + 1024 + 64; }
+
+static int tc05_shape(int in_type, int out_type, int partition, int P, int M, int N, int K, int a_layout,
+                      int b_layout, Tc05Shape *s)
+{
+    if (in_type != KAMI_F16 && in_type != KAMI_BF16)
+        return fail(KAMI_ERR_UNSUPPORTED, "tcgen05 variant: FP16/BF16 inputs only");
+    if (out_type != KAMI_F32 && out_type != KAMI_F16 && out_type != KAMI_BF16)
+        return fail(KAMI_ERR_UNSUPPORTED, "tcgen05 variant: FP32/FP16/BF16 output only");
+    if (a_layout != KAMI_A_ROW_MK || b_layout != KAMI_B_REF_NK)
+        return fail(KAMI_ERR_UNSUPPORTED, "tcgen05 variant: K-major A (row_mk) and B (ref_nk) only");
+    if (M > 128 || N > 256 || K > 256)
+        return fail(KAMI_ERR_UNSUPPORTED, "tcgen05 variant: M <= 128, N <= 256, K <= 256 (got %d, %d, %d)", M, N, K);
+    if (K % 8)
+        return fail(KAMI_ERR_UNSUPPORTED, "tcgen05 variant: K must be a multiple of 8");
+    const int part = partition == KAMI_PARTITION_AUTO ? KAMI_PARTITION_1D : partition;
+    const int bm = M <= 64 ? 64 : 128;
+    const int ngran = 16; // MMA N granule; also keeps every 16-column TMEM read inside the allocation
+    int p = part == KAMI_PARTITION_1D ? 1 : (P > 0 ? P : 2);
+    if (part != KAMI_PARTITION_1D && p != 2 && p != 4)
+        return fail(KAMI_ERR_UNSUPPORTED, "tcgen05 variant: P must be 2 or 4 for 2D/3D");
+    int bn = (N + ngran - 1) / ngran * ngran;
+    if (part == KAMI_PARTITION_2D)
+        bn = (N + ngran * p - 1) / (ngran * p) * (ngran * p);
+    if (bn > 256)
+        return fail(KAMI_ERR_UNSUPPORTED, "tcgen05 variant: padded N %d exceeds 256", bn);
+    const int ksteps = (K + 15) / 16;
+    if (part == KAMI_PARTITION_3D && ksteps < p)
+        return fail(KAMI_ERR_UNSUPPORTED, "tcgen05 variant: 3D needs at least P k-steps of 16");
+    const int cols = (part == KAMI_PARTITION_3D ? p : 1) * bn;
+    if (cols > 512)
+        return fail(KAMI_ERR_UNSUPPORTED, "tcgen05 variant: %d accumulator columns exceed TMEM", cols);
+    uint32_t tc = 32;
+    while ((int)tc < cols)
+        tc <<= 1;
+    const int nkb = (K + 63) / 64;
+    s->bm = bm;
+    s->bn = bn;
+    s->nkb = nkb;
+    s->ksteps = ksteps;
+    s->part = part;
+    s->P = p;
+    s->tmem_cols = tc;
+    s->smem = smem_bytes(bm, bn, nkb);
+    if (s->smem > 227 * 1024)
+        return fail(KAMI_ERR_UNSUPPORTED, "tcgen05 variant: %zu bytes of shared memory", s->smem);
+    return KAMI_OK;
+}
+
+bool tc05_prefer(int in_type, int partition, int M, int N, int K, int a_layout, int b_layout)
+{
+    // the tensor-memory path wins where one MMA tile holds the problem
+    // densely; tiny problems stay on mma.sync (see the variant sweep)
+    return (in_type == KAMI_F16 || in_type == KAMI_BF16) && a_layout == KAMI_A_ROW_MK &&
+           b_layout == KAMI_B_REF_NK && M > 32 && M <= 128 && N <= 256 && N >= 32 && K <= 256 && K % 8 == 0;
+}
+
+int tc05_plan(int in_type, int out_type, int partition, int P, int M, int N, int K, int64_t batch, int a_layout,
+              int b_layout, LaunchInfo *info)
+{
+    Tc05Shape s;
+    int st = tc05_shape(in_type, out_type, partition, P, M, N, K, a_layout, b_layout, &s);
+    if (st)
+        return st;
+    info->variant = KAMI_VARIANT_TCGEN05;
+    info->partition = s.part;
+    info->P = s.P;
+    info->threads = 128;
+    info->smem = (int)s.smem;
+    info->problems_per_cta = 1;
+    info->grid = batch;
+    return KAMI_OK;
+}
+
+int tc05_launch(const GemmArgs &g, int in_type, int partition, int P, void *, size_t, cudaStream_t stream)
+{
+    Tc05Shape s;
+    int st = tc05_shape(in_type, g.out_type, partition, P, g.M, g.N, g.K, g.a_layout, g.b_layout, &s);
+    if (st)
+        return st;
+    const bool bf16 = in_type == KAMI_BF16;
+    if ((reinterpret_cast<uintptr_t>(g.A) & 15) || (reinterpret_cast<uintptr_t>(g.B) & 15) || g.lda % 8 ||
+        g.ldb % 8 || (g.batch > 1 && (g.sA % 8 || g.sB % 8 || g.sA == 0 || g.sB == 0)))
+        return fail(KAMI_ERR_UNSUPPORTED, "tcgen05 variant: TMA needs 16-byte aligned bases and strides");
+    if (g.batch > 0x7fffffff)
+        return fail(KAMI_ERR_UNSUPPORTED, "tcgen05 variant: batch above 2^31-1");
+    CUtensorMap ma, mb;
+    st = make_map(&ma, bf16, g.A, g.K, g.M, g.batch, g.lda, g.sA, s.bm);
+    if (st)
+        return st;
+    st = make_map(&mb, bf16, g.B, g.K, g.N, g.batch, g.ldb, g.sB, s.bn);
+    if (st)
+        return st;
+    Tc05Params p{};
+    p.g = g;
+    p.bm = s.bm;
+    p.bn = s.bn;
+    p.nkb = s.nkb;
+    p.ksteps = s.ksteps;
+    p.part = s.part;
+    p.P = s.P;
+    p.idesc = tc::idesc_f16(bf16, s.bm, s.part == KAMI_PARTITION_2D ? s.bn / s.P : s.bn);
+    p.tmem_cols = s.tmem_cols;
+    const double mmas = (double)g.num_iter * s.ksteps * (s.part == KAMI_PARTITION_2D ? s.P : 1);
+    p.timeout_ns = (uint64_t)(2e9 + mmas * 2000.0);
+
+    const void *fn = bf16 ? (const void *)&tc05_block_kernel<true> : (const void *)&tc05_block_kernel<false>;
+    static std::once_flag once[2];
+    cudaError_t e = cudaSuccess;
+    std::call_once(once[bf16 ? 1 : 0], [&] {
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    });
+    if (e != cudaSuccess)
+        return cuda_fail(e, "cudaFuncSetAttribute(tc05_block_kernel)");
+    void *args[] = {&ma, &mb, &p};
+    e = cudaLaunchKernel(fn, dim3((unsigned)g.batch), dim3(128), args, s.smem, stream);
+    if (e != cudaSuccess)
+        return cuda_fail(e, "cudaLaunchKernel(tc05_block_kernel)");
+    return KAMI_OK;
+}
+
+int tc05_read_error(int *flag)
+{
+    int zero = 0;
+    cudaError_t e = cudaMemcpyFromSymbol(flag, g_tc05_error, sizeof(int));
+    if (e != cudaSuccess)
+        return cuda_fail(e, "cudaMemcpyFromSymbol(g_tc05_error)");
+    e = cudaMemcpyToSymbol(g_tc05_error, &zero, sizeof(int));
+    if (e != cudaSuccess)
+        return cuda_fail(e, "cudaMemcpyToSymbol(g_tc05_error)");
+    return KAMI_OK;
 }
 
 } // namespace kami

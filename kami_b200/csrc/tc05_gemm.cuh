@@ -21,4 +21,8 @@ int tc05_plan(int in_type, int out_type, int partition, int P, int M, int N, int
 int tc05_launch(const GemmArgs &g, int in_type, int partition, int P, void *workspace, size_t ws_bytes,
                 cudaStream_t stream);
 
+// Read and clear the device-side error flag of the tcgen05 kernels (0 = none,
+// 1 = operand loads timed out, 2 = MMA completion timed out).  Synchronous.
+int tc05_read_error(int *flag);
+
 } // namespace kami

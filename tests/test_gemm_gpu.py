@@ -59,7 +59,7 @@ H16_INST = [(16, 16, 16, 1, "1d"), (16, 16, 16, 1, "2d"), (16, 16, 16, 1, "3d"),
 F64_INST = [(16, 16, 16, 1, "1d"), (16, 16, 16, 1, "2d"), (16, 16, 16, 1, "3d"), (32, 32, 32, 1, "1d"),
             (32, 32, 32, 2, "1d"), (32, 32, 32, 1, "2d"), (32, 32, 32, 2, "2d"), (32, 32, 32, 1, "3d"),
             (32, 32, 32, 2, "3d"), (64, 64, 64, 4, "1d"), (64, 64, 64, 2, "2d"), (64, 64, 64, 4, "2d"),
-            (64, 64, 64, 2, "3d"), (128, 128, 128, 4, "2d")]
+            (64, 64, 64, 2, "3d")]
 
 CASES = [("f16",) + c for c in H16_INST] + [("bf16",) + c for c in H16_INST[::3]] + [("f64",) + c for c in F64_INST]
 

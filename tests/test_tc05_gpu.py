@@ -1,0 +1,112 @@
+"""Parity of the tcgen05 (TMEM / TMA) block GEMM with the CPU oracle,
+through the C ABI, for the three partition mappings, FP16 and BF16, the
+output types, ragged shapes and the in-register repeat count."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from kami_b200 import _lib, api
+from kami_b200._lib import KamiError
+
+pytestmark = pytest.mark.gpu
+
+TDT = {"f16": torch.float16, "bf16": torch.bfloat16}
+
+
+def _inputs(prec, batch, M, N, K, integer, seed=0):
+    rng = np.random.default_rng(seed)
+    if integer:
+        A = rng.integers(-2, 3, (batch, M, K)).astype(np.float64)
+        B = rng.integers(-2, 3, (batch, N, K)).astype(np.float64)
+    else:
+        A = rng.uniform(-1, 1, (batch, M, K))
+        B = rng.uniform(-1, 1, (batch, N, K))
+    tA = torch.tensor(A, dtype=TDT[prec])
+    tB = torch.tensor(B, dtype=TDT[prec])
+    return tA.cuda(), tB.cuda(), tA.double().numpy(), tB.double().numpy()
+
+
+def _status_clean():
+    code = __import__("ctypes").c_int(0)
+    st = _lib.load().kami_device_status(code)
+    assert st == 0 and code.value == 0
+
+
+SHAPES = [(128, 128, 128), (64, 64, 64), (128, 128, 16), (128, 128, 32), (128, 128, 8), (128, 256, 128),
+          (64, 256, 64), (100, 72, 40), (128, 16, 64), (33, 48, 24), (128, 128, 256), (96, 200, 136)]
+
+
+@pytest.mark.parametrize("prec", ["f16", "bf16"])
+@pytest.mark.parametrize("M,N,K", SHAPES)
+def test_tc05_1d_exact(cuda, prec, M, N, K):
+    A, B, A64, B64 = _inputs(prec, 7, M, N, K, integer=True, seed=M + N + K)
+    C = api.gemm_batched(A, B, variant="tcgen05", partition="1d")
+    torch.cuda.synchronize()
+    _status_clean()
+    assert np.array_equal(C.double().cpu().numpy(), oracle.gemm(A64, B64))
+
+
+@pytest.mark.parametrize("part,P", [("2d", 2), ("2d", 4), ("3d", 2), ("3d", 4)])
+@pytest.mark.parametrize("M,N,K", [(128, 128, 128), (64, 64, 64), (128, 256, 64), (100, 72, 80)])
+def test_tc05_partitions_exact(cuda, part, P, M, N, K):
+    if part == "3d" and (K + 15) // 16 < P:
+        pytest.skip("fewer k-steps than depth ranks")
+    A, B, A64, B64 = _inputs("f16", 5, M, N, K, integer=True, seed=P)
+    C = api.gemm_batched(A, B, variant="tcgen05", partition=part, P=P)
+    torch.cuda.synchronize()
+    _status_clean()
+    assert np.array_equal(C.double().cpu().numpy(), oracle.gemm(A64, B64))
+
+
+@pytest.mark.parametrize("prec", ["f16", "bf16"])
+@pytest.mark.parametrize("M,N,K", [(128, 128, 128), (64, 64, 64), (128, 128, 32)])
+def test_tc05_uniform_tolerance(cuda, prec, M, N, K):
+    A, B, A64, B64 = _inputs(prec, 9, M, N, K, integer=False, seed=11)
+    C = api.gemm_batched(A, B, variant="tcgen05").double().cpu().numpy()
+    ref = oracle.gemm(A64, B64)
+    bound = (K + 2) * 2.0 ** -23 * (np.abs(A64) @ np.abs(B64).transpose(0, 2, 1))
+    assert np.all(np.abs(C - ref) <= bound)
+    assert np.linalg.norm(C - ref) / np.linalg.norm(ref) < 2e-6
+
+
+@pytest.mark.parametrize("num_iter", [1, 3, 1000])
+def test_tc05_num_iter(cuda, num_iter):
+    A, B, A64, B64 = _inputs("f16", 4, 128, 128, 128, integer=True, seed=num_iter)
+    C = api.gemm_batched(A, B, variant="tcgen05", num_iter=num_iter)
+    ref = oracle.gemm(A64, B64) * num_iter
+    # integer sums stay below 2^24, so FP32 accumulation is exact
+    assert np.array_equal(C.double().cpu().numpy(), ref)
+
+
+def test_tc05_out_types_alpha_beta(cuda):
+    A, B, A64, B64 = _inputs("f16", 3, 128, 128, 64, integer=True, seed=2)
+    ref = oracle.gemm(A64, B64)
+    for odt in (torch.float16, torch.bfloat16):
+        C = api.gemm_batched(A, B, variant="tcgen05", out_dtype=odt)
+        assert np.array_equal(C.double().cpu().numpy(), torch.tensor(ref).to(odt).double().numpy())
+    C0 = torch.full((3, 128, 128), 1.0, device="cuda")
+    api.gemm_batched(A, B, C0, variant="tcgen05", alpha=2.0, beta=-1.0)
+    assert np.array_equal(C0.double().cpu().numpy(), 2 * ref - 1)
+
+
+def test_tc05_matches_mma_sync_large_batch(cuda):
+    A, B, _, _ = _inputs("bf16", 4096, 64, 64, 64, integer=False, seed=5)
+    C1 = api.gemm_batched(A, B, variant="tcgen05")
+    C2 = api.gemm_batched(A, B, variant="mma_sync")
+    assert torch.allclose(C1, C2, rtol=0, atol=1e-5)
+
+
+def test_tc05_rejects_what_it_cannot_do(cuda):
+    A = torch.zeros((2, 256, 64), dtype=torch.float16, device="cuda")
+    with pytest.raises(KamiError):
+        api.gemm_batched(A, A, variant="tcgen05")
+    A = torch.zeros((2, 64, 64), dtype=torch.float16, device="cuda")
+    with pytest.raises(KamiError):
+        api.gemm_batched(A, A, variant="tcgen05", b_layout="row_kn")
+
+
+def test_auto_picks_tcgen05_for_128(cuda):
+    assert api.describe(128, 128, 128, 592)["variant"] == "tcgen05"
+    A, B, A64, B64 = _inputs("f16", 8, 128, 128, 128, integer=True)
+    assert np.array_equal(api.gemm_batched(A, B).double().cpu().numpy(), oracle.gemm(A64, B64))
