@@ -144,6 +144,74 @@ int kami_gemm_describe(kami_dtype_t in_type, kami_dtype_t out_type,
                        int M, int N, int K, int P, int alloc_warps, int64_t batch,
                        kami_a_layout_t a_layout, kami_b_layout_t b_layout, int out[8]);
 
+/* ------------------------------------------------------------------------ */
+/* FP64-accurate batched GEMM on the FP16/BF16 tensor cores                 */
+/* ------------------------------------------------------------------------ */
+/*
+ * C[b] = alpha * A[b] * op(B[b]) + beta * C[b] in FP64, M, N, K <= 64, computed
+ * by splitting each row of A and each column of op(B) into `nslices` exact
+ * integer digits (power-of-two row/column scaling; 9-bit digits in binary16
+ * or 7-bit digits in bfloat16), multiplying digit pairs on the tensor cores
+ * with exact FP32 accumulation, and recombining in FP64.  FP64 arithmetic is
+ * used only for scaling/splitting and recombination.  nslices: 2..6
+ * (KAMI_F16) or 2..8 (KAMI_BF16).  A is M x K row-major; B is N x K
+ * (KAMI_B_REF_NK) or K x N (KAMI_B_ROW_KN).  No counterpart in the
+ * reference; its FP64 comparator is kami_gemm_batched with in_type KAMI_F64
+ * (batched_gemm_{1d,2d,3d}_double_mma.cu).  num_iter repeats the tensor-core
+ * products on the resident digits (C then holds num_iter times the product).
+ */
+int kami_split_f64_gemm_batched(int nslices, kami_dtype_t slice_type,
+                                int M, int N, int K, int64_t batch,
+                                const double *A, int64_t lda, int64_t strideA,
+                                const double *B, int64_t ldb, int64_t strideB,
+                                kami_b_layout_t b_layout,
+                                double *C, int64_t ldc, int64_t strideC,
+                                double alpha, double beta, int num_iter, void *stream);
+
+/* ------------------------------------------------------------------------ */
+/* Block SpGEMM on BSR matrices (16 x 16 tiles)                             */
+/* ------------------------------------------------------------------------ */
+/*
+ * C = A * B with A (mb x kb blocks), B (kb x nb blocks) and C in BSR form:
+ * row_ptr (int32, rows + 1), col_idx (int32, sorted ascending within each
+ * block-row, as the reference generator emits them), values as nnz tiles of
+ * bsr x bsr elements, each tile row-major (ValA[e*256 + r*16 + c],
+ * block_spgemm_2d_half_mma.cu:242-245; B tiles are used as K x N).
+ * bsr must be 16 (BSR_M = BSR_K = BSR_N = 16).  The three calls follow the
+ * reference's host sequence (block_spgemm_2d_half_mma.cu:805-825):
+ */
+
+/* Symbolic pass: row_ptr_c[0..mb] (device) = exclusive scan of the number
+ * of distinct block columns per block-row of C.  Replaces
+ * spgemm_symbolic_kernel (:58-86) + thrust::exclusive_scan (:806).  When
+ * nnz_c_host is not NULL the total is copied to it and the stream is
+ * synchronised (the reference's D2H copy of nnzC, :808). */
+int kami_spgemm_bsr_symbolic(int bsr, int mb, int kb, int nb,
+                             const int *row_ptr_a, const int *col_idx_a,
+                             const int *row_ptr_b, const int *col_idx_b,
+                             int *row_ptr_c, int *nnz_c_host, void *stream);
+
+/* Column fill: col_idx_c (nnz_c entries, device) in ascending order per
+ * block-row.  Replaces spgemm_symbolic_col_kernel (:88-116). */
+int kami_spgemm_bsr_fill_colidx(int bsr, int mb, int kb, int nb,
+                                const int *row_ptr_a, const int *col_idx_a,
+                                const int *row_ptr_b, const int *col_idx_b,
+                                const int *row_ptr_c, int *col_idx_c, void *stream);
+
+/* Numeric pass: val_c (nnz_c tiles in col_idx_c order) = alpha *
+ * num_iter * (A * B) + beta * val_c, FP16 or BF16 tiles with FP32
+ * accumulation; out_type KAMI_F32, KAMI_F16 or KAMI_BF16.  Replaces
+ * block_spgemm_{1d,2d,3d}_half_mma (e.g. :171-174, argument order kept:
+ * RowPtrA, ColIdxA, ValA, RowPtrB, ColIdxB, ValB, RowPtrC, ColIdxC, ValC,
+ * alpha, beta); num_iter is the reference's NUM_ITER repeat. */
+int kami_spgemm_bsr_numeric(kami_dtype_t in_type, kami_dtype_t out_type, int bsr,
+                            int mb, int kb, int nb,
+                            const int *row_ptr_a, const int *col_idx_a, const void *val_a,
+                            const int *row_ptr_b, const int *col_idx_b, const void *val_b,
+                            const int *row_ptr_c, const int *col_idx_c, void *val_c,
+                            int64_t nnz_c, double alpha, double beta, int num_iter,
+                            void *stream);
+
 #ifdef __cplusplus
 }
 #endif

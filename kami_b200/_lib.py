@@ -41,6 +41,12 @@ SIGNATURES = {
                            _d, _d, _i, _vp, _sz, _vp], _i),
     "kami_gemm_workspace_size": ([_i, _i, _i, _i, _i, _i, _i, _i64, ctypes.POINTER(_sz)], _i),
     "kami_gemm_describe": ([_i, _i, _i, _i, _i, _i, _i, _i, _i, _i64, _i, _i, ctypes.POINTER(_i)], _i),
+    "kami_split_f64_gemm_batched": ([_i, _i, _i, _i, _i, _i64, _vp, _i64, _i64, _vp, _i64, _i64, _i,
+                                     _vp, _i64, _i64, _d, _d, _i, _vp], _i),
+    "kami_spgemm_bsr_symbolic": ([_i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(_i), _vp], _i),
+    "kami_spgemm_bsr_fill_colidx": ([_i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp], _i),
+    "kami_spgemm_bsr_numeric": ([_i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64,
+                                 _d, _d, _i, _vp], _i),
 }
 
 

@@ -92,3 +92,89 @@ def describe(M: int, N: int, K: int, batch: int, dtype=torch.float16, out_dtype=
     d["variant"] = {1: "mma_sync", 2: "tcgen05"}[d["variant"]]
     d["partition"] = {1: "1d", 2: "2d", 3: "3d"}[d["partition"]]
     return d
+
+
+def split_f64_gemm(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = None, *, nslices: int = 6,
+                   slice_dtype=torch.float16, b_layout: str = "ref_nk", alpha: float = 1.0, beta: float = 0.0,
+                   num_iter: int = 1, stream=None) -> torch.Tensor:
+    """FP64 C = A op(B) via exact FP16/BF16 digit slices on the tensor cores
+    (kami_split_f64_gemm_batched).  A: [batch, M, K] float64; B: [batch, N, K]
+    (ref_nk) or [batch, K, N] (row_kn)."""
+    squeeze = A.dim() == 2
+    A3, B3 = _as3(A), _as3(B)
+    if A3.dtype != torch.float64 or B3.dtype != torch.float64:
+        raise TypeError("split_f64_gemm takes float64 operands")
+    _check_inner(A3, "A")
+    _check_inner(B3, "B")
+    batch, M, K = A3.shape
+    N = B3.shape[1] if b_layout == "ref_nk" else B3.shape[2]
+    C3 = torch.empty((batch, M, N), dtype=torch.float64, device=A3.device) if C is None else _as3(C)
+    check(load().kami_split_f64_gemm_batched(
+        int(nslices), _DT[slice_dtype], M, N, K, batch, A3.data_ptr(), A3.stride(1), A3.stride(0),
+        B3.data_ptr(), B3.stride(1), B3.stride(0), _BL[b_layout], C3.data_ptr(), C3.stride(1), C3.stride(0),
+        float(alpha), float(beta), int(num_iter), _stream_ptr(stream)))
+    if C is not None:
+        return C
+    return C3[0] if squeeze else C3
+
+
+# ---------------------------------------------------------------------------
+# block SpGEMM (BSR, 16 x 16 tiles)
+# ---------------------------------------------------------------------------
+class BSR:
+    """A block-sparse matrix on the device: row_ptr (int32, rows+1), col_idx
+    (int32, ascending per block-row) and values [nnz, 16, 16]."""
+
+    def __init__(self, row_ptr: torch.Tensor, col_idx: torch.Tensor, values: torch.Tensor, block_cols: int):
+        self.row_ptr, self.col_idx, self.values = row_ptr, col_idx, values
+        self.block_rows = row_ptr.numel() - 1
+        self.block_cols = block_cols
+
+    @property
+    def nnz_blocks(self) -> int:
+        return self.col_idx.numel()
+
+
+def spgemm_symbolic(A: BSR, B: BSR, stream=None):
+    """RowPtrC and nnzC (host int; synchronises like the reference's D2H)."""
+    if A.block_cols != B.block_rows:
+        raise ValueError("inner block dimensions differ")
+    rpc = torch.empty(A.block_rows + 1, dtype=torch.int32, device=A.row_ptr.device)
+    nnz = ctypes.c_int(0)
+    check(load().kami_spgemm_bsr_symbolic(16, A.block_rows, A.block_cols, B.block_cols, A.row_ptr.data_ptr(),
+                                          _ptr(A.col_idx), B.row_ptr.data_ptr(), _ptr(B.col_idx),
+                                          rpc.data_ptr(), ctypes.byref(nnz), _stream_ptr(stream)))
+    return rpc, nnz.value
+
+
+def spgemm_fill_colidx(A: BSR, B: BSR, row_ptr_c: torch.Tensor, nnz_c: int, stream=None) -> torch.Tensor:
+    cic = torch.empty(max(nnz_c, 1), dtype=torch.int32, device=A.row_ptr.device)
+    check(load().kami_spgemm_bsr_fill_colidx(16, A.block_rows, A.block_cols, B.block_cols, A.row_ptr.data_ptr(),
+                                             _ptr(A.col_idx), B.row_ptr.data_ptr(), _ptr(B.col_idx),
+                                             row_ptr_c.data_ptr(), cic.data_ptr(), _stream_ptr(stream)))
+    return cic[:nnz_c]
+
+
+def spgemm_numeric(A: BSR, B: BSR, row_ptr_c, col_idx_c, out_dtype=torch.float32, C_values=None, *,
+                   alpha=1.0, beta=0.0, num_iter=1, stream=None) -> torch.Tensor:
+    nnz_c = col_idx_c.numel()
+    if C_values is None:
+        C_values = torch.empty((max(nnz_c, 1), 16, 16), dtype=out_dtype, device=A.row_ptr.device)
+    check(load().kami_spgemm_bsr_numeric(_DT[A.values.dtype], _DT[C_values.dtype], 16, A.block_rows, A.block_cols,
+                                         B.block_cols, A.row_ptr.data_ptr(), _ptr(A.col_idx), _ptr(A.values),
+                                         B.row_ptr.data_ptr(), _ptr(B.col_idx), _ptr(B.values),
+                                         row_ptr_c.data_ptr(), _ptr(col_idx_c), _ptr(C_values), nnz_c,
+                                         float(alpha), float(beta), int(num_iter), _stream_ptr(stream)))
+    return C_values[:nnz_c]
+
+
+def spgemm(A: BSR, B: BSR, out_dtype=torch.float32, *, num_iter=1, stream=None) -> BSR:
+    """C = A * B: symbolic, column fill, numeric (the reference's sequence)."""
+    rpc, nnz = spgemm_symbolic(A, B, stream)
+    cic = spgemm_fill_colidx(A, B, rpc, nnz, stream)
+    vals = spgemm_numeric(A, B, rpc, cic, out_dtype, num_iter=num_iter, stream=stream)
+    return BSR(rpc, cic, vals, B.block_cols)
+
+
+def _ptr(t: torch.Tensor) -> int:
+    return t.data_ptr() if t.numel() else 0

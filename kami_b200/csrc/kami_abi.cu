@@ -12,6 +12,8 @@
 
 namespace kami {
 
+int split_read_error(int *flag);
+
 static thread_local char g_err[512] = "no error";
 
 int fail(int code, const char *fmt, ...)
@@ -230,6 +232,11 @@ int kami_device_status(int *code)
     int st = tc05_read_error(code);
     if (st)
         return st;
+    int c2 = 0;
+    if ((st = split_read_error(&c2)))
+        return st;
+    if (!*code)
+        *code = c2;
     if (*code)
         return fail(KAMI_ERR_TIMEOUT, "a bounded device wait gave up (code %d)", *code);
     return KAMI_OK;

@@ -1,0 +1,503 @@
+// spgemm.cu -- block SpGEMM C = A * B on BSR matrices with 16 x 16 tiles.
+//
+// Reference path (src/sparse/spgemm/2d/block_spgemm_2d_half_mma.cu):
+//   spgemm_symbolic_kernel (:58-86)  per block-row a dense flag array over
+//                                    the block columns, then a count;
+//   thrust::exclusive_scan (:806)    RowPtrC;
+//   cudaMemcpy D2H of nnzC (:808)    so the host can allocate ColIdxC/ValC;
+//   spgemm_symbolic_col_kernel (:88-116)  ColIdxC, ascending per row;
+//   block_spgemm_2d_half_mma (:171-555)   numeric: per warp, local CSR
+//                                    slices, staged exchange, and a linear
+//                                    search for each product's C column.
+//
+// This implementation keeps the same three phases, the same outputs (RowPtrC,
+// ColIdxC ascending per row, ValC tiles in ColIdxC order) and the same tile
+// layouts (A and B tiles row-major 16 x 16, B used as K x N), re-designed for
+// B200 and for large matrices (the reference handles one <= 192^2 block per
+// CTA):
+//   * symbolic: one warp per block-row builds the row's column set as a
+//     bitmap in shared memory (shared atomics), counts it with popc, and the
+//     column fill walks the bitmap words in order (ascending by
+//     construction);  the scan is a single-CTA in-place scan; no scratch.
+//   * numeric: one warp per C tile (i, j).  Its lanes take the nonzero
+//     blocks A(i, k) of row i, binary-search j in block-row k of B (column
+//     indices sorted ascending, as the reference generator emits them), and
+//     the warp accumulates every matching A(i,k) * B(k,j) with two
+//     m16n8k16 MMAs (FP32 accumulation) in ascending k -- the order of the
+//     reference's sparse accumulator.  No C tile is touched twice, so the
+//     kernel writes C once (the HBM floor of the product).
+#include <cstdint>
+
+#include "kami_common.cuh"
+
+namespace kami {
+
+int fail(int code, const char *fmt, ...);
+int cuda_fail(cudaError_t e, const char *what);
+
+namespace {
+
+constexpr int kBsr = 16;
+
+// ---------------------------------------------------------------------------
+// symbolic
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void build_row_bitmap(uint32_t *bm, int words, int row, const int *__restrict__ rpa,
+                                                 const int *__restrict__ cia, const int *__restrict__ rpb,
+                                                 const int *__restrict__ cib, int lane)
+{
+    for (int w = lane; w < words; w += 32)
+        bm[w] = 0u;
+    __syncwarp();
+    const int a0 = rpa[row], a1 = rpa[row + 1];
+    for (int e = a0 + lane; e < a1; e += 32)
+    {
+        const int k = cia[e];
+        const int b1 = rpb[k + 1];
+        for (int b = rpb[k]; b < b1; ++b)
+        {
+            const int c = cib[b];
+            atomicOr(&bm[c >> 5], 1u << (c & 31));
+        }
+    }
+    __syncwarp();
+}
+
+__global__ void spgemm_count_kernel(int mb, int nb, const int *__restrict__ rpa, const int *__restrict__ cia,
+                                    const int *__restrict__ rpb, const int *__restrict__ cib, int *__restrict__ rpc)
+{
+    extern __shared__ uint32_t bm_all[];
+    const int words = (nb + 31) >> 5;
+    const int wpc = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31;
+    uint32_t *bm = bm_all + (threadIdx.x >> 5) * words;
+    for (int row = blockIdx.x * wpc + (threadIdx.x >> 5); row < mb; row += gridDim.x * wpc)
+    {
+        build_row_bitmap(bm, words, row, rpa, cia, rpb, cib, lane);
+        int cnt = 0;
+        for (int w = lane; w < words; w += 32)
+            cnt += __popc(bm[w]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+            cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+        if (lane == 0)
+            rpc[row] = cnt;
+        __syncwarp();
+    }
+}
+
+// In-place exclusive scan of rpc[0..n-1] by one CTA of 1024 threads; the
+// total lands in rpc[n].
+__global__ void __launch_bounds__(1024) spgemm_scan_kernel(int n, int *__restrict__ rpc)
+{
+    __shared__ int warp_sums[32];
+    __shared__ int carry_s;
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+    if (t == 0)
+        carry_s = 0;
+    __syncthreads();
+    for (int base = 0; base < n; base += 1024)
+    {
+        const int i = base + t;
+        const int v = i < n ? rpc[i] : 0;
+        int x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o)
+                x += y;
+        }
+        if (lane == 31)
+            warp_sums[wid] = x;
+        __syncthreads();
+        if (wid == 0)
+        {
+            int s = warp_sums[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1)
+            {
+                const int y = __shfl_up_sync(0xffffffffu, s, o);
+                if (lane >= o)
+                    s += y;
+            }
+            warp_sums[lane] = s; // inclusive over warps
+        }
+        __syncthreads();
+        const int carry = carry_s;
+        const int incl = x + (wid > 0 ? warp_sums[wid - 1] : 0);
+        if (i < n)
+            rpc[i] = carry + incl - v;
+        __syncthreads();
+        if (t == 1023)
+            carry_s = carry + incl;
+        __syncthreads();
+    }
+    if (t == 0)
+        rpc[n] = carry_s;
+}
+
+__global__ void spgemm_colfill_kernel(int mb, int nb, const int *__restrict__ rpa, const int *__restrict__ cia,
+                                      const int *__restrict__ rpb, const int *__restrict__ cib,
+                                      const int *__restrict__ rpc, int *__restrict__ cic)
+{
+    extern __shared__ uint32_t bm_all[];
+    const int words = (nb + 31) >> 5;
+    const int wpc = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31;
+    uint32_t *bm = bm_all + (threadIdx.x >> 5) * words;
+    for (int row = blockIdx.x * wpc + (threadIdx.x >> 5); row < mb; row += gridDim.x * wpc)
+    {
+        build_row_bitmap(bm, words, row, rpa, cia, rpb, cib, lane);
+        int out = rpc[row];
+        for (int w0 = 0; w0 < words; w0 += 32)
+        {
+            const int w = w0 + lane;
+            uint32_t bits = w < words ? bm[w] : 0u;
+            const int c = __popc(bits);
+            int pre = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1)
+            {
+                const int y = __shfl_up_sync(0xffffffffu, pre, o);
+                if (lane >= o)
+                    pre += y;
+            }
+            int pos = out + pre - c;
+            while (bits)
+            {
+                const int b = __ffs(bits) - 1;
+                cic[pos++] = w * 32 + b;
+                bits &= bits - 1;
+            }
+            out += __shfl_sync(0xffffffffu, pre, 31);
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// numeric
+// ---------------------------------------------------------------------------
+template <bool BF16>
+__device__ __forceinline__ void mma16816(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                         uint32_t b0, uint32_t b1)
+{
+    if constexpr (BF16)
+        asm("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+            "{%0,%1,%2,%3};"
+            : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+            : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+    else
+        asm("mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+            "{%0,%1,%2,%3};"
+            : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+            : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+struct SpNumArgs
+{
+    int mb, nb;
+    const int *rpa, *cia, *rpb, *cib, *rpc, *cic;
+    const uint16_t *va, *vb;
+    void *vc;
+    int64_t nnzc;
+    int out_type;
+    float alpha, beta;
+    int num_iter;
+};
+
+template <bool BF16>
+__global__ void __launch_bounds__(256) spgemm_numeric_kernel(const SpNumArgs p)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (c >= p.nnzc)
+        return;
+    // block-row of this C tile: last i with rpc[i] <= c
+    int lo = 0, hi = p.mb - 1;
+    while (lo < hi)
+    {
+        const int mid = (lo + hi + 1) >> 1;
+        if (p.rpc[mid] <= c)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const int i = lo;
+    const int j = p.cic[c];
+    const int gq = lane >> 2, tq = lane & 3;
+
+    float acc0[4] = {0.f, 0.f, 0.f, 0.f}; // C columns 0..7
+    float acc1[4] = {0.f, 0.f, 0.f, 0.f}; // C columns 8..15
+    const int a_begin = p.rpa[i], a_end = p.rpa[i + 1];
+    for (int it = 0; it < p.num_iter; ++it)
+    {
+        for (int base = a_begin; base < a_end; base += 32)
+        {
+            // each lane searches one A block of the row for a matching B block
+            const int e = base + lane;
+            int match = -1;
+            if (e < a_end)
+            {
+                const int k = p.cia[e];
+                int l = p.rpb[k], h = p.rpb[k + 1] - 1;
+                while (l <= h)
+                {
+                    const int m = (l + h) >> 1;
+                    const int v = p.cib[m];
+                    if (v == j)
+                    {
+                        match = m;
+                        break;
+                    }
+                    if (v < j)
+                        l = m + 1;
+                    else
+                        h = m - 1;
+                }
+            }
+            uint32_t hits = __ballot_sync(0xffffffffu, match >= 0);
+            while (hits)
+            {
+                const int src = __ffs(hits) - 1;
+                hits &= hits - 1;
+                const int eb = __shfl_sync(0xffffffffu, match, src);
+                const int ea = base + src;
+                const uint16_t *ta = p.va + (int64_t)ea * 256;
+                const uint16_t *tb = p.vb + (int64_t)eb * 256;
+                // A fragment with the k index permuted inside the k-step: lane
+                // (g, t) holds A[g][4t..4t+3] and A[g+8][4t..4t+3]
+                const uint2 ra = __ldg(reinterpret_cast<const uint2 *>(ta + gq * 16 + 4 * tq));
+                const uint2 rb = __ldg(reinterpret_cast<const uint2 *>(ta + (gq + 8) * 16 + 4 * tq));
+                // B fragment (K x N, row-major tile), same k permutation
+                uint32_t b00, b01, b10, b11;
+                {
+                    const uint16_t *col0 = tb + gq;     // n = g      (columns 0..7)
+                    const uint16_t *col1 = tb + gq + 8; // n = g + 8  (columns 8..15)
+                    const int k0 = 4 * tq;
+                    b00 = (uint32_t)__ldg(col0 + (k0 + 0) * 16) | ((uint32_t)__ldg(col0 + (k0 + 1) * 16) << 16);
+                    b01 = (uint32_t)__ldg(col0 + (k0 + 2) * 16) | ((uint32_t)__ldg(col0 + (k0 + 3) * 16) << 16);
+                    b10 = (uint32_t)__ldg(col1 + (k0 + 0) * 16) | ((uint32_t)__ldg(col1 + (k0 + 1) * 16) << 16);
+                    b11 = (uint32_t)__ldg(col1 + (k0 + 2) * 16) | ((uint32_t)__ldg(col1 + (k0 + 3) * 16) << 16);
+                }
+                mma16816<BF16>(acc0, ra.x, rb.x, ra.y, rb.y, b00, b01);
+                mma16816<BF16>(acc1, ra.x, rb.x, ra.y, rb.y, b10, b11);
+            }
+        }
+    }
+
+    // store the tile: lane holds rows g, g+8 and columns 2t, 2t+1 (+8)
+    const int r0 = gq, r1 = gq + 8, c0 = 2 * tq;
+    if (p.out_type == KAMI_F32)
+    {
+        float *out = reinterpret_cast<float *>(p.vc) + c * 256;
+        float2 v00 = make_float2(acc0[0], acc0[1]), v01 = make_float2(acc1[0], acc1[1]);
+        float2 v10 = make_float2(acc0[2], acc0[3]), v11 = make_float2(acc1[2], acc1[3]);
+        if (p.alpha != 1.f || p.beta != 0.f)
+        {
+            const float2 o00 = *reinterpret_cast<float2 *>(out + r0 * 16 + c0);
+            const float2 o01 = *reinterpret_cast<float2 *>(out + r0 * 16 + c0 + 8);
+            const float2 o10 = *reinterpret_cast<float2 *>(out + r1 * 16 + c0);
+            const float2 o11 = *reinterpret_cast<float2 *>(out + r1 * 16 + c0 + 8);
+            const float a = p.alpha, b = p.beta;
+            v00 = make_float2(a * v00.x + (b != 0.f ? b * o00.x : 0.f), a * v00.y + (b != 0.f ? b * o00.y : 0.f));
+            v01 = make_float2(a * v01.x + (b != 0.f ? b * o01.x : 0.f), a * v01.y + (b != 0.f ? b * o01.y : 0.f));
+            v10 = make_float2(a * v10.x + (b != 0.f ? b * o10.x : 0.f), a * v10.y + (b != 0.f ? b * o10.y : 0.f));
+            v11 = make_float2(a * v11.x + (b != 0.f ? b * o11.x : 0.f), a * v11.y + (b != 0.f ? b * o11.y : 0.f));
+        }
+        *reinterpret_cast<float2 *>(out + r0 * 16 + c0) = v00;
+        *reinterpret_cast<float2 *>(out + r0 * 16 + c0 + 8) = v01;
+        *reinterpret_cast<float2 *>(out + r1 * 16 + c0) = v10;
+        *reinterpret_cast<float2 *>(out + r1 * 16 + c0 + 8) = v11;
+    }
+    else
+    {
+        uint16_t *out = reinterpret_cast<uint16_t *>(p.vc) + c * 256;
+        const bool bf = p.out_type == KAMI_BF16;
+        auto cvt = [&](float x, uint16_t old) -> uint16_t {
+            float y = p.alpha * x;
+            if (p.beta != 0.f)
+                y += p.beta * to_float(old, bf);
+            return bf ? __bfloat16_as_ushort(__float2bfloat16_rn(y)) : __half_as_ushort(__float2half_rn(y));
+        };
+        const int offs[4] = {r0 * 16 + c0, r0 * 16 + c0 + 8, r1 * 16 + c0, r1 * 16 + c0 + 8};
+        const float vals[4][2] = {{acc0[0], acc0[1]}, {acc1[0], acc1[1]}, {acc0[2], acc0[3]}, {acc1[2], acc1[3]}};
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+        {
+            uint32_t *dst = reinterpret_cast<uint32_t *>(out + offs[q]);
+            const uint32_t old = p.beta != 0.f ? *dst : 0u;
+            const uint16_t lo16 = cvt(vals[q][0], (uint16_t)(old & 0xffff));
+            const uint16_t hi16 = cvt(vals[q][1], (uint16_t)(old >> 16));
+            *dst = (uint32_t)lo16 | ((uint32_t)hi16 << 16);
+        }
+    }
+}
+
+int bitmap_launch(int nb, int *warps_per_cta, size_t *smem)
+{
+    const int words = (nb + 31) >> 5;
+    int w = 8;
+    while (w > 1 && (size_t)w * words * 4 > 96 * 1024)
+        w >>= 1;
+    if ((size_t)w * words * 4 > 200 * 1024)
+        return fail(KAMI_ERR_UNSUPPORTED, "spgemm: %d block columns exceed the shared-memory bitmap", nb);
+    *warps_per_cta = w;
+    *smem = (size_t)w * words * 4;
+    return KAMI_OK;
+}
+
+int prep_bitmap_fn(const void *fn, size_t smem)
+{
+    if (smem > 48 * 1024)
+    {
+        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess)
+            return cuda_fail(e, "cudaFuncSetAttribute(spgemm bitmap kernel)");
+    }
+    return KAMI_OK;
+}
+
+// Row pointers must be present; column-index arrays may be NULL when the
+// matrix has no nonzero block.
+int check_bsr_args(int bsr, int mb, int kb, int nb, const void *a, const void *, const void *c, const void *)
+{
+    if (bsr != kBsr)
+        return fail(KAMI_ERR_UNSUPPORTED, "spgemm: only 16 x 16 BSR tiles are supported (got %d)", bsr);
+    if (mb < 0 || kb < 0 || nb < 0)
+        return fail(KAMI_ERR_INVALID_VALUE, "spgemm: negative block dimensions");
+    if (mb > 0 && (!a || !c))
+        return fail(KAMI_ERR_INVALID_VALUE, "spgemm: null row pointer");
+    return KAMI_OK;
+}
+
+} // namespace
+} // namespace kami
+
+using namespace kami;
+
+extern "C" {
+
+int kami_spgemm_bsr_symbolic(int bsr, int mb, int kb, int nb, const int *row_ptr_a, const int *col_idx_a,
+                             const int *row_ptr_b, const int *col_idx_b, int *row_ptr_c, int *nnz_c_host,
+                             void *stream)
+{
+    int st = check_bsr_args(bsr, mb, kb, nb, row_ptr_a, col_idx_a, row_ptr_b, col_idx_b);
+    if (st)
+        return st;
+    if (!row_ptr_c)
+        return fail(KAMI_ERR_INVALID_VALUE, "spgemm: row_ptr_c is NULL");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    cudaError_t e;
+    if (mb > 0 && nb > 0)
+    {
+        int wpc;
+        size_t smem;
+        if ((st = bitmap_launch(nb, &wpc, &smem)))
+            return st;
+        if ((st = prep_bitmap_fn((const void *)spgemm_count_kernel, smem)))
+            return st;
+        const int grid = (mb + wpc - 1) / wpc;
+        spgemm_count_kernel<<<grid, wpc * 32, smem, s>>>(mb, nb, row_ptr_a, col_idx_a, row_ptr_b, col_idx_b,
+                                                        row_ptr_c);
+        if ((e = cudaGetLastError()) != cudaSuccess)
+            return cuda_fail(e, "spgemm_count_kernel");
+        spgemm_scan_kernel<<<1, 1024, 0, s>>>(mb, row_ptr_c);
+        if ((e = cudaGetLastError()) != cudaSuccess)
+            return cuda_fail(e, "spgemm_scan_kernel");
+    }
+    else
+    {
+        if ((e = cudaMemsetAsync(row_ptr_c, 0, sizeof(int) * (size_t)(mb + 1), s)) != cudaSuccess)
+            return cuda_fail(e, "cudaMemsetAsync(row_ptr_c)");
+    }
+    if (nnz_c_host)
+    {
+        if ((e = cudaMemcpyAsync(nnz_c_host, row_ptr_c + mb, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+            return cuda_fail(e, "cudaMemcpyAsync(nnzC)");
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess)
+            return cuda_fail(e, "cudaStreamSynchronize");
+    }
+    return KAMI_OK;
+}
+
+int kami_spgemm_bsr_fill_colidx(int bsr, int mb, int kb, int nb, const int *row_ptr_a, const int *col_idx_a,
+                                const int *row_ptr_b, const int *col_idx_b, const int *row_ptr_c, int *col_idx_c,
+                                void *stream)
+{
+    int st = check_bsr_args(bsr, mb, kb, nb, row_ptr_a, col_idx_a, row_ptr_b, col_idx_b);
+    if (st)
+        return st;
+    if (mb == 0 || nb == 0)
+        return KAMI_OK;
+    if (!row_ptr_c || !col_idx_c)
+        return fail(KAMI_ERR_INVALID_VALUE, "spgemm: row_ptr_c / col_idx_c is NULL");
+    int wpc;
+    size_t smem;
+    if ((st = bitmap_launch(nb, &wpc, &smem)))
+        return st;
+    if ((st = prep_bitmap_fn((const void *)spgemm_colfill_kernel, smem)))
+        return st;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    spgemm_colfill_kernel<<<(mb + wpc - 1) / wpc, wpc * 32, smem, s>>>(mb, nb, row_ptr_a, col_idx_a, row_ptr_b,
+                                                                      col_idx_b, row_ptr_c, col_idx_c);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return cuda_fail(e, "spgemm_colfill_kernel");
+    return KAMI_OK;
+}
+
+int kami_spgemm_bsr_numeric(kami_dtype_t in_type, kami_dtype_t out_type, int bsr, int mb, int kb, int nb,
+                            const int *row_ptr_a, const int *col_idx_a, const void *val_a, const int *row_ptr_b,
+                            const int *col_idx_b, const void *val_b, const int *row_ptr_c, const int *col_idx_c,
+                            void *val_c, int64_t nnz_c, double alpha, double beta, int num_iter, void *stream)
+{
+    int st = check_bsr_args(bsr, mb, kb, nb, row_ptr_a, col_idx_a, row_ptr_b, col_idx_b);
+    if (st)
+        return st;
+    if (in_type != KAMI_F16 && in_type != KAMI_BF16)
+        return fail(KAMI_ERR_UNSUPPORTED, "spgemm numeric: FP16/BF16 tiles only");
+    if (out_type != KAMI_F32 && out_type != KAMI_F16 && out_type != KAMI_BF16)
+        return fail(KAMI_ERR_UNSUPPORTED, "spgemm numeric: FP32/FP16/BF16 output only");
+    if (num_iter < 1 || nnz_c < 0)
+        return fail(KAMI_ERR_INVALID_VALUE, "spgemm numeric: num_iter >= 1 and nnz_c >= 0 required");
+    if (nnz_c == 0 || mb == 0)
+        return KAMI_OK;
+    if (!row_ptr_c || !col_idx_c || !val_a || !val_b || !val_c)
+        return fail(KAMI_ERR_INVALID_VALUE, "spgemm numeric: null pointer");
+    if ((reinterpret_cast<uintptr_t>(val_a) & 7) || (reinterpret_cast<uintptr_t>(val_b) & 1) ||
+        (reinterpret_cast<uintptr_t>(val_c) & 7))
+        return fail(KAMI_ERR_MISALIGNED, "spgemm numeric: tile arrays must be 8-byte aligned");
+    SpNumArgs p{};
+    p.mb = mb;
+    p.nb = nb;
+    p.rpa = row_ptr_a;
+    p.cia = col_idx_a;
+    p.rpb = row_ptr_b;
+    p.cib = col_idx_b;
+    p.rpc = row_ptr_c;
+    p.cic = col_idx_c;
+    p.va = reinterpret_cast<const uint16_t *>(val_a);
+    p.vb = reinterpret_cast<const uint16_t *>(val_b);
+    p.vc = val_c;
+    p.nnzc = nnz_c;
+    p.out_type = out_type;
+    p.alpha = (float)alpha;
+    p.beta = (float)beta;
+    p.num_iter = num_iter;
+    const int64_t grid = (nnz_c + 7) / 8;
+    if (grid > 0x7fffffff)
+        return fail(KAMI_ERR_UNSUPPORTED, "spgemm numeric: too many C tiles");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (in_type == KAMI_BF16)
+        spgemm_numeric_kernel<true><<<(unsigned)grid, 256, 0, s>>>(p);
+    else
+        spgemm_numeric_kernel<false><<<(unsigned)grid, 256, 0, s>>>(p);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return cuda_fail(e, "spgemm_numeric_kernel");
+    return KAMI_OK;
+}
+
+} // extern "C"

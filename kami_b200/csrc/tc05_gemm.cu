@@ -134,8 +134,8 @@ __global__ void __launch_bounds__(128) tc05_block_kernel(const __grid_constant__
     __syncwarp();
 
     // ---- epilogue: TMEM -> registers -> C ----
-    const bool done = tc::mbar_wait_bounded(&bars[1], 0, p.timeout_ns);
-    __syncwarp(); // tcgen05.ld is .sync.aligned: the warp must be converged
+    // tcgen05.ld is .sync.aligned: the outcome must be warp-uniform
+    const bool done = __all_sync(0xffffffffu, tc::mbar_wait_bounded(&bars[1], 0, p.timeout_ns));
     tc::tc_fence_after();
     if (!done)
         tc05_flag(2);
@@ -351,7 +351,7 @@ int tc05_launch(const GemmArgs &g, int in_type, int partition, int P, void *, si
     p.idesc = tc::idesc_f16(bf16, s.bm, s.part == KAMI_PARTITION_2D ? s.bn / s.P : s.bn);
     p.tmem_cols = s.tmem_cols;
     const double mmas = (double)g.num_iter * s.ksteps * (s.part == KAMI_PARTITION_2D ? s.P : 1);
-    p.timeout_ns = (uint64_t)(2e9 + mmas * 2000.0);
+    p.timeout_ns = (uint64_t)(5e8 + mmas * 2000.0);
 
     const void *fn = bf16 ? (const void *)&tc05_block_kernel<true> : (const void *)&tc05_block_kernel<false>;
     static std::once_flag once[2];
