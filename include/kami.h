@@ -145,6 +145,42 @@ int kami_gemm_describe(kami_dtype_t in_type, kami_dtype_t out_type,
                        kami_a_layout_t a_layout, kami_b_layout_t b_layout, int out[8]);
 
 /* ------------------------------------------------------------------------ */
+/* Uneven (grouped) batched GEMM: one persistent launch                    */
+/* ------------------------------------------------------------------------ */
+/*
+ * `count` independent problems C_i = alpha * A_i * B_i^T + beta * C_i with
+ * their own M_i, N_i, K_i (each 1..128; K a multiple of 8 for 16-bit
+ * inputs, of 2 for FP64).  A_i is M_i x K_i row-major at A + a_offsets[i],
+ * B_i is N_i x K_i row-major (the reference layout) at B + b_offsets[i],
+ * C_i is M_i x N_i row-major at C + c_offsets[i] (offsets in elements).
+ * The reference runs one launch per compile-time shape
+ * (batched_gemm_{1d,2d,3d}_double_mma.cu, one problem per CTA); here one
+ * persistent launch runs every problem, each with the warp partition (1D /
+ * 2D / 3D warp grid) chosen for its shape.
+ *
+ * kami_gemm_grouped_plan_create builds (host, synchronous) the device
+ * descriptors and a longest-first schedule over persistent CTAs; with
+ * flags & KAMI_PLAN_AUTOTUNE it first measures every valid partition per
+ * 16-rounded shape bucket on this device (cached per process) instead of
+ * using the static cost model.  kami_gemm_grouped_run is a single kernel
+ * launch that allocates nothing and synchronises nothing, so it can be
+ * captured in a CUDA graph; the plan must outlive the graph.
+ */
+#define KAMI_PLAN_AUTOTUNE 1
+typedef struct kami_grouped_plan kami_grouped_plan;
+
+int kami_gemm_grouped_plan_create(kami_dtype_t in_type, kami_dtype_t out_type, int count,
+                                  const int *M, const int *N, const int *K,
+                                  const int64_t *a_offsets, const int64_t *b_offsets,
+                                  const int64_t *c_offsets, int flags, kami_grouped_plan **plan);
+int kami_gemm_grouped_run(const kami_grouped_plan *plan, const void *A, const void *B, void *C,
+                          double alpha, double beta, int num_iter, void *stream);
+/* out[0] = problems, out[1] = persistent CTAs, out[2] = shared memory bytes,
+ * out[3] = FLOPs, out[4] = bytes moved, out[5..11] = problems per partition. */
+int kami_gemm_grouped_plan_info(const kami_grouped_plan *plan, int64_t out[12]);
+int kami_gemm_grouped_plan_destroy(kami_grouped_plan *plan);
+
+/* ------------------------------------------------------------------------ */
 /* FP64-accurate batched GEMM on the FP16/BF16 tensor cores                 */
 /* ------------------------------------------------------------------------ */
 /*
@@ -153,7 +189,7 @@ int kami_gemm_describe(kami_dtype_t in_type, kami_dtype_t out_type,
  * integer digits (power-of-two row/column scaling; 9-bit digits in binary16
  * or 7-bit digits in bfloat16), multiplying digit pairs on the tensor cores
  * with exact FP32 accumulation, and recombining in FP64.  FP64 arithmetic is
- * used only for scaling/splitting and recombination.  nslices: 2..6
+ * used only for scaling/splitting and recombination.  nslices: 2..7
  * (KAMI_F16) or 2..8 (KAMI_BF16).  A is M x K row-major; B is N x K
  * (KAMI_B_REF_NK) or K x N (KAMI_B_ROW_KN).  No counterpart in the
  * reference; its FP64 comparator is kami_gemm_batched with in_type KAMI_F64

@@ -33,8 +33,18 @@ def _as3(x: torch.Tensor) -> torch.Tensor:
 
 
 def _check_inner(x: torch.Tensor, name: str):
-    if x.stride(-1) != 1:
+    if x.stride(-1) != 1 and x.shape[-1] > 1:
         raise ValueError(f"{name} must be contiguous in its last dimension")
+
+
+def _ld(x: torch.Tensor) -> int:
+    """Row stride of a [batch, rows, cols] operand; a single row has no
+    meaningful stride (torch may report anything), so use the row length."""
+    return x.stride(1) if x.shape[1] > 1 else x.shape[2]
+
+
+def _bs(x: torch.Tensor) -> int:
+    return x.stride(0) if x.shape[0] > 1 else 0
 
 
 def gemm_batched(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = None, *,
@@ -70,9 +80,9 @@ def gemm_batched(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = None
         _check_inner(C3, "C")
     st = load().kami_gemm_batched(
         _DT[A3.dtype], _DT[C3.dtype], _PART[partition], _VAR[variant], M, N, K, P, alloc_warps, batch,
-        A3.data_ptr(), A3.stride(1), A3.stride(0) if batch > 1 else 0, _AL[a_layout],
-        B3.data_ptr(), B3.stride(1), B3.stride(0) if batch > 1 else 0, _BL[b_layout],
-        C3.data_ptr(), C3.stride(1), C3.stride(0) if batch > 1 else 0,
+        A3.data_ptr(), _ld(A3), _bs(A3), _AL[a_layout],
+        B3.data_ptr(), _ld(B3), _bs(B3), _BL[b_layout],
+        C3.data_ptr(), _ld(C3), _bs(C3),
         float(alpha), float(beta), int(num_iter), None, 0, _stream_ptr(stream))
     check(st)
     if C is not None:
@@ -94,6 +104,58 @@ def describe(M: int, N: int, K: int, batch: int, dtype=torch.float16, out_dtype=
     return d
 
 
+class GroupedPlan:
+    """A persistent-launch plan for uneven problems (kami_gemm_grouped_*).
+
+    shapes: sequence of (M, N, K).  Problems are packed back to back in the
+    A, B and C buffers (A_i M x K, B_i N x K, C_i M x N, row-major) unless
+    explicit element offsets are given."""
+
+    def __init__(self, shapes, dtype=torch.float16, out_dtype=None, *, autotune=False, offsets=None):
+        import numpy as np
+        sh = np.asarray(shapes, dtype=np.int64).reshape(-1, 3)
+        self.count = len(sh)
+        self.dtype = dtype
+        self.out_dtype = out_dtype or (torch.float64 if dtype == torch.float64 else torch.float32)
+        M, N, K = (np.ascontiguousarray(sh[:, i], dtype=np.int32) for i in range(3))
+        if offsets is None:
+            a = np.concatenate([[0], np.cumsum(sh[:, 0] * sh[:, 2])])
+            b = np.concatenate([[0], np.cumsum(sh[:, 1] * sh[:, 2])])
+            c = np.concatenate([[0], np.cumsum(sh[:, 0] * sh[:, 1])])
+            offsets = (a[:-1], b[:-1], c[:-1])
+            self.sizes = (int(a[-1]), int(b[-1]), int(c[-1]))
+        ao, bo, co = (np.ascontiguousarray(o, dtype=np.int64) for o in offsets)
+        self.shapes, self.offsets = sh, (ao, bo, co)
+        h = ctypes.c_void_p()
+        check(load().kami_gemm_grouped_plan_create(_DT[dtype], _DT[self.out_dtype], self.count,
+                                                   M.ctypes.data, N.ctypes.data, K.ctypes.data, ao.ctypes.data,
+                                                   bo.ctypes.data, co.ctypes.data, 1 if autotune else 0,
+                                                   ctypes.byref(h)))
+        self._h = h
+
+    def info(self) -> dict:
+        out = (ctypes.c_int64 * 12)()
+        check(load().kami_gemm_grouped_plan_info(self._h, out))
+        v = list(out)
+        return {"problems": v[0], "ctas": v[1], "smem": v[2], "flops": v[3], "bytes": v[4],
+                "partitions": v[5:12]}
+
+    def run(self, A: torch.Tensor, B: torch.Tensor, C: torch.Tensor, *, alpha=1.0, beta=0.0, num_iter=1,
+            stream=None) -> torch.Tensor:
+        check(load().kami_gemm_grouped_run(self._h, A.data_ptr(), B.data_ptr(), C.data_ptr(), float(alpha),
+                                           float(beta), int(num_iter), _stream_ptr(stream)))
+        return C
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                load().kami_gemm_grouped_plan_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+
 def split_f64_gemm(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = None, *, nslices: int = 6,
                    slice_dtype=torch.float16, b_layout: str = "ref_nk", alpha: float = 1.0, beta: float = 0.0,
                    num_iter: int = 1, stream=None) -> torch.Tensor:
@@ -110,8 +172,8 @@ def split_f64_gemm(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = No
     N = B3.shape[1] if b_layout == "ref_nk" else B3.shape[2]
     C3 = torch.empty((batch, M, N), dtype=torch.float64, device=A3.device) if C is None else _as3(C)
     check(load().kami_split_f64_gemm_batched(
-        int(nslices), _DT[slice_dtype], M, N, K, batch, A3.data_ptr(), A3.stride(1), A3.stride(0),
-        B3.data_ptr(), B3.stride(1), B3.stride(0), _BL[b_layout], C3.data_ptr(), C3.stride(1), C3.stride(0),
+        int(nslices), _DT[slice_dtype], M, N, K, batch, A3.data_ptr(), _ld(A3), _bs(A3),
+        B3.data_ptr(), _ld(B3), _bs(B3), _BL[b_layout], C3.data_ptr(), _ld(C3), _bs(C3),
         float(alpha), float(beta), int(num_iter), _stream_ptr(stream)))
     if C is not None:
         return C

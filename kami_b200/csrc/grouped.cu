@@ -1,0 +1,794 @@
+// grouped.cu -- thousands of independent block GEMMs of uneven M/N/K in ONE
+// persistent launch (graph-capturable), with the warp partition chosen per
+// problem shape by a measuring autotuner.
+//
+// The reference launches one kernel per compile-time shape, one problem per
+// CTA (batched_gemm_{1d,2d,3d}_double_mma.cu: blockIdx.x = problem, :83-86).
+// Here every problem carries its own (M, N, K) and partition, and a fixed
+// grid of persistent CTAs (8 warps each) walks a host-built schedule
+// (longest-processing-time-first over the CTAs).  Each CTA streams its
+// problems through a multi-stage cp.async pipeline of K chunks staged in
+// shared memory, so the loads of the next chunk (or the next problem)
+// overlap the MMAs of the current one.
+//
+// Partitions of the 8 warps (R x C x D warp grids, R*C*D = 8), the KAMI
+// 1D / 2D / 3D ideas applied to a runtime-sized tile:
+//   cfg 0  8x1x1  1D: warps split M (16-row strips), each owns all of N
+//   cfg 1  4x2x1  2D
+//   cfg 2  2x4x1  2D
+//   cfg 3  2x2x2  3D: K steps interleaved over 2 depth ranks (M, N <= 64)
+//   cfg 4  1x1x8  3D: 8 depth ranks (M, N <= 32)
+//   cfg 5  2x1x4  3D (M <= 64, N <= 32)
+//   cfg 6  1x2x4  3D (M <= 32, N <= 64)
+// Depth partials are reduced on the device through shared memory.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <queue>
+#include <tuple>
+#include <vector>
+
+#include "kami_common.cuh"
+#include "mma_engine.cuh"
+
+namespace kami {
+
+int fail(int code, const char *fmt, ...);
+int cuda_fail(cudaError_t e, const char *what);
+
+struct GroupedDesc
+{
+    int M, N, K, cfg;
+    int64_t a_off, b_off, c_off;
+    int lda, ldb, ldc, pad_;
+};
+
+struct GroupedParams
+{
+    const GroupedDesc *desc; // problems in schedule order
+    const int *cta_begin;    // ctas + 1 offsets into desc
+    const void *A;
+    const void *B;
+    void *C;
+    int out_type;
+    double alpha, beta;
+    int num_iter;
+};
+
+namespace {
+
+constexpr int kWarps = 8;
+constexpr int kThreads = kWarps * 32;
+constexpr int kCfgs = 7;
+__host__ __device__ constexpr int cfg_R(int c) { return c == 0 ? 8 : c == 1 ? 4 : c == 2 ? 2 : c == 3 ? 2 : c == 4 ? 1 : c == 5 ? 2 : 1; }
+__host__ __device__ constexpr int cfg_C(int c) { return c == 0 ? 1 : c == 1 ? 2 : c == 2 ? 4 : c == 3 ? 2 : c == 4 ? 1 : c == 5 ? 1 : 2; }
+__host__ __device__ constexpr int cfg_D(int c) { return c <= 2 ? 1 : c == 3 ? 2 : c == 4 ? 8 : 4; }
+// register tile (fragment rows x fragment cols) a warp can hold per cfg
+__host__ __device__ constexpr int cfg_MI(int c) { return c == 0 ? 1 : c == 1 ? 2 : c == 2 ? 4 : 2; }
+__host__ __device__ constexpr int cfg_MJ(int c) { return c == 0 ? 16 : c == 1 ? 8 : c == 2 ? 4 : 4; }
+
+// per-precision pipeline geometry
+template <class Tr>
+struct GGeom
+{
+    static constexpr int ES = sizeof(typename Tr::Elem);
+    static constexpr int KCH = ES == 2 ? 64 : 32; // K elements per chunk
+    static constexpr int PAD = ES == 2 ? 16 : 8;  // row padding (elements) for conflict-free fragment loads
+    static constexpr int LD = KCH + PAD;          // smem row stride (elements)
+    static constexpr int STAGES = ES == 2 ? 3 : 2;
+    static constexpr int OPER = 128 * LD * ES;    // bytes of one operand in a stage
+    static constexpr int STAGE = 2 * OPER;
+    static constexpr int RED = kWarps * 8 * 128 * (int)sizeof(typename Tr::Acc); // depth partials
+    static constexpr int SMEM = STAGES * STAGE + RED;
+};
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, bool valid)
+{
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+    const int n = valid ? 16 : 0; // src-size 0: zero-fill
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+template <class Tr>
+__device__ __forceinline__ void load_chunk(const GroupedParams &p, const GroupedDesc &d, int k0, uint8_t *stage)
+{
+    using G = GGeom<Tr>;
+    using Elem = typename Tr::Elem;
+    constexpr int CPR = G::KCH * G::ES / 16; // 16-byte chunks per staged row
+    const Elem *A = reinterpret_cast<const Elem *>(p.A) + d.a_off;
+    const Elem *B = reinterpret_cast<const Elem *>(p.B) + d.b_off;
+    Elem *sA = reinterpret_cast<Elem *>(stage);
+    Elem *sB = reinterpret_cast<Elem *>(stage + G::OPER);
+    const int epc = 16 / G::ES; // elements per 16-byte chunk
+    for (int c = threadIdx.x; c < d.M * CPR; c += kThreads)
+    {
+        const int r = c / CPR, q = c % CPR;
+        const int k = k0 + q * epc;
+        const bool v = k < d.K;
+        cp_async16(sA + r * G::LD + q * epc, v ? (const void *)(A + (int64_t)r * d.lda + k) : (const void *)A, v);
+    }
+    for (int c = threadIdx.x; c < d.N * CPR; c += kThreads)
+    {
+        const int r = c / CPR, q = c % CPR;
+        const int k = k0 + q * epc;
+        const bool v = k < d.K;
+        cp_async16(sB + r * G::LD + q * epc, v ? (const void *)(B + (int64_t)r * d.ldb + k) : (const void *)B, v);
+    }
+}
+
+struct Tile
+{
+    int i0, ni, j0, nj, d, D;
+};
+
+__device__ __forceinline__ Tile warp_tile(const GroupedDesc &d, int warp)
+{
+    const int cfg = d.cfg;
+    const int R = cfg_R(cfg), C = cfg_C(cfg), D = cfg_D(cfg);
+    const int MF = (d.M + 15) >> 4, NF = (d.N + 7) >> 3;
+    const int dr = warp % D, c = (warp / D) % C, r = warp / (D * C);
+    const int mi = (MF + R - 1) / R, mj = (NF + C - 1) / C;
+    Tile t;
+    t.i0 = r * mi;
+    t.ni = max(0, min(mi, MF - t.i0));
+    t.j0 = c * mj;
+    t.nj = max(0, min(mj, NF - t.j0));
+    t.d = dr;
+    t.D = D;
+    return t;
+}
+
+template <class Tr, int MI, int MJ>
+__device__ __forceinline__ void compute_chunk(const GroupedDesc &d, const Tile &t, int k0, const uint8_t *stage,
+                                              int num_iter, typename Tr::Acc (&acc)[16][4])
+{
+    using G = GGeom<Tr>;
+    using Unit = typename Tr::Unit;
+    using Elem = typename Tr::Elem;
+    const Elem *sA = reinterpret_cast<const Elem *>(stage);
+    const Elem *sB = reinterpret_cast<const Elem *>(stage + G::OPER);
+    const int lane = threadIdx.x & 31, gq = lane >> 2, tq = lane & 3;
+    const int kin = min(G::KCH, d.K - k0);
+    const int ksteps = (kin + Tr::KSTEP - 1) / Tr::KSTEP;
+    const int lane_k = tq * 2 * Tr::EPU;
+    if (t.ni <= 0 || t.nj <= 0)
+        return;
+    for (int it = 0; it < num_iter; ++it)
+        for (int ks = t.d; ks < ksteps; ks += t.D)
+        {
+            const int kk = ks * Tr::KSTEP + lane_k;
+            Unit a[MI][4];
+#pragma unroll
+            for (int ii = 0; ii < MI; ++ii)
+                if (ii < t.ni)
+                {
+                    const int r = (t.i0 + ii) * 16 + gq;
+                    Tr::ld2_smem(sA + r * G::LD + kk, a[ii][0], a[ii][2]);
+                    Tr::ld2_smem(sA + (r + 8) * G::LD + kk, a[ii][1], a[ii][3]);
+                }
+            // B fragments one at a time: only the A fragments and one B
+            // fragment are live next to the accumulators
+#pragma unroll
+            for (int jj = 0; jj < MJ; ++jj)
+                if (jj < t.nj)
+                {
+                    Unit b0, b1;
+                    const int n = (t.j0 + jj) * 8 + gq;
+                    Tr::ld2_smem(sB + n * G::LD + kk, b0, b1);
+#pragma unroll
+                    for (int ii = 0; ii < MI; ++ii)
+                        if (ii < t.ni)
+                            Tr::mma(acc[ii * MJ + jj], a[ii], b0, b1);
+                }
+        }
+}
+
+template <class Acc>
+__device__ __forceinline__ void gstore_pair(const GroupedParams &p, const GroupedDesc &d, int r, int c, Acc v0,
+                                            Acc v1)
+{
+    GemmArgs g{};
+    g.M = d.M;
+    g.N = d.N;
+    g.ldc = d.ldc;
+    g.out_type = p.out_type;
+    g.c_vec = ((d.ldc & 1) == 0) && ((d.c_off & 1) == 0); // the C base is 16-byte aligned (host-checked)
+    g.alpha = p.alpha;
+    g.beta = p.beta;
+    const int osz = p.out_type == KAMI_F64 ? 8 : p.out_type == KAMI_F32 ? 4 : 2;
+    void *Cb = reinterpret_cast<char *>(p.C) + d.c_off * osz;
+    store_pair<Acc>(g, Cb, r, c, v0, v1);
+}
+
+template <class Tr, int MI, int MJ>
+__device__ __forceinline__ void finish_problem(const GroupedParams &p, const GroupedDesc &d, const Tile &t,
+                                               uint8_t *red_raw, typename Tr::Acc (&acc)[16][4])
+{
+    using Acc = typename Tr::Acc;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (t.D > 1)
+    {
+        // depth ranks d > 0 leave their partials; rank 0 of each (r, c) sums
+        Acc *red = reinterpret_cast<Acc *>(red_raw);
+        if (t.d > 0)
+        {
+            Acc *dst = red + (size_t)warp * (MI * MJ * 128) + lane * 4;
+#pragma unroll
+            for (int ii = 0; ii < MI; ++ii)
+#pragma unroll
+                for (int jj = 0; jj < MJ; ++jj)
+#pragma unroll
+                    for (int e = 0; e < 4; ++e)
+                        dst[(ii * MJ + jj) * 128 + e] = acc[ii * MJ + jj][e];
+        }
+        __syncthreads();
+        if (t.d == 0)
+        {
+            for (int dd = 1; dd < t.D; ++dd)
+            {
+                const Acc *src = red + (size_t)(warp + dd) * (MI * MJ * 128) + lane * 4;
+#pragma unroll
+                for (int ii = 0; ii < MI; ++ii)
+#pragma unroll
+                    for (int jj = 0; jj < MJ; ++jj)
+#pragma unroll
+                        for (int e = 0; e < 4; ++e)
+                            acc[ii * MJ + jj][e] += src[(ii * MJ + jj) * 128 + e];
+            }
+        }
+    }
+    if (t.d == 0)
+    {
+        const int gq = lane >> 2, tq = lane & 3;
+#pragma unroll
+        for (int ii = 0; ii < MI; ++ii)
+#pragma unroll
+            for (int jj = 0; jj < MJ; ++jj)
+                if (ii < t.ni && jj < t.nj)
+                {
+                    const int r = (t.i0 + ii) * 16 + gq, c = (t.j0 + jj) * 8 + 2 * tq;
+                    gstore_pair<Acc>(p, d, r, c, acc[ii * MJ + jj][0], acc[ii * MJ + jj][1]);
+                    gstore_pair<Acc>(p, d, r + 8, c, acc[ii * MJ + jj][2], acc[ii * MJ + jj][3]);
+                }
+    }
+}
+
+template <class Tr, int MI, int MJ>
+__device__ __forceinline__ void run_chunk(const GroupedParams &p, const GroupedDesc &d, int k0, bool first,
+                                          bool last, const uint8_t *stage, uint8_t *red,
+                                          typename Tr::Acc (&acc)[16][4])
+{
+    static_assert(MI * MJ <= 16, "register tile");
+    const Tile t = warp_tile(d, threadIdx.x >> 5);
+    if (first)
+    {
+#pragma unroll
+        for (int f = 0; f < 16; ++f)
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+                acc[f][e] = 0;
+    }
+    compute_chunk<Tr, MI, MJ>(d, t, k0, stage, p.num_iter, acc);
+    if (last)
+        finish_problem<Tr, MI, MJ>(p, d, t, red, acc);
+}
+
+template <class Tr>
+__global__ void __launch_bounds__(kThreads, 1) grouped_kernel(const GroupedParams p)
+{
+    using G = GGeom<Tr>;
+    using Acc = typename Tr::Acc;
+    extern __shared__ __align__(128) uint8_t smem[];
+    uint8_t *red = smem + G::STAGES * G::STAGE;
+    const int begin = p.cta_begin[blockIdx.x], end = p.cta_begin[blockIdx.x + 1];
+    if (begin >= end)
+        return;
+
+    // unit cursor for the loads (problem index, chunk start)
+    int lp = begin, lk = 0;
+    auto issue = [&](int slot) {
+        if (lp < end)
+        {
+            const GroupedDesc d = p.desc[lp];
+            load_chunk<Tr>(p, d, lk, smem + slot * G::STAGE);
+            lk += G::KCH;
+            if (lk >= d.K)
+            {
+                lk = 0;
+                ++lp;
+            }
+        }
+        cp_async_commit();
+    };
+#pragma unroll
+    for (int s = 0; s < G::STAGES - 1; ++s)
+        issue(s);
+
+    // accumulators (up to 16 fragments per warp), live across K chunks; each
+    // register-tile shape indexes them as [ii * MJ + jj]
+    Acc acc[16][4];
+    int cp = begin, ck = 0, u = 0;
+    while (cp < end)
+    {
+        issue((u + G::STAGES - 1) % G::STAGES);
+        cp_async_wait<G::STAGES - 1>();
+        __syncthreads();
+        const GroupedDesc d = p.desc[cp];
+        const uint8_t *stage = smem + (u % G::STAGES) * G::STAGE;
+        const bool first = ck == 0, last = ck + G::KCH >= d.K;
+        switch (d.cfg)
+        {
+        case 0:
+            run_chunk<Tr, 1, 16>(p, d, ck, first, last, stage, red, acc);
+            break;
+        case 1:
+            run_chunk<Tr, 2, 8>(p, d, ck, first, last, stage, red, acc);
+            break;
+        case 2:
+            run_chunk<Tr, 4, 4>(p, d, ck, first, last, stage, red, acc);
+            break;
+        default:
+            run_chunk<Tr, 2, 4>(p, d, ck, first, last, stage, red, acc);
+            break;
+        }
+        __syncthreads();
+        ck += G::KCH;
+        if (last)
+        {
+            ck = 0;
+            ++cp;
+        }
+        ++u;
+    }
+    cp_async_wait<0>();
+}
+
+} // namespace
+} // namespace kami
+
+// ---------------------------------------------------------------------------
+// host side: plan = descriptors + schedule (+ autotuned partitions)
+// ---------------------------------------------------------------------------
+using namespace kami;
+
+struct kami_grouped_plan
+{
+    int in_type, out_type, count, ctas, smem;
+    GroupedDesc *d_desc = nullptr;
+    int *d_begin = nullptr;
+    int cfg_hist[kCfgs] = {0};
+    int64_t flops = 0, bytes = 0;
+};
+
+namespace kami {
+namespace {
+
+bool cfg_valid(int cfg, int M, int N)
+{
+    const int MF = (M + 15) / 16, NF = (N + 7) / 8;
+    return (MF + cfg_R(cfg) - 1) / cfg_R(cfg) <= cfg_MI(cfg) && (NF + cfg_C(cfg) - 1) / cfg_C(cfg) <= cfg_MJ(cfg);
+}
+
+// static choice: fewest MMA steps on the busiest warp, then fewer depth ranks
+int cfg_heuristic(int in_type, int M, int N, int K)
+{
+    const int kstep = in_type == KAMI_F64 ? 8 : 16;
+    const int MF = (M + 15) / 16, NF = (N + 7) / 8, KS = (K + kstep - 1) / kstep;
+    int best = -1;
+    double bc = 0;
+    for (int c = 0; c < kCfgs; ++c)
+    {
+        if (!cfg_valid(c, M, N))
+            continue;
+        const int mi = (MF + cfg_R(c) - 1) / cfg_R(c), mj = (NF + cfg_C(c) - 1) / cfg_C(c);
+        const int kd = (KS + cfg_D(c) - 1) / cfg_D(c);
+        const double cost = (double)mi * mj * kd + 0.5 * (mi + mj) * kd + (cfg_D(c) > 1 ? 4.0 * mi * mj : 0.0);
+        if (best < 0 || cost < bc)
+        {
+            best = c;
+            bc = cost;
+        }
+    }
+    return best;
+}
+
+// autotune cache: (in_type, M/8, N/8, K/8) -> cfg, measured on this device
+std::mutex g_tune_mu;
+struct TuneKey
+{
+    int dev, in_type, M, N, K;
+    bool operator<(const TuneKey &o) const
+    {
+        return std::tie(dev, in_type, M, N, K) < std::tie(o.dev, o.in_type, o.M, o.N, o.K);
+    }
+};
+std::map<TuneKey, int> g_tune;
+
+} // namespace
+} // namespace kami
+
+static const void *grouped_fn(int in_type)
+{
+    return in_type == KAMI_F64    ? (const void *)&grouped_kernel<TrF64>
+           : in_type == KAMI_BF16 ? (const void *)&grouped_kernel<TrH16<true>>
+                                  : (const void *)&grouped_kernel<TrH16<false>>;
+}
+
+static int grouped_smem(int in_type)
+{
+    return in_type == KAMI_F64 ? GGeom<TrF64>::SMEM : GGeom<TrH16<false>>::SMEM;
+}
+
+static int launch_grouped(const kami_grouped_plan *plan, const void *A, const void *B, void *C, double alpha,
+                          double beta, int num_iter, cudaStream_t s)
+{
+    GroupedParams p{};
+    p.desc = plan->d_desc;
+    p.cta_begin = plan->d_begin;
+    p.A = A;
+    p.B = B;
+    p.C = C;
+    p.out_type = plan->out_type;
+    p.alpha = alpha;
+    p.beta = beta;
+    p.num_iter = num_iter;
+    void *args[] = {&p};
+    cudaError_t e = cudaLaunchKernel(grouped_fn(plan->in_type), dim3(plan->ctas), dim3(kThreads), args,
+                                     (size_t)plan->smem, s);
+    if (e != cudaSuccess)
+        return cuda_fail(e, "cudaLaunchKernel(grouped_kernel)");
+    return KAMI_OK;
+}
+
+static int free_plan(kami_grouped_plan *pl)
+{
+    if (!pl)
+        return KAMI_OK;
+    if (pl->d_desc)
+        cudaFree(pl->d_desc);
+    if (pl->d_begin)
+        cudaFree(pl->d_begin);
+    delete pl;
+    return KAMI_OK;
+}
+
+// Build descriptors + LPT schedule for `count` problems (host arrays) with
+// the given partitions and upload them.
+static int build_plan(int in_type, int out_type, int count, const int *M, const int *N, const int *K,
+                      const int64_t *ao, const int64_t *bo, const int64_t *co, const int *cfg,
+                      kami_grouped_plan **out, const int *lda = nullptr, const int *ldb = nullptr,
+                      const int *ldc = nullptr)
+{
+    int dev = 0, sms = 0, occ = 0;
+    cudaError_t e;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess)
+        return cuda_fail(e, "cudaGetDevice");
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+        return cuda_fail(e, "cudaDeviceGetAttribute");
+    const void *fn = grouped_fn(in_type);
+    const int smem = grouped_smem(in_type);
+    if ((e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
+        return cuda_fail(e, "cudaFuncSetAttribute(grouped_kernel)");
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kThreads, smem)) != cudaSuccess)
+        return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    occ = std::max(occ, 1);
+    const int ctas = std::max(1, std::min(count, sms * occ));
+    const int esz = in_type == KAMI_F64 ? 8 : 2;
+    const int osz = out_type == KAMI_F64 ? 8 : out_type == KAMI_F32 ? 4 : 2;
+    const double balance = in_type == KAMI_F64 ? 6.0 : 150.0; // FLOP per byte where compute and HBM meet
+
+    auto *pl = new kami_grouped_plan();
+    pl->in_type = in_type;
+    pl->out_type = out_type;
+    pl->count = count;
+    pl->ctas = ctas;
+    pl->smem = smem;
+    std::vector<double> cost(count);
+    std::vector<int> order(count);
+    for (int i = 0; i < count; ++i)
+    {
+        const double fl = 2.0 * M[i] * N[i] * K[i];
+        const double by = (double)(M[i] + N[i]) * K[i] * esz + (double)M[i] * N[i] * osz;
+        cost[i] = std::max(fl / balance, by) + 2048.0; // + fixed per-problem latency
+        order[i] = i;
+        pl->flops += (int64_t)fl;
+        pl->bytes += (int64_t)by;
+        pl->cfg_hist[cfg[i]]++;
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    typedef std::pair<double, int> Load;
+    std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
+    for (int c = 0; c < ctas; ++c)
+        heap.push(Load(0.0, c));
+    std::vector<std::vector<int>> lists(ctas);
+    for (int i : order)
+    {
+        Load l = heap.top();
+        heap.pop();
+        lists[l.second].push_back(i);
+        heap.push(Load(l.first + cost[i], l.second));
+    }
+    std::vector<GroupedDesc> desc;
+    desc.reserve(count);
+    std::vector<int> begin(ctas + 1, 0);
+    for (int c = 0; c < ctas; ++c)
+    {
+        begin[c] = (int)desc.size();
+        for (int i : lists[c])
+            desc.push_back(GroupedDesc{M[i], N[i], K[i], cfg[i], ao[i], bo[i], co[i], lda ? lda[i] : K[i],
+                                       ldb ? ldb[i] : K[i], ldc ? ldc[i] : N[i], 0});
+    }
+    begin[ctas] = (int)desc.size();
+    if ((e = cudaMalloc(&pl->d_desc, sizeof(GroupedDesc) * std::max(count, 1))) != cudaSuccess ||
+        (e = cudaMalloc(&pl->d_begin, sizeof(int) * (ctas + 1))) != cudaSuccess)
+    {
+        free_plan(pl);
+        return cuda_fail(e, "cudaMalloc(grouped plan)");
+    }
+    if ((e = cudaMemcpy(pl->d_desc, desc.data(), sizeof(GroupedDesc) * count, cudaMemcpyHostToDevice)) !=
+            cudaSuccess ||
+        (e = cudaMemcpy(pl->d_begin, begin.data(), sizeof(int) * (ctas + 1), cudaMemcpyHostToDevice)) != cudaSuccess)
+    {
+        free_plan(pl);
+        return cuda_fail(e, "cudaMemcpy(grouped plan)");
+    }
+    *out = pl;
+    return KAMI_OK;
+}
+
+// Measure every valid partition on a batch of problems of one shape and
+// return the fastest.  Scratch buffers are the caller's.
+static int tune_shape(int in_type, int out_type, int M, int N, int K, void *A, void *B, void *C, int reps_problems,
+                      int *best_cfg)
+{
+    std::vector<int> vm(reps_problems, M), vn(reps_problems, N), vk(reps_problems, K), vc(reps_problems);
+    std::vector<int64_t> ao(reps_problems), bo(reps_problems), co(reps_problems);
+    for (int i = 0; i < reps_problems; ++i)
+    {
+        ao[i] = (int64_t)i * M * K;
+        bo[i] = (int64_t)i * N * K;
+        co[i] = (int64_t)i * M * N;
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = 1e30f;
+    int bc = cfg_heuristic(in_type, M, N, K);
+    for (int c = 0; c < kCfgs; ++c)
+    {
+        if (!cfg_valid(c, M, N))
+            continue;
+        std::fill(vc.begin(), vc.end(), c);
+        kami_grouped_plan *pl = nullptr;
+        int st = build_plan(in_type, out_type, reps_problems, vm.data(), vn.data(), vk.data(), ao.data(), bo.data(),
+                            co.data(), vc.data(), &pl);
+        if (st)
+        {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            return st;
+        }
+        launch_grouped(pl, A, B, C, 1.0, 0.0, 1, 0);
+        cudaEventRecord(e0, 0);
+        for (int r = 0; r < 3; ++r)
+            launch_grouped(pl, A, B, C, 1.0, 0.0, 1, 0);
+        cudaEventRecord(e1, 0);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        free_plan(pl);
+        if (ms < best)
+        {
+            best = ms;
+            bc = c;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return cuda_fail(e, "grouped autotune");
+    *best_cfg = bc;
+    return KAMI_OK;
+}
+
+namespace kami {
+
+// Serve a batched request that no compiled block instance covers (e.g. FP64
+// above 64^3) with the grouped kernel: one plan per distinct request shape,
+// cached (descriptors hold offsets, not pointers, so a plan serves any
+// buffers).
+int grouped_fallback(const GemmArgs &g, int in_type, cudaStream_t stream)
+{
+    if (g.a_layout != KAMI_A_ROW_MK || g.b_layout != KAMI_B_REF_NK)
+        return fail(KAMI_ERR_UNSUPPORTED, "no kernel for this shape with these layouts");
+    const int q = in_type == KAMI_F64 ? 2 : 8;
+    if (g.M > 128 || g.N > 128 || g.K > 128 || g.K % q || g.lda % q || g.ldb % q || g.sA % q || g.sB % q ||
+        g.batch > 1000000)
+        return fail(KAMI_ERR_UNSUPPORTED, "no kernel for M=%d N=%d K=%d (lda=%lld ldb=%lld)", g.M, g.N, g.K,
+                    (long long)g.lda, (long long)g.ldb);
+    if ((reinterpret_cast<uintptr_t>(g.A) & 15) || (reinterpret_cast<uintptr_t>(g.B) & 15) ||
+        (reinterpret_cast<uintptr_t>(g.C) & 15))
+        return fail(KAMI_ERR_UNSUPPORTED, "no kernel for this shape with unaligned buffers");
+    static std::mutex mu;
+    static std::map<std::vector<int64_t>, kami_grouped_plan *> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::vector<int64_t> key = {dev, in_type, g.out_type, g.M, g.N, g.K, g.batch, g.lda, g.ldb, g.ldc, g.sA, g.sB, g.sC};
+    kami_grouped_plan *pl = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find(key);
+        if (it != cache.end())
+            pl = it->second;
+    }
+    if (!pl)
+    {
+        const int n = (int)g.batch;
+        std::vector<int> vm(n, g.M), vn(n, g.N), vk(n, g.K), vc(n, cfg_heuristic(in_type, g.M, g.N, g.K));
+        std::vector<int> la(n, (int)g.lda), lb(n, (int)g.ldb), lc(n, (int)g.ldc);
+        std::vector<int64_t> ao(n), bo(n), co(n);
+        for (int i = 0; i < n; ++i)
+        {
+            ao[i] = (int64_t)i * g.sA;
+            bo[i] = (int64_t)i * g.sB;
+            co[i] = (int64_t)i * g.sC;
+        }
+        int st = build_plan(in_type, g.out_type, n, vm.data(), vn.data(), vk.data(), ao.data(), bo.data(), co.data(),
+                            vc.data(), &pl, la.data(), lb.data(), lc.data());
+        if (st)
+            return st;
+        std::lock_guard<std::mutex> lk(mu);
+        if (cache.size() < 256)
+            cache[key] = pl;
+    }
+    return launch_grouped(pl, g.A, g.B, g.C, g.alpha, g.beta, g.num_iter, stream);
+}
+
+} // namespace kami
+
+extern "C" {
+
+int kami_gemm_grouped_plan_create(kami_dtype_t in_type, kami_dtype_t out_type, int count, const int *M, const int *N,
+                                  const int *K, const int64_t *a_offsets, const int64_t *b_offsets,
+                                  const int64_t *c_offsets, int flags, kami_grouped_plan **plan)
+{
+    if (!plan)
+        return fail(KAMI_ERR_INVALID_VALUE, "grouped: plan is NULL");
+    *plan = nullptr;
+    if (in_type != KAMI_F16 && in_type != KAMI_BF16 && in_type != KAMI_F64)
+        return fail(KAMI_ERR_INVALID_VALUE, "grouped: in_type must be KAMI_F16, KAMI_BF16 or KAMI_F64");
+    if ((in_type == KAMI_F64) != (out_type == KAMI_F64) ||
+        (out_type != KAMI_F64 && out_type != KAMI_F32 && out_type != KAMI_F16 && out_type != KAMI_BF16))
+        return fail(KAMI_ERR_UNSUPPORTED, "grouped: output type does not match the input type");
+    if (count < 0 || (count > 0 && (!M || !N || !K || !a_offsets || !b_offsets || !c_offsets)))
+        return fail(KAMI_ERR_INVALID_VALUE, "grouped: bad count or null shape/offset arrays");
+    const int kq = in_type == KAMI_F64 ? 2 : 8;
+    for (int i = 0; i < count; ++i)
+    {
+        if (M[i] < 1 || N[i] < 1 || K[i] < 1 || M[i] > 128 || N[i] > 128 || K[i] > 128)
+            return fail(KAMI_ERR_UNSUPPORTED, "grouped: problem %d has M, N, K = %d, %d, %d (each must be 1..128)",
+                        i, M[i], N[i], K[i]);
+        if (K[i] % kq)
+            return fail(KAMI_ERR_UNSUPPORTED, "grouped: problem %d: K must be a multiple of %d", i, kq);
+        if (a_offsets[i] % kq || b_offsets[i] % kq || a_offsets[i] < 0 || b_offsets[i] < 0 || c_offsets[i] < 0)
+            return fail(KAMI_ERR_MISALIGNED, "grouped: problem %d: A/B offsets must be multiples of %d", i, kq);
+    }
+    std::vector<int> cfg(count);
+    const bool tune = (flags & 1) != 0;
+    if (!tune)
+    {
+        for (int i = 0; i < count; ++i)
+            cfg[i] = cfg_heuristic(in_type, M[i], N[i], K[i]);
+    }
+    else
+    {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        // tune per 16-rounded shape bucket, measured at the bucket's largest shape
+        std::map<TuneKey, int> need;
+        for (int i = 0; i < count; ++i)
+        {
+            TuneKey k{dev, in_type, (M[i] + 15) / 16, (N[i] + 15) / 16, (K[i] + 15) / 16};
+            need[k] = -1;
+        }
+        {
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            for (auto &kv : need)
+            {
+                auto it = g_tune.find(kv.first);
+                if (it != g_tune.end())
+                    kv.second = it->second;
+            }
+        }
+        const int reps = 1024;
+        const int esz = in_type == KAMI_F64 ? 8 : 2, osz = out_type == KAMI_F64 ? 8 : out_type == KAMI_F32 ? 4 : 2;
+        void *tA = nullptr, *tB = nullptr, *tC = nullptr;
+        bool missing = false;
+        for (auto &kv : need)
+            missing |= kv.second < 0;
+        if (missing)
+        {
+            cudaError_t e;
+            if ((e = cudaMalloc(&tA, (size_t)reps * 128 * 128 * esz)) != cudaSuccess ||
+                (e = cudaMalloc(&tB, (size_t)reps * 128 * 128 * esz)) != cudaSuccess ||
+                (e = cudaMalloc(&tC, (size_t)reps * 128 * 128 * osz)) != cudaSuccess)
+            {
+                cudaFree(tA);
+                cudaFree(tB);
+                return cuda_fail(e, "cudaMalloc(grouped autotune scratch)");
+            }
+            cudaMemset(tA, 0, (size_t)reps * 128 * 128 * esz);
+            cudaMemset(tB, 0, (size_t)reps * 128 * 128 * esz);
+            for (auto &kv : need)
+            {
+                if (kv.second >= 0)
+                    continue;
+                const int m = std::min(128, kv.first.M * 16), n = std::min(128, kv.first.N * 16),
+                          k = std::min(128, kv.first.K * 16);
+                int best = 0;
+                int st = tune_shape(in_type, out_type, m, n, k, tA, tB, tC, reps, &best);
+                if (st)
+                {
+                    cudaFree(tA);
+                    cudaFree(tB);
+                    cudaFree(tC);
+                    return st;
+                }
+                kv.second = best;
+                std::lock_guard<std::mutex> lk(g_tune_mu);
+                g_tune[kv.first] = best;
+            }
+            cudaFree(tA);
+            cudaFree(tB);
+            cudaFree(tC);
+        }
+        for (int i = 0; i < count; ++i)
+        {
+            TuneKey k{dev, in_type, (M[i] + 15) / 16, (N[i] + 15) / 16, (K[i] + 15) / 16};
+            int c = need[k];
+            cfg[i] = cfg_valid(c, M[i], N[i]) ? c : cfg_heuristic(in_type, M[i], N[i], K[i]);
+        }
+    }
+    return build_plan(in_type, out_type, count, M, N, K, a_offsets, b_offsets, c_offsets, cfg.data(), plan);
+}
+
+int kami_gemm_grouped_run(const kami_grouped_plan *plan, const void *A, const void *B, void *C, double alpha,
+                          double beta, int num_iter, void *stream)
+{
+    if (!plan)
+        return fail(KAMI_ERR_INVALID_VALUE, "grouped: plan is NULL");
+    if (num_iter < 1)
+        return fail(KAMI_ERR_INVALID_VALUE, "grouped: num_iter must be >= 1");
+    if (plan->count == 0)
+        return KAMI_OK;
+    if (!A || !B || !C)
+        return fail(KAMI_ERR_INVALID_VALUE, "grouped: null buffer");
+    if ((reinterpret_cast<uintptr_t>(A) & 15) || (reinterpret_cast<uintptr_t>(B) & 15) ||
+        (reinterpret_cast<uintptr_t>(C) & 15))
+        return fail(KAMI_ERR_MISALIGNED, "grouped: A, B, C must be 16-byte aligned");
+    return launch_grouped(plan, A, B, C, alpha, beta, num_iter, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int kami_gemm_grouped_plan_info(const kami_grouped_plan *plan, int64_t out[12])
+{
+    if (!plan || !out)
+        return fail(KAMI_ERR_INVALID_VALUE, "grouped: null plan or out");
+    out[0] = plan->count;
+    out[1] = plan->ctas;
+    out[2] = plan->smem;
+    out[3] = plan->flops;
+    out[4] = plan->bytes;
+    for (int c = 0; c < kCfgs; ++c)
+        out[5 + c] = plan->cfg_hist[c];
+    return KAMI_OK;
+}
+
+int kami_gemm_grouped_plan_destroy(kami_grouped_plan *plan) { return free_plan(plan); }
+
+} // extern "C"

@@ -13,6 +13,7 @@
 namespace kami {
 
 int split_read_error(int *flag);
+int grouped_fallback(const GemmArgs &g, int in_type, cudaStream_t stream);
 
 static thread_local char g_err[512] = "no error";
 
@@ -355,6 +356,12 @@ int kami_gemm_batched(kami_dtype_t in_type, kami_dtype_t out_type, kami_partitio
     const MmaInstance *inst = nullptr;
     LaunchInfo info{};
     st = plan_mma(in_type, partition, P, alloc_warps, M, N, K, batch, &inst, &info, true);
+    if (st == KAMI_ERR_UNSUPPORTED && variant == KAMI_VARIANT_AUTO && partition == KAMI_PARTITION_AUTO && P == 0 &&
+        alloc_warps == 0)
+    {
+        g.problems_per_cta = 1;
+        return grouped_fallback(g, in_type, s);
+    }
     if (st)
         return st;
     int max_threads = 0;

@@ -84,6 +84,13 @@ struct TrH16
     {
         *reinterpret_cast<uint2 *>(s) = make_uint2(x, y);
     }
+    // two units (4 contiguous elements) from shared memory
+    __device__ __forceinline__ static void ld2_smem(const Elem *p, Unit &lo, Unit &hi)
+    {
+        uint2 v = *reinterpret_cast<const uint2 *>(p);
+        lo = v.x;
+        hi = v.y;
+    }
     __device__ __forceinline__ static void lds2(const Unit *s, Unit &x, Unit &y)
     {
         uint2 v = *reinterpret_cast<const uint2 *>(s);
@@ -122,6 +129,12 @@ struct TrF64
     __device__ __forceinline__ static void st2(Unit *s, Unit x, Unit y)
     {
         *reinterpret_cast<double2 *>(s) = make_double2(x, y);
+    }
+    __device__ __forceinline__ static void ld2_smem(const Elem *p, Unit &lo, Unit &hi)
+    {
+        double2 v = *reinterpret_cast<const double2 *>(p);
+        lo = v.x;
+        hi = v.y;
     }
     __device__ __forceinline__ static void lds2(const Unit *s, Unit &x, Unit &y)
     {

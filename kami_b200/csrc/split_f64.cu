@@ -19,9 +19,9 @@
 //      half those with p + q = c + 1.  Products with 2t+1+q > s+1 are
 //      dropped (their weight is below 2^(-beta (s+2))).  With at most
 //      ceil(s/2) digit pairs per half, |d| <= 2^(beta-1) and K <= 64, every
-//      partial sum is an integer of magnitude <= 3 * 2^(2 beta - 2) * 64 <
-//      2^24 (beta = 9, s <= 6; beta = 7, s <= 8), so the FP32 accumulation
-//      is exact;
+//      partial sum is an integer of magnitude <= ceil(s/2) * 2^(2 beta - 2) *
+//      64 <= 2^24 (beta = 9, s <= 7; beta = 7, s <= 8), so the FP32
+//      accumulation is exact;
 //   4. recombination in FP64: C_ij = 2^(eA_i + eB_j) * sum_c (top_c 2^(-beta c)
 //      + bottom_c 2^(-beta (c+1))), smallest weights first.
 // FP64 is used only in steps 1, 2 and 4; all products run on the tensor
@@ -376,7 +376,7 @@ extern "C" int kami_split_f64_gemm_batched(int nslices, kami_dtype_t slice_type,
     const bool bf = slice_type == KAMI_BF16;
     if (slice_type != KAMI_F16 && slice_type != KAMI_BF16)
         return fail(KAMI_ERR_INVALID_VALUE, "split-FP64: slice_type must be KAMI_F16 or KAMI_BF16");
-    const int smax = bf ? 8 : 6;
+    const int smax = bf ? 8 : 7;
     if (nslices < 2 || nslices > smax)
         return fail(KAMI_ERR_UNSUPPORTED, "split-FP64: %d slices; supported 2..%d for this slice type", nslices,
                     smax);

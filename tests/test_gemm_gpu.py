@@ -102,7 +102,7 @@ def test_mma_layouts(cuda, prec, b_layout, a_layout, part, P):
 @pytest.mark.parametrize("num_iter", [1, 2, 7])
 def test_num_iter_accumulates(cuda, prec, num_iter):
     # the reference's in-register repeat: C = NUM_ITER * A*B, checked as C / NUM_ITER
-    for part, P in [("1d", 2), ("2d", 2), ("3d", 2)]:
+    for part, P in [("1d", 4), ("2d", 2), ("3d", 2)]:
         A, B, A64, Bt64 = _make(prec, 4, 64, 64, 64, "ref_nk", "row_mk", integer=True, seed=num_iter)
         C = api.gemm_batched(A, B, variant="mma_sync", partition=part, P=P, num_iter=num_iter)
         assert np.array_equal(C.double().cpu().numpy() / num_iter, _ref(A64, Bt64)), part

@@ -52,6 +52,8 @@ def test_tc05_1d_exact(cuda, prec, M, N, K):
 def test_tc05_partitions_exact(cuda, part, P, M, N, K):
     if part == "3d" and (K + 15) // 16 < P:
         pytest.skip("fewer k-steps than depth ranks")
+    if part == "3d" and P * ((N + 15) // 16 * 16) > 512:
+        pytest.skip("P accumulators of N columns exceed the 512 TMEM columns")
     A, B, A64, B64 = _inputs("f16", 5, M, N, K, integer=True, seed=P)
     C = api.gemm_batched(A, B, variant="tcgen05", partition=part, P=P)
     torch.cuda.synchronize()
