@@ -88,6 +88,13 @@ int kami_version(void);
  * with the device. */
 int kami_device_status(int *code);
 
+/* Failure-detection self test (no counterpart in the reference): launch a
+ * one-thread kernel that waits, with the library's bounded wait, on an
+ * mbarrier that nothing arrives at.  The wait gives up after timeout_ns
+ * (<= 10 s) and records a timeout, which the next kami_device_status call
+ * reports as KAMI_ERR_TIMEOUT (code 4); the context stays usable. */
+int kami_selftest_bounded_wait(uint64_t timeout_ns, void *stream);
+
 /* ------------------------------------------------------------------------ */
 /* Batched block GEMM                                                       */
 /* ------------------------------------------------------------------------ */

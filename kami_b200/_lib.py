@@ -34,6 +34,7 @@ SIGNATURES = {
     "kami_last_error_string": ([], ctypes.c_char_p),
     "kami_version": ([], _i),
     "kami_device_status": ([ctypes.POINTER(_i)], _i),
+    "kami_selftest_bounded_wait": ([ctypes.c_uint64, _vp], _i),
     "kami_gemm_batched": ([_i, _i, _i, _i, _i, _i, _i, _i, _i, _i64,
                            _vp, _i64, _i64, _i,
                            _vp, _i64, _i64, _i,

@@ -1,0 +1,53 @@
+"""Differentiable batched block GEMM: a torch.autograd.Function whose forward
+and backward both run the library's partitioned block-GEMM kernels through
+the C ABI (no torch matmul on the path).
+
+    C  = A @ B            A: [batch, M, K], B: [batch, K, N]   (torch.bmm)
+    dA = dC @ B^T         B [K, N] row-major is the reference's N x K operand
+                          of this product (b_layout="ref_nk")
+    dB = A^T @ dC         A read transposed (a_layout="col_mk"), dC as the
+                          K x N operand (b_layout="row_kn")
+
+All three products accumulate in FP32 (FP16/BF16 inputs) or FP64 and are
+returned in the input dtype, as torch.bmm does.
+"""
+from __future__ import annotations
+
+import torch
+
+from . import api
+
+
+def _out_dtype(dt):
+    return dt if dt in (torch.float16, torch.bfloat16, torch.float64) else None
+
+
+class KamiBmm(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, A: torch.Tensor, B: torch.Tensor, partition: str = "auto", variant: str = "auto"):
+        if A.dtype != B.dtype or A.dtype not in (torch.float16, torch.bfloat16, torch.float64):
+            raise TypeError("KamiBmm takes two float16, bfloat16 or float64 tensors of the same dtype")
+        A = A.contiguous()
+        B = B.contiguous()
+        ctx.save_for_backward(A, B)
+        ctx.partition, ctx.variant = partition, variant
+        return api.gemm_batched(A, B, b_layout="row_kn", partition=partition, variant=variant,
+                                out_dtype=_out_dtype(A.dtype))
+
+    @staticmethod
+    def backward(ctx, dC: torch.Tensor):
+        A, B = ctx.saved_tensors
+        dC = dC.contiguous()
+        dA = dB = None
+        if ctx.needs_input_grad[0]:
+            dA = api.gemm_batched(dC, B, b_layout="ref_nk", partition=ctx.partition, variant=ctx.variant,
+                                  out_dtype=_out_dtype(A.dtype))
+        if ctx.needs_input_grad[1]:
+            dB = api.gemm_batched(A, dC, a_layout="col_mk", b_layout="row_kn", partition=ctx.partition,
+                                  variant=ctx.variant, out_dtype=_out_dtype(B.dtype))
+        return dA, dB, None, None
+
+
+def bmm(A: torch.Tensor, B: torch.Tensor, partition: str = "auto", variant: str = "auto") -> torch.Tensor:
+    """torch.bmm semantics, computed by the KAMI block-GEMM kernels."""
+    return KamiBmm.apply(A, B, partition, variant)

@@ -226,6 +226,13 @@ const char *kami_last_error_string(void) { return g_err; }
 
 int kami_version(void) { return 100; }
 
+int kami_selftest_bounded_wait(uint64_t timeout_ns, void *stream)
+{
+    if (timeout_ns > 10000000000ull)
+        return fail(KAMI_ERR_INVALID_VALUE, "self-test timeout above 10 s");
+    return tc05_selftest_bounded_wait(timeout_ns, reinterpret_cast<cudaStream_t>(stream));
+}
+
 int kami_device_status(int *code)
 {
     if (!code)

@@ -42,6 +42,7 @@ struct Tc05Params
     int nkb;            // 64-element K boxes
     int ksteps;         // 16-element MMA k-steps
     int part, P;
+    int a_mn, b_mn;     // operand stored MN-major (A as K x M, B as K x N)
     uint32_t idesc;     // instruction descriptor (N = bn, or bn / P for 2D)
     uint32_t tmem_cols; // allocated TMEM columns (power of two >= 32)
     uint64_t timeout_ns;
@@ -92,8 +93,16 @@ __global__ void __launch_bounds__(128) tc05_block_kernel(const __grid_constant__
         tc::mbar_expect_tx(&bars[0], bytes);
         for (int kb = 0; kb < p.nkb; ++kb)
         {
-            tc::tma_load_3d(sA + kb * a_box, &tmA, &bars[0], kb * 64, 0, prob);
-            tc::tma_load_3d(sB + kb * b_box, &tmB, &bars[0], kb * 64, 0, prob);
+            if (p.a_mn)
+                for (int mc = 0; mc < p.bm / 64; ++mc)
+                    tc::tma_load_3d(sA + kb * a_box + mc * 8192, &tmA, &bars[0], mc * 64, kb * 64, prob);
+            else
+                tc::tma_load_3d(sA + kb * a_box, &tmA, &bars[0], kb * 64, 0, prob);
+            if (p.b_mn)
+                for (int nc = 0; nc < p.bn / 64; ++nc)
+                    tc::tma_load_3d(sB + kb * b_box + nc * 8192, &tmB, &bars[0], nc * 64, kb * 64, prob);
+            else
+                tc::tma_load_3d(sB + kb * b_box, &tmB, &bars[0], kb * 64, 0, prob);
         }
         if (!tc::mbar_wait_bounded(&bars[0], 0, p.timeout_ns))
         {
@@ -118,11 +127,14 @@ __global__ void __launch_bounds__(128) tc05_block_kernel(const __grid_constant__
                     for (int ks = k_lo; ks < k_hi; ++ks)
                     {
                         const int kb = ks >> 2, kin = ks & 3;
-                        const uint64_t adesc = tc::desc_kmajor_sw128(a0 + kb * a_box + kin * 32);
+                        const uint64_t adesc = p.a_mn ? tc::desc_mnmajor_sw128(a0 + kb * a_box + kin * 2048, 8192)
+                                                      : tc::desc_kmajor_sw128(a0 + kb * a_box + kin * 32);
                         const uint32_t acc = (it > 0 || ks > k_lo) ? 1u : 0u;
                         for (int q = 0; q < panels; ++q)
                         {
-                            const uint64_t bdesc = tc::desc_kmajor_sw128(b0 + kb * b_box + q * pn * 128 + kin * 32);
+                            const uint64_t bdesc =
+                                p.b_mn ? tc::desc_mnmajor_sw128(b0 + kb * b_box + (q * pn / 64) * 8192 + kin * 2048, 8192)
+                                       : tc::desc_kmajor_sw128(b0 + kb * b_box + q * pn * 128 + kin * 32);
                             tc::mma_f16_ss(tmem + acc_col + q * pn, adesc, bdesc, p.idesc, acc);
                         }
                     }
@@ -218,10 +230,29 @@ static EncodeTiledFn encode_fn()
 }
 
 // 3D map {K, rows, batch} over a K-major operand, box {64, box_rows, 1},
-// 128-byte swizzle, zero fill out of bounds.
+// 128-byte swizzle, zero fill out of bounds.  With mn_major the operand is
+// stored K x rows (rows contiguous): map {rows, K, batch}, box {64, 64, 1}.
 static int make_map(CUtensorMap *map, bool bf16, const void *base, int K, int rows, int64_t batch, int64_t ld,
-                    int64_t stride, int box_rows)
+                    int64_t stride, int box_rows, bool mn_major = false)
 {
+    if (mn_major)
+    {
+        EncodeTiledFn fn = encode_fn();
+        if (!fn)
+            return fail(KAMI_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
+        cuuint64_t dims[3] = {(cuuint64_t)rows, (cuuint64_t)K, (cuuint64_t)batch};
+        const int64_t s2 = batch > 1 ? stride : (int64_t)K * ld;
+        cuuint64_t strides[2] = {(cuuint64_t)(ld * 2), (cuuint64_t)(s2 * 2)};
+        cuuint32_t box[3] = {64, 64, 1};
+        cuuint32_t estr[3] = {1, 1, 1};
+        CUresult r = fn(map, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3,
+                        const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS)
+            return fail(KAMI_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled failed (%d) for an MN-major operand", (int)r);
+        return KAMI_OK;
+    }
     EncodeTiledFn fn = encode_fn();
     if (!fn)
         return fail(KAMI_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
@@ -242,7 +273,7 @@ static int make_map(CUtensorMap *map, bool bf16, const void *base, int K, int ro
 
 struct Tc05Shape
 {
-    int bm, bn, nkb, ksteps, part, P;
+    int bm, bn, nkb, ksteps, part, P, a_mn, b_mn;
     uint32_t tmem_cols;
     size_t smem;
 };
@@ -256,8 +287,7 @@ static int tc05_shape(int in_type, int out_type, int partition, int P, int M, in
         return fail(KAMI_ERR_UNSUPPORTED, "tcgen05 variant: FP16/BF16 inputs only");
     if (out_type != KAMI_F32 && out_type != KAMI_F16 && out_type != KAMI_BF16)
         return fail(KAMI_ERR_UNSUPPORTED, "tcgen05 variant: FP32/FP16/BF16 output only");
-    if (a_layout != KAMI_A_ROW_MK || b_layout != KAMI_B_REF_NK)
-        return fail(KAMI_ERR_UNSUPPORTED, "tcgen05 variant: K-major A (row_mk) and B (ref_nk) only");
+    const int a_mn = a_layout == KAMI_A_COL_MK ? 1 : 0, b_mn = b_layout == KAMI_B_ROW_KN ? 1 : 0;
     if (M > 128 || N > 256 || K > 256)
         return fail(KAMI_ERR_UNSUPPORTED, "tcgen05 variant: M <= 128, N <= 256, K <= 256 (got %d, %d, %d)", M, N, K);
     if (K % 8)
@@ -271,6 +301,13 @@ static int tc05_shape(int in_type, int out_type, int partition, int P, int M, in
     int bn = (N + ngran - 1) / ngran * ngran;
     if (part == KAMI_PARTITION_2D)
         bn = (N + ngran * p - 1) / (ngran * p) * (ngran * p);
+    if (b_mn)
+    {
+        // MN-major B is staged in 64-column swizzle boxes; 2D panels must be whole boxes
+        bn = (N + 63) / 64 * 64;
+        if (part == KAMI_PARTITION_2D && (bn / p) % 64)
+            return fail(KAMI_ERR_UNSUPPORTED, "tcgen05 variant: 2D panels of an N-major B must be multiples of 64");
+    }
     if (bn > 256)
         return fail(KAMI_ERR_UNSUPPORTED, "tcgen05 variant: padded N %d exceeds 256", bn);
     const int ksteps = (K + 15) / 16;
@@ -289,6 +326,8 @@ static int tc05_shape(int in_type, int out_type, int partition, int P, int M, in
     s->ksteps = ksteps;
     s->part = part;
     s->P = p;
+    s->a_mn = a_mn;
+    s->b_mn = b_mn;
     s->tmem_cols = tc;
     s->smem = smem_bytes(bm, bn, nkb);
     if (s->smem > 227 * 1024)
@@ -300,8 +339,10 @@ bool tc05_prefer(int in_type, int partition, int M, int N, int K, int a_layout, 
 {
     // the tensor-memory path wins where one MMA tile holds the problem
     // densely; tiny problems stay on mma.sync (see the variant sweep)
-    return (in_type == KAMI_F16 || in_type == KAMI_BF16) && a_layout == KAMI_A_ROW_MK &&
-           b_layout == KAMI_B_REF_NK && M > 32 && M <= 128 && N <= 256 && N >= 32 && K <= 256 && K % 8 == 0;
+    (void)a_layout;
+    (void)b_layout;
+    return (in_type == KAMI_F16 || in_type == KAMI_BF16) && M > 32 && M <= 128 && N <= 256 && N >= 32 && K <= 256 &&
+           K % 8 == 0;
 }
 
 int tc05_plan(int in_type, int out_type, int partition, int P, int M, int N, int K, int64_t batch, int a_layout,
@@ -334,10 +375,10 @@ int tc05_launch(const GemmArgs &g, int in_type, int partition, int P, void *, si
     if (g.batch > 0x7fffffff)
         return fail(KAMI_ERR_UNSUPPORTED, "tcgen05 variant: batch above 2^31-1");
     CUtensorMap ma, mb;
-    st = make_map(&ma, bf16, g.A, g.K, g.M, g.batch, g.lda, g.sA, s.bm);
+    st = make_map(&ma, bf16, g.A, g.K, g.M, g.batch, g.lda, g.sA, s.bm, s.a_mn != 0);
     if (st)
         return st;
-    st = make_map(&mb, bf16, g.B, g.K, g.N, g.batch, g.ldb, g.sB, s.bn);
+    st = make_map(&mb, bf16, g.B, g.K, g.N, g.batch, g.ldb, g.sB, s.bn, s.b_mn != 0);
     if (st)
         return st;
     Tc05Params p{};
@@ -348,7 +389,9 @@ int tc05_launch(const GemmArgs &g, int in_type, int partition, int P, void *, si
     p.ksteps = s.ksteps;
     p.part = s.part;
     p.P = s.P;
-    p.idesc = tc::idesc_f16(bf16, s.bm, s.part == KAMI_PARTITION_2D ? s.bn / s.P : s.bn);
+    p.a_mn = s.a_mn;
+    p.b_mn = s.b_mn;
+    p.idesc = tc::idesc_f16(bf16, s.bm, s.part == KAMI_PARTITION_2D ? s.bn / s.P : s.bn, s.a_mn, s.b_mn);
     p.tmem_cols = s.tmem_cols;
     const double mmas = (double)g.num_iter * s.ksteps * (s.part == KAMI_PARTITION_2D ? s.P : 1);
     p.timeout_ns = (uint64_t)(5e8 + mmas * 2000.0);
@@ -365,6 +408,27 @@ int tc05_launch(const GemmArgs &g, int in_type, int partition, int P, void *, si
     e = cudaLaunchKernel(fn, dim3((unsigned)g.batch), dim3(128), args, s.smem, stream);
     if (e != cudaSuccess)
         return cuda_fail(e, "cudaLaunchKernel(tc05_block_kernel)");
+    return KAMI_OK;
+}
+
+// Failure-detection self test: one thread waits on an mbarrier that nothing
+// arrives at, with the same bounded wait the GEMM kernels use, and records
+// code 4 in the status word when the wait gives up.
+__global__ void bounded_wait_selftest_kernel(uint64_t limit_ns)
+{
+    __shared__ uint64_t bar;
+    tc::mbar_init(&bar, 1);
+    tc::fence_mbar_init();
+    if (!tc::mbar_wait_bounded(&bar, 0, limit_ns))
+        tc05_flag(4);
+}
+
+int tc05_selftest_bounded_wait(uint64_t limit_ns, cudaStream_t s)
+{
+    bounded_wait_selftest_kernel<<<1, 1, 0, s>>>(limit_ns);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return cuda_fail(e, "bounded_wait_selftest_kernel");
     return KAMI_OK;
 }
 

@@ -25,4 +25,7 @@ int tc05_launch(const GemmArgs &g, int in_type, int partition, int P, void *work
 // 1 = operand loads timed out, 2 = MMA completion timed out).  Synchronous.
 int tc05_read_error(int *flag);
 
+// Launch a one-thread kernel whose bounded wait must time out (status 4).
+int tc05_selftest_bounded_wait(uint64_t limit_ns, cudaStream_t s);
+
 } // namespace kami

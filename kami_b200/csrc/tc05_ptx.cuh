@@ -158,13 +158,31 @@ __device__ __forceinline__ uint64_t desc_kmajor_sw128(uint32_t addr)
     return d;
 }
 
-// Instruction descriptor of tcgen05.mma kind::f16: FP32 accumulator,
-// A and B K-major, given M (64 or 128) and N (multiple of 8 / 16, <= 256).
-__host__ __device__ constexpr uint32_t idesc_f16(bool bf16, int M, int N)
+// Descriptor of an MN-major operand written by TMA with 128-byte swizzling
+// in boxes of 64 MN-elements x 64 K-rows: each K-row is 128 bytes (64
+// consecutive M or N elements), 8-row groups 1024 bytes apart (SBO), and the
+// next 64-element MN chunk `lbo` bytes away (the next box).
+__device__ __forceinline__ uint64_t desc_mnmajor_sw128(uint32_t addr, uint32_t lbo)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((addr & 0x3FFFF) >> 4);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16; // LBO: next 64-element MN chunk
+    d |= (uint64_t)(1024 >> 4) << 32;          // SBO: next group of 8 K rows
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)2 << 61;
+    return d;
+}
+
+// Instruction descriptor of tcgen05.mma kind::f16: FP32 accumulator, given
+// M (64 or 128), N (multiple of 16, <= 256) and the operand majors
+// (0 = K-major, 1 = MN-major).
+__host__ __device__ constexpr uint32_t idesc_f16(bool bf16, int M, int N, int a_mn = 0, int b_mn = 0)
 {
     return (1u << 4)                         // D format F32
            | ((bf16 ? 1u : 0u) << 7)         // A format
            | ((bf16 ? 1u : 0u) << 10)        // B format
+           | ((uint32_t)(a_mn & 1) << 15)    // A major
+           | ((uint32_t)(b_mn & 1) << 16)    // B major
            | ((uint32_t)(N >> 3) << 17)      // N / 8
            | ((uint32_t)(M >> 4) << 24);     // M / 16
 }

@@ -112,3 +112,19 @@ def test_auto_picks_tcgen05_for_128(cuda):
     assert api.describe(128, 128, 128, 592)["variant"] == "tcgen05"
     A, B, A64, B64 = _inputs("f16", 8, 128, 128, 128, integer=True)
     assert np.array_equal(api.gemm_batched(A, B).double().cpu().numpy(), oracle.gemm(A64, B64))
+
+
+@pytest.mark.parametrize("a_layout,b_layout", [("col_mk", "ref_nk"), ("row_mk", "row_kn"), ("col_mk", "row_kn")])
+@pytest.mark.parametrize("M,N,K", [(128, 128, 128), (64, 64, 64), (100, 72, 40), (128, 256, 64), (64, 48, 136)])
+def test_tc05_mn_major_layouts(cuda, a_layout, b_layout, M, N, K):
+    """MN-major operands (A stored K x M, B stored K x N) staged by TMA in
+    64-element swizzle boxes: the layouts of the backward pass."""
+    rng = np.random.default_rng(M + 3 * N + 7 * K)
+    A64 = rng.integers(-2, 3, (5, M, K)).astype(np.float64)
+    B64 = rng.integers(-2, 3, (5, N, K)).astype(np.float64)
+    A = torch.tensor(A64 if a_layout == "row_mk" else A64.transpose(0, 2, 1).copy(), dtype=torch.float16).cuda()
+    B = torch.tensor(B64 if b_layout == "ref_nk" else B64.transpose(0, 2, 1).copy(), dtype=torch.float16).cuda()
+    C = api.gemm_batched(A, B, a_layout=a_layout, b_layout=b_layout, variant="tcgen05")
+    torch.cuda.synchronize()
+    _status_clean()
+    assert np.array_equal(C.double().cpu().numpy(), oracle.gemm(A64, B64))
