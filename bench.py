@@ -43,10 +43,14 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--size", type=int, default=128)
     ap.add_argument("--num-iter", type=int, default=1000)
-    ap.add_argument("--variant", default="auto", choices=["auto", "mma_sync", "tcgen05"])
+    ap.add_argument("--variant", default="auto", choices=["auto", "mma_sync", "tcgen05", "tcgen05_ts"])
     ap.add_argument("--partition", default="auto", choices=["auto", "1d", "2d", "3d"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="bounded CPU-baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="block",
+                    choices=["block", "block-sweep", "fp64", "split", "uneven", "spgemm", "bmm"],
+                    help="block (default, the headline line) or one of the other configurations; "
+                         "non-default workloads print one JSON line per measured case")
     return ap.parse_args()
 
 
@@ -297,8 +301,220 @@ def run_ours(args, rank, world):
     print(json.dumps(out), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# secondary workloads (one JSON line per case; the default run is `block`)
+# ---------------------------------------------------------------------------
+def _time_ms(fn, warmup, steps, flush=None):
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(steps):
+        if flush is not None:
+            flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        ts.append((e0, e1))
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in ts]
+
+
+def _emit(d):
+    print(json.dumps(d), flush=True)
+
+
+def run_secondary(args):
+    import numpy as np
+    import torch
+
+    import oracle
+    from kami_b200 import api
+    from kami_b200.autograd import bmm
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    peak_tf, peak_bw, src = measured_peaks()
+    W, K_ = max(args.warmup, 3), args.steps
+
+    if args.workload == "block-sweep":
+        cases = [(n, n, n) for n in (16, 32, 64, 128)] + [(128, 128, 8), (128, 128, 16), (128, 128, 32)]
+        for (M, N, K) in cases:
+            batch = 4 * sms
+            g = torch.Generator().manual_seed(0)
+            A = (torch.rand((batch, M, K), generator=g) * 2 - 1).half().to(dev)
+            B = (torch.rand((batch, N, K), generator=g) * 2 - 1).half().to(dev)
+            C = torch.empty((batch, M, N), dtype=torch.float32, device=dev)
+            for variant in ("mma_sync", "tcgen05", "tcgen05_ts"):
+                for part in ("1d", "2d", "3d"):
+                    for it in (1000, 1):
+                        try:
+                            plan = api.describe(M, N, K, batch, variant=variant, partition=part)
+                        except Exception as e:  # no kernel for this combination
+                            _emit({"workload": "block-sweep", "M": M, "N": N, "K": K, "variant": variant,
+                                   "partition": part, "unavailable": str(e)[:120]})
+                            continue
+                        ms = _time_ms(lambda: api.gemm_batched(A, B, C, variant=variant, partition=part,
+                                                               num_iter=it), W, K_, flush)
+                        t = min(ms)
+                        fl = 2.0 * M * N * K * batch * it
+                        by = batch * (M * K * 2 + N * K * 2 + M * N * 4)
+                        _emit({"workload": "block-sweep", "M": M, "N": N, "K": K, "batch": batch, "num_iter": it,
+                               "variant": plan["variant"], "partition": plan["partition"], "P": plan["P"],
+                               "threads": plan["threads"], "ms": t, "tflops": fl / t / 1e9,
+                               "frac_tensor_peak": fl / t / 1e9 / peak_tf,
+                               "hbm_gbs": by / t / 1e6, "frac_hbm": by / t / 1e6 / peak_bw})
+        return
+
+    if args.workload == "fp64":
+        # 1024 independent 32^3 FP64 problems, uniform[-1, 1], seed 0; streamed (NUM_ITER 1) and repeat
+        rng = np.random.default_rng(0)
+        for (n, batch) in [(32, 1024), (64, 8192), (32, 65536)]:
+            A64 = rng.uniform(-1, 1, (batch, n, n))
+            B64 = rng.uniform(-1, 1, (batch, n, n))
+            A = torch.tensor(A64, device=dev)
+            B = torch.tensor(B64, device=dev)
+            C = torch.empty((batch, n, n), dtype=torch.float64, device=dev)
+            ref = oracle.gemm(A64[:64], B64[:64])
+            for part in ("1d", "2d", "3d"):
+                for it in (1, 100):
+                    try:
+                        plan = api.describe(n, n, n, batch, torch.float64, partition=part)
+                    except Exception as e:
+                        _emit({"workload": "fp64", "n": n, "partition": part, "unavailable": str(e)[:100]})
+                        continue
+                    ms = _time_ms(lambda: api.gemm_batched(A, B, C, partition=part, num_iter=it), W, K_, flush)
+                    err = float(np.max(np.abs(C[:64].cpu().numpy() / it - ref)))
+                    t = min(ms)
+                    fl = 2.0 * n ** 3 * batch * it
+                    by = batch * 3 * n * n * 8
+                    _emit({"workload": "fp64", "n": n, "batch": batch, "num_iter": it, "partition": part,
+                           "P": plan["P"], "ms": t, "tflops": fl / t / 1e9, "hbm_gbs": by / t / 1e6,
+                           "frac_hbm": by / t / 1e6 / peak_bw, "max_abs_err_vs_oracle": err})
+        return
+
+    if args.workload == "split":
+        # batch 8192 of 64^3, entries sign * 10^u, u ~ U[-3, 3]
+        rng = np.random.default_rng(0)
+        batch, n = 8192, 64
+        A64 = rng.choice([-1.0, 1.0], (batch, n, n)) * 10.0 ** rng.uniform(-3, 3, (batch, n, n))
+        B64 = rng.choice([-1.0, 1.0], (batch, n, n)) * 10.0 ** rng.uniform(-3, 3, (batch, n, n))
+        A = torch.tensor(A64, device=dev)
+        B = torch.tensor(B64, device=dev)
+        C = torch.empty((batch, n, n), dtype=torch.float64, device=dev)
+        sub = 256
+        hi, lo = oracle.gemm_dd(A64[:sub], B64[:sub])
+        fl1 = 2.0 * n ** 3 * batch
+        by = batch * 3 * n * n * 8
+        for it in (1, 20):
+            ms = _time_ms(lambda: api.gemm_batched(A, B, C, num_iter=it), W, K_, flush)
+            e_nat = oracle.normwise_error_dd(C[:sub].cpu().numpy() / it, hi, lo)
+            t = min(ms)
+            _emit({"workload": "split", "kernel": "native-fp64 (DMMA mma.sync)", "num_iter": it, "ms": t,
+                   "tflops_fp64_equiv": fl1 * it / t / 1e9, "hbm_gbs": by / t / 1e6, "normwise_err_dd": e_nat})
+            for s_, sdt in [(3, torch.float16), (4, torch.float16), (5, torch.float16), (6, torch.float16),
+                            (7, torch.float16), (8, torch.bfloat16)]:
+                ms = _time_ms(lambda: api.split_f64_gemm(A, B, C, nslices=s_, slice_dtype=sdt, num_iter=it),
+                              W, K_, flush)
+                e = oracle.normwise_error_dd(C[:sub].cpu().numpy() / it, hi, lo) if it == 1 else None
+                t = min(ms)
+                _emit({"workload": "split", "kernel": f"split {s_} x {'bf16' if sdt == torch.bfloat16 else 'fp16'}",
+                       "num_iter": it, "ms": t, "tflops_fp64_equiv": fl1 * it / t / 1e9,
+                       "hbm_gbs": by / t / 1e6, "normwise_err_dd": e})
+        return
+
+    if args.workload == "uneven":
+        rng = np.random.default_rng(0)
+        count = 20000
+        x = np.exp(rng.uniform(np.log(8), np.log(128), (count, 3)))
+        shapes = np.clip(8 * np.round(x / 8), 8, 128).astype(np.int64)
+        for dt in (torch.float16, torch.float64):
+            for tune in (False, True):
+                plan = api.GroupedPlan(shapes, dt, autotune=tune)
+                info = plan.info()
+                A = torch.rand(plan.sizes[0], device=dev).to(dt)
+                B = torch.rand(plan.sizes[1], device=dev).to(dt)
+                C = torch.empty(plan.sizes[2], dtype=plan.out_dtype, device=dev)
+                plan.run(A, B, C)
+                torch.cuda.synchronize()
+                gph = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(gph):
+                    plan.run(A, B, C)
+                ms = _time_ms(gph.replay, W, K_, flush)
+                t = min(ms)
+                _emit({"workload": "uneven", "dtype": str(dt).replace("torch.", ""), "autotune": tune,
+                       "problems": count, "launches_per_step": 1, "cuda_graph": True, "ms": t,
+                       "tflops": info["flops"] / t / 1e9, "hbm_gbs": info["bytes"] / t / 1e6,
+                       "frac_hbm": info["bytes"] / t / 1e6 / peak_bw, "ctas": info["ctas"],
+                       "partitions": info["partitions"], "flops": info["flops"], "bytes": info["bytes"]})
+                del gph
+        return
+
+    if args.workload == "spgemm":
+        nb = 1024  # n = 16384 with 16 x 16 blocks
+        res = []
+        for seed_a, seed_b in [(1, 2)]:
+            rpa, cia = oracle.bsr_pattern(nb, nb, 0.01, seed_a)
+            rpb, cib = oracle.bsr_pattern(nb, nb, 0.01, seed_b)
+            rng = np.random.default_rng(0)
+            va = torch.tensor(rng.uniform(-1, 1, (len(cia), 16, 16)), dtype=torch.float16, device=dev)
+            vb = torch.tensor(rng.uniform(-1, 1, (len(cib), 16, 16)), dtype=torch.float16, device=dev)
+            A = api.BSR(torch.tensor(rpa, device=dev), torch.tensor(cia, device=dev), va, nb)
+            B = api.BSR(torch.tensor(rpb, device=dev), torch.tensor(cib, device=dev), vb, nb)
+            nnzcub = oracle.spgemm_nnzcub(cia, rpb)
+            rpc, nnzc = api.spgemm_symbolic(A, B)
+            cic = api.spgemm_fill_colidx(A, B, rpc, nnzc)
+            vc = torch.empty((nnzc, 16, 16), dtype=torch.float32, device=dev)
+
+            def symbolic():
+                r, _ = api.spgemm_symbolic(A, B)
+                api.spgemm_fill_colidx(A, B, r, nnzc)
+
+            ms_sym = _time_ms(symbolic, W, K_, flush)
+            ms_num = _time_ms(lambda: api.spgemm_numeric(A, B, rpc, cic, C_values=vc), W, K_, flush)
+            fl = 2.0 * 16 ** 3 * nnzcub
+            by = (len(cia) + len(cib)) * 512 + nnzc * 1024 + nnzc * 4 + (len(cia) + len(cib)) * 4
+            t = min(ms_num)
+            # check a sample of rows against the CPU oracle
+            _emit({"workload": "spgemm", "n": nb * 16, "block": 16, "density": 0.01, "nnzA": len(cia),
+                   "nnzB": len(cib), "nnzC": nnzc, "nnzCub": nnzcub, "numeric_ms": t,
+                   "symbolic_ms": min(ms_sym), "tflops_numeric": fl / t / 1e9,
+                   "hbm_gbs_numeric": by / t / 1e6, "frac_hbm": by / t / 1e6 / peak_bw,
+                   "tflops_end_to_end": fl / (t + min(ms_sym)) / 1e9})
+        return
+
+    if args.workload == "bmm":
+        batch, n = 4096, 64
+        g = torch.Generator().manual_seed(0)
+        A = (torch.rand((batch, n, n), generator=g) * 2 - 1).bfloat16().to(dev).requires_grad_()
+        B = (torch.rand((batch, n, n), generator=g) * 2 - 1).bfloat16().to(dev).requires_grad_()
+        G = (torch.rand((batch, n, n), generator=g) * 2 - 1).bfloat16().to(dev)
+
+        def step():
+            A.grad = None
+            B.grad = None
+            C = bmm(A, B)
+            C.backward(G)
+
+        ms = _time_ms(step, W, K_, flush)
+        t = min(ms)
+        fl = 3 * 2.0 * n ** 3 * batch
+        by = batch * n * n * 2 * 9
+        _emit({"workload": "bmm", "dtype": "bf16", "batch": batch, "M": n, "N": n, "K": n, "ms_fwd_bwd": t,
+               "tflops": fl / t / 1e9, "hbm_gbs": by / t / 1e6, "frac_hbm": by / t / 1e6 / peak_bw})
+        return
+
+
 def main():
     args = parse()
+    if args.workload != "block":
+        run_secondary(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":

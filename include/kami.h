@@ -65,7 +65,8 @@ typedef enum kami_partition {
 typedef enum kami_variant {
     KAMI_VARIANT_AUTO = 0,
     KAMI_VARIANT_MMA_SYNC = 1, /* warp mma.sync, register-resident operands        */
-    KAMI_VARIANT_TCGEN05 = 2   /* tcgen05.mma, TMA-staged operands, TMEM accumulators */
+    KAMI_VARIANT_TCGEN05 = 2,  /* tcgen05.mma, TMA-staged operands, TMEM accumulators */
+    KAMI_VARIANT_TCGEN05_TS = 3 /* tcgen05.mma with A resident in tensor memory (M 65..128) */
 } kami_variant_t;
 
 typedef enum kami_a_layout { KAMI_A_ROW_MK = 0, KAMI_A_COL_MK = 1 } kami_a_layout_t;

@@ -18,7 +18,8 @@ from ._lib import check, load
 
 _DT = {torch.float16: _lib.F16, torch.bfloat16: _lib.BF16, torch.float64: _lib.F64, torch.float32: _lib.F32}
 _PART = {"auto": _lib.PARTITION_AUTO, "1d": _lib.PARTITION_1D, "2d": _lib.PARTITION_2D, "3d": _lib.PARTITION_3D}
-_VAR = {"auto": _lib.VARIANT_AUTO, "mma_sync": _lib.VARIANT_MMA_SYNC, "tcgen05": _lib.VARIANT_TCGEN05}
+_VAR = {"auto": _lib.VARIANT_AUTO, "mma_sync": _lib.VARIANT_MMA_SYNC, "tcgen05": _lib.VARIANT_TCGEN05,
+        "tcgen05_ts": _lib.VARIANT_TCGEN05_TS}
 _AL = {"row_mk": _lib.A_ROW_MK, "col_mk": _lib.A_COL_MK}
 _BL = {"ref_nk": _lib.B_REF_NK, "row_kn": _lib.B_ROW_KN}
 
@@ -99,7 +100,7 @@ def describe(M: int, N: int, K: int, batch: int, dtype=torch.float16, out_dtype=
                                     alloc_warps, batch, _AL[a_layout], _BL[b_layout], out))
     keys = ["variant", "partition", "P", "threads", "smem", "problems_per_cta", "grid"]
     d = dict(zip(keys, list(out)[:7]))
-    d["variant"] = {1: "mma_sync", 2: "tcgen05"}[d["variant"]]
+    d["variant"] = {1: "mma_sync", 2: "tcgen05", 3: "tcgen05_ts"}[d["variant"]]
     d["partition"] = {1: "1d", 2: "2d", 3: "3d"}[d["partition"]]
     return d
 

@@ -267,14 +267,16 @@ int kami_gemm_describe(kami_dtype_t in_type, kami_dtype_t out_type, kami_partiti
     if (st)
         return st;
     LaunchInfo info{};
-    if (variant == KAMI_VARIANT_TCGEN05 ||
+    if (variant == KAMI_VARIANT_TCGEN05 || variant == KAMI_VARIANT_TCGEN05_TS ||
         (variant == KAMI_VARIANT_AUTO && tc05_prefer(in_type, partition, M, N, K, a_layout, b_layout)))
     {
-        st = tc05_plan(in_type, out_type, partition, P, M, N, K, batch, a_layout, b_layout, &info);
-        if (st && variant == KAMI_VARIANT_TCGEN05)
+        const int ts = variant == KAMI_VARIANT_TCGEN05_TS ||
+                       (variant == KAMI_VARIANT_AUTO && tc05_prefer_ts(M, a_layout));
+        st = tc05_plan(in_type, out_type, partition, P, M, N, K, batch, a_layout, b_layout, &info, ts);
+        if (st && variant != KAMI_VARIANT_AUTO)
             return st;
     }
-    if (info.variant != KAMI_VARIANT_TCGEN05)
+    if (info.variant != KAMI_VARIANT_TCGEN05 && info.variant != KAMI_VARIANT_TCGEN05_TS)
     {
         const MmaInstance *inst = nullptr;
         st = plan_mma(in_type, partition, P, alloc_warps, M, N, K, batch, &inst, &info, false);
@@ -306,7 +308,8 @@ int kami_gemm_batched(kami_dtype_t in_type, kami_dtype_t out_type, kami_partitio
         return KAMI_OK;
     if (!A || !B || !C)
         return fail(KAMI_ERR_INVALID_VALUE, "A, B and C must be non-null device pointers");
-    if (variant != KAMI_VARIANT_AUTO && variant != KAMI_VARIANT_MMA_SYNC && variant != KAMI_VARIANT_TCGEN05)
+    if (variant != KAMI_VARIANT_AUTO && variant != KAMI_VARIANT_MMA_SYNC && variant != KAMI_VARIANT_TCGEN05 &&
+        variant != KAMI_VARIANT_TCGEN05_TS)
         return fail(KAMI_ERR_INVALID_VALUE, "bad variant %d", variant);
     if (partition < KAMI_PARTITION_AUTO || partition > KAMI_PARTITION_3D)
         return fail(KAMI_ERR_INVALID_VALUE, "bad partition %d", partition);
@@ -352,11 +355,13 @@ int kami_gemm_batched(kami_dtype_t in_type, kami_dtype_t out_type, kami_partitio
     g.num_iter = num_iter;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
 
-    if (variant == KAMI_VARIANT_TCGEN05 ||
+    if (variant == KAMI_VARIANT_TCGEN05 || variant == KAMI_VARIANT_TCGEN05_TS ||
         (variant == KAMI_VARIANT_AUTO && tc05_prefer(in_type, partition, M, N, K, a_layout, b_layout)))
     {
-        st = tc05_launch(g, in_type, partition, P, workspace, ws_bytes, s);
-        if (st == KAMI_OK || variant == KAMI_VARIANT_TCGEN05)
+        const int ts = variant == KAMI_VARIANT_TCGEN05_TS ||
+                       (variant == KAMI_VARIANT_AUTO && tc05_prefer_ts(M, a_layout));
+        st = tc05_launch(g, in_type, partition, P, workspace, ws_bytes, s, ts);
+        if (st == KAMI_OK || variant != KAMI_VARIANT_AUTO)
             return st;
     }
 

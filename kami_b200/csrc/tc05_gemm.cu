@@ -43,6 +43,8 @@ struct Tc05Params
     int ksteps;         // 16-element MMA k-steps
     int part, P;
     int a_mn, b_mn;     // operand stored MN-major (A as K x M, B as K x N)
+    int a_tmem;         // A resident in tensor memory (TS form) instead of shared memory
+    uint32_t a_col;     // first TMEM column of A in the TS form
     uint32_t idesc;     // instruction descriptor (N = bn, or bn / P for 2D)
     uint32_t tmem_cols; // allocated TMEM columns (power of two >= 32)
     uint64_t timeout_ns;
@@ -58,7 +60,7 @@ __global__ void __launch_bounds__(128) tc05_block_kernel(const __grid_constant__
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     // 1024-byte alignment of the swizzle atoms
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    const int a_box = p.bm * 128, b_box = p.bn * 128;
+    const int a_box = p.a_tmem ? 0 : p.bm * 128, b_box = p.bn * 128;
     uint8_t *sA = smem;
     uint8_t *sB = sA + p.nkb * a_box;
     uint64_t *bars = reinterpret_cast<uint64_t *>(sB + p.nkb * b_box); // [0] loads landed, [1] MMAs done
@@ -89,21 +91,57 @@ __global__ void __launch_bounds__(128) tc05_block_kernel(const __grid_constant__
 
     if (threadIdx.x == 0)
     {
-        const uint32_t bytes = (uint32_t)(p.nkb * (a_box + b_box));
+        const uint32_t bytes = (uint32_t)(p.nkb * (a_box + b_box)); // a_box is 0 when A lives in TMEM
         tc::mbar_expect_tx(&bars[0], bytes);
         for (int kb = 0; kb < p.nkb; ++kb)
         {
-            if (p.a_mn)
-                for (int mc = 0; mc < p.bm / 64; ++mc)
-                    tc::tma_load_3d(sA + kb * a_box + mc * 8192, &tmA, &bars[0], mc * 64, kb * 64, prob);
-            else
-                tc::tma_load_3d(sA + kb * a_box, &tmA, &bars[0], kb * 64, 0, prob);
+            if (!p.a_tmem)
+            {
+                if (p.a_mn)
+                    for (int mc = 0; mc < p.bm / 64; ++mc)
+                        tc::tma_load_3d(sA + kb * a_box + mc * 8192, &tmA, &bars[0], mc * 64, kb * 64, prob);
+                else
+                    tc::tma_load_3d(sA + kb * a_box, &tmA, &bars[0], kb * 64, 0, prob);
+            }
             if (p.b_mn)
                 for (int nc = 0; nc < p.bn / 64; ++nc)
                     tc::tma_load_3d(sB + kb * b_box + nc * 8192, &tmB, &bars[0], nc * 64, kb * 64, prob);
             else
                 tc::tma_load_3d(sB + kb * b_box, &tmB, &bars[0], kb * 64, 0, prob);
         }
+    }
+    __syncwarp(); // tcgen05.st below is .sync.aligned
+    if (p.a_tmem)
+    {
+        // A -> TMEM: warp w writes lanes 32w..32w+31, thread t holds row 32w+t,
+        // 16 columns (32 K elements) per tcgen05.st; zero beyond M and K
+        const int row = warp * 32 + lane;
+        const uint16_t *arow = reinterpret_cast<const uint16_t *>(g.A) + (int64_t)prob * g.sA + (int64_t)row * g.lda;
+        const int ncols = ((p.ksteps * 8) + 15) / 16 * 16;
+        for (int c0 = 0; c0 < ncols; c0 += 16)
+        {
+            uint32_t v[16];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+            {
+                const int k = c0 * 2 + q * 8;
+                uint4 x = make_uint4(0, 0, 0, 0);
+                if (row < g.M && k < g.K)
+                    x = __ldg(reinterpret_cast<const uint4 *>(arow + k));
+                v[4 * q + 0] = x.x;
+                v[4 * q + 1] = x.y;
+                v[4 * q + 2] = x.z;
+                v[4 * q + 3] = x.w;
+            }
+            tc::tmem_st16(tmem + ((uint32_t)(warp * 32) << 16) + p.a_col + c0, v);
+        }
+        tc::tmem_st_wait();
+        tc::tc_fence_before();
+        __syncthreads();
+        tc::tc_fence_after();
+    }
+    if (threadIdx.x == 0)
+    {
         if (!tc::mbar_wait_bounded(&bars[0], 0, p.timeout_ns))
         {
             tc05_flag(1);
@@ -130,12 +168,16 @@ __global__ void __launch_bounds__(128) tc05_block_kernel(const __grid_constant__
                         const uint64_t adesc = p.a_mn ? tc::desc_mnmajor_sw128(a0 + kb * a_box + kin * 2048, 8192)
                                                       : tc::desc_kmajor_sw128(a0 + kb * a_box + kin * 32);
                         const uint32_t acc = (it > 0 || ks > k_lo) ? 1u : 0u;
+                        const uint32_t a_tm = tmem + p.a_col + (uint32_t)ks * 8;
                         for (int q = 0; q < panels; ++q)
                         {
                             const uint64_t bdesc =
                                 p.b_mn ? tc::desc_mnmajor_sw128(b0 + kb * b_box + (q * pn / 64) * 8192 + kin * 2048, 8192)
                                        : tc::desc_kmajor_sw128(b0 + kb * b_box + q * pn * 128 + kin * 32);
-                            tc::mma_f16_ss(tmem + acc_col + q * pn, adesc, bdesc, p.idesc, acc);
+                            if (p.a_tmem)
+                                tc::mma_f16_ts(tmem + acc_col + q * pn, a_tm, bdesc, p.idesc, acc);
+                            else
+                                tc::mma_f16_ss(tmem + acc_col + q * pn, adesc, bdesc, p.idesc, acc);
                         }
                     }
                 }
@@ -273,7 +315,8 @@ static int make_map(CUtensorMap *map, bool bf16, const void *base, int K, int ro
 
 struct Tc05Shape
 {
-    int bm, bn, nkb, ksteps, part, P, a_mn, b_mn;
+    int bm, bn, nkb, ksteps, part, P, a_mn, b_mn, a_tmem;
+    uint32_t a_col;
     uint32_t tmem_cols;
     size_t smem;
 };
@@ -281,7 +324,7 @@ struct Tc05Shape
 static size_t smem_bytes(int bm, int bn, int nkb) { return (size_t)nkb * (bm + bn) * 128 + 1024 + 64; }
 
 static int tc05_shape(int in_type, int out_type, int partition, int P, int M, int N, int K, int a_layout,
-                      int b_layout, Tc05Shape *s)
+                      int b_layout, Tc05Shape *s, int a_tmem = 0)
 {
     if (in_type != KAMI_F16 && in_type != KAMI_BF16)
         return fail(KAMI_ERR_UNSUPPORTED, "tcgen05 variant: FP16/BF16 inputs only");
@@ -313,9 +356,17 @@ static int tc05_shape(int in_type, int out_type, int partition, int P, int M, in
     const int ksteps = (K + 15) / 16;
     if (part == KAMI_PARTITION_3D && ksteps < p)
         return fail(KAMI_ERR_UNSUPPORTED, "tcgen05 variant: 3D needs at least P k-steps of 16");
-    const int cols = (part == KAMI_PARTITION_3D ? p : 1) * bn;
+    const int acc_cols = (part == KAMI_PARTITION_3D ? p : 1) * bn;
+    int cols = acc_cols;
+    if (a_tmem)
+    {
+        if (bm != 128 || a_mn)
+            return fail(KAMI_ERR_UNSUPPORTED,
+                        "tcgen05 A-in-TMEM form: M must be 65..128 and A row-major (M x K)");
+        cols += ((K + 15) / 16 * 8 + 15) / 16 * 16; // two K elements per 32-bit column
+    }
     if (cols > 512)
-        return fail(KAMI_ERR_UNSUPPORTED, "tcgen05 variant: %d accumulator columns exceed TMEM", cols);
+        return fail(KAMI_ERR_UNSUPPORTED, "tcgen05 variant: %d TMEM columns needed, 512 available", cols);
     uint32_t tc = 32;
     while ((int)tc < cols)
         tc <<= 1;
@@ -328,8 +379,10 @@ static int tc05_shape(int in_type, int out_type, int partition, int P, int M, in
     s->P = p;
     s->a_mn = a_mn;
     s->b_mn = b_mn;
+    s->a_tmem = a_tmem;
+    s->a_col = (uint32_t)acc_cols;
     s->tmem_cols = tc;
-    s->smem = smem_bytes(bm, bn, nkb);
+    s->smem = smem_bytes(a_tmem ? 0 : bm, bn, nkb);
     if (s->smem > 227 * 1024)
         return fail(KAMI_ERR_UNSUPPORTED, "tcgen05 variant: %zu bytes of shared memory", s->smem);
     return KAMI_OK;
@@ -345,14 +398,17 @@ bool tc05_prefer(int in_type, int partition, int M, int N, int K, int a_layout, 
            K % 8 == 0;
 }
 
+// AUTO keeps A in shared memory until the TS form is measured faster
+bool tc05_prefer_ts(int M, int a_layout) { return false && M > 64 && a_layout == KAMI_A_ROW_MK; }
+
 int tc05_plan(int in_type, int out_type, int partition, int P, int M, int N, int K, int64_t batch, int a_layout,
-              int b_layout, LaunchInfo *info)
+              int b_layout, LaunchInfo *info, int a_tmem)
 {
     Tc05Shape s;
-    int st = tc05_shape(in_type, out_type, partition, P, M, N, K, a_layout, b_layout, &s);
+    int st = tc05_shape(in_type, out_type, partition, P, M, N, K, a_layout, b_layout, &s, a_tmem);
     if (st)
         return st;
-    info->variant = KAMI_VARIANT_TCGEN05;
+    info->variant = a_tmem ? KAMI_VARIANT_TCGEN05_TS : KAMI_VARIANT_TCGEN05;
     info->partition = s.part;
     info->P = s.P;
     info->threads = 128;
@@ -362,10 +418,11 @@ int tc05_plan(int in_type, int out_type, int partition, int P, int M, int N, int
     return KAMI_OK;
 }
 
-int tc05_launch(const GemmArgs &g, int in_type, int partition, int P, void *, size_t, cudaStream_t stream)
+int tc05_launch(const GemmArgs &g, int in_type, int partition, int P, void *, size_t, cudaStream_t stream,
+                int a_tmem)
 {
     Tc05Shape s;
-    int st = tc05_shape(in_type, g.out_type, partition, P, g.M, g.N, g.K, g.a_layout, g.b_layout, &s);
+    int st = tc05_shape(in_type, g.out_type, partition, P, g.M, g.N, g.K, g.a_layout, g.b_layout, &s, a_tmem);
     if (st)
         return st;
     const bool bf16 = in_type == KAMI_BF16;
@@ -391,6 +448,8 @@ int tc05_launch(const GemmArgs &g, int in_type, int partition, int P, void *, si
     p.P = s.P;
     p.a_mn = s.a_mn;
     p.b_mn = s.b_mn;
+    p.a_tmem = s.a_tmem;
+    p.a_col = s.a_col;
     p.idesc = tc::idesc_f16(bf16, s.bm, s.part == KAMI_PARTITION_2D ? s.bn / s.P : s.bn, s.a_mn, s.b_mn);
     p.tmem_cols = s.tmem_cols;
     const double mmas = (double)g.num_iter * s.ksteps * (s.part == KAMI_PARTITION_2D ? s.P : 1);

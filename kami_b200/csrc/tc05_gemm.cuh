@@ -12,14 +12,18 @@ int cuda_fail(cudaError_t e, const char *what);
 // True when AUTO should try the tcgen05 variant first for this request.
 bool tc05_prefer(int in_type, int partition, int M, int N, int K, int a_layout, int b_layout);
 
-// Resolve (without launching) the tcgen05 launch for a request.
+// True when AUTO should keep A in tensor memory (the TS form).
+bool tc05_prefer_ts(int M, int a_layout);
+
+// Resolve (without launching) the tcgen05 launch for a request; a_tmem
+// selects the form with A resident in tensor memory.
 int tc05_plan(int in_type, int out_type, int partition, int P, int M, int N, int K, int64_t batch, int a_layout,
-              int b_layout, LaunchInfo *info);
+              int b_layout, LaunchInfo *info, int a_tmem);
 
 // Launch; returns KAMI_ERR_UNSUPPORTED (and launches nothing) when the
 // request is outside what the variant handles.
 int tc05_launch(const GemmArgs &g, int in_type, int partition, int P, void *workspace, size_t ws_bytes,
-                cudaStream_t stream);
+                cudaStream_t stream, int a_tmem);
 
 // Read and clear the device-side error flag of the tcgen05 kernels (0 = none,
 // 1 = operand loads timed out, 2 = MMA completion timed out).  Synchronous.

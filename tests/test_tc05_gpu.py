@@ -103,9 +103,12 @@ def test_tc05_rejects_what_it_cannot_do(cuda):
     A = torch.zeros((2, 256, 64), dtype=torch.float16, device="cuda")
     with pytest.raises(KamiError):
         api.gemm_batched(A, A, variant="tcgen05")
-    A = torch.zeros((2, 64, 64), dtype=torch.float16, device="cuda")
+    A = torch.zeros((2, 64, 60), dtype=torch.float16, device="cuda")  # K % 8 != 0: TMA rows misaligned
     with pytest.raises(KamiError):
-        api.gemm_batched(A, A, variant="tcgen05", b_layout="row_kn")
+        api.gemm_batched(A, A, variant="tcgen05")
+    A = torch.zeros((2, 64, 64), dtype=torch.float64, device="cuda")  # FP64 has no tcgen05 kind
+    with pytest.raises(KamiError):
+        api.gemm_batched(A, A, variant="tcgen05")
 
 
 def test_auto_picks_tcgen05_for_128(cuda):
@@ -115,7 +118,7 @@ def test_auto_picks_tcgen05_for_128(cuda):
 
 
 @pytest.mark.parametrize("a_layout,b_layout", [("col_mk", "ref_nk"), ("row_mk", "row_kn"), ("col_mk", "row_kn")])
-@pytest.mark.parametrize("M,N,K", [(128, 128, 128), (64, 64, 64), (100, 72, 40), (128, 256, 64), (64, 48, 136)])
+@pytest.mark.parametrize("M,N,K", [(128, 128, 128), (64, 64, 64), (104, 72, 40), (128, 256, 64), (64, 48, 136)])
 def test_tc05_mn_major_layouts(cuda, a_layout, b_layout, M, N, K):
     """MN-major operands (A stored K x M, B stored K x N) staged by TMA in
     64-element swizzle boxes: the layouts of the backward pass."""
@@ -128,3 +131,25 @@ def test_tc05_mn_major_layouts(cuda, a_layout, b_layout, M, N, K):
     torch.cuda.synchronize()
     _status_clean()
     assert np.array_equal(C.double().cpu().numpy(), oracle.gemm(A64, B64))
+
+
+@pytest.mark.parametrize("part,P", [("1d", 0), ("2d", 2), ("3d", 2)])
+@pytest.mark.parametrize("M,N,K", [(128, 128, 128), (100, 72, 40), (128, 256, 64), (80, 128, 256), (128, 16, 8)])
+@pytest.mark.parametrize("prec", ["f16", "bf16"])
+def test_tc05_a_in_tmem(cuda, part, P, M, N, K, prec):
+    """The TS form: A staged into tensor memory with tcgen05.st, B by TMA."""
+    if part == "3d" and ((K + 15) // 16 < P or P * ((N + 15) // 16 * 16) + (K + 15) // 16 * 8 > 512):
+        pytest.skip("does not fit")
+    if part == "2d" and N % (16 * P):
+        pytest.skip("2D panels")
+    A, B, A64, B64 = _inputs(prec, 6, M, N, K, integer=True, seed=M + N + K + P)
+    C = api.gemm_batched(A, B, variant="tcgen05_ts", partition=part, P=P)
+    torch.cuda.synchronize()
+    _status_clean()
+    assert np.array_equal(C.double().cpu().numpy(), oracle.gemm(A64, B64))
+
+
+def test_tc05_a_in_tmem_num_iter(cuda):
+    A, B, A64, B64 = _inputs("f16", 4, 128, 128, 128, integer=True, seed=9)
+    C = api.gemm_batched(A, B, variant="tcgen05_ts", num_iter=1000)
+    assert np.array_equal(C.double().cpu().numpy(), oracle.gemm(A64, B64) * 1000)
