@@ -188,6 +188,34 @@ int kami_gemm_grouped_run(const kami_grouped_plan *plan, const void *A, const vo
 int kami_gemm_grouped_plan_info(const kami_grouped_plan *plan, int64_t out[12]);
 int kami_gemm_grouped_plan_destroy(kami_grouped_plan *plan);
 
+/*
+ * Allocation-free grouped GEMM (no counterpart in the reference).  The same
+ * computation as kami_gemm_grouped_plan_create + kami_gemm_grouped_run, for
+ * callers that may not allocate device memory: code that runs while a CUDA
+ * graph is being captured, processes whose allocator forbids cudaMalloc
+ * after start-up, and embedded or real-time hosts that preallocate
+ * everything.  Instead of a plan in cudaMalloc'd memory it uses one fixed
+ * device array owned by the library (room for KAMI_NOALLOC_MAX_PROBLEMS
+ * problem descriptors plus the CTA schedule, about 0.45 MB, resident on every
+ * GPU that loads the library until the process exits).  Each call rebuilds
+ * the schedule on the host, copies it into that array with cudaMemcpyAsync
+ * on `stream` and launches the grouped kernel; it calls no cudaMalloc or
+ * cudaFree.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) and sets the kernel's attributes, so make that first
+ * call before any stream capture.  Requests with more than
+ * KAMI_NOALLOC_MAX_PROBLEMS problems are rejected with KAMI_ERR_UNSUPPORTED.
+ * All calls share the array, which keeps the last call's contents: calls
+ * whose work overlaps on the GPU (other streams, other host threads) race.
+ * Partitions come from the static cost model (autotuning would allocate).
+ * Argument meaning as in kami_gemm_grouped_plan_create / _run.
+ */
+#define KAMI_NOALLOC_MAX_PROBLEMS 8192
+int kami_gemm_grouped_noalloc(kami_dtype_t in_type, kami_dtype_t out_type, int count,
+                              const int *M, const int *N, const int *K,
+                              const int64_t *a_offsets, const int64_t *b_offsets,
+                              const int64_t *c_offsets, const void *A, const void *B, void *C,
+                              double alpha, double beta, int num_iter, void *stream);
+
 /* ------------------------------------------------------------------------ */
 /* FP64-accurate batched GEMM on the FP16/BF16 tensor cores                 */
 /* ------------------------------------------------------------------------ */

@@ -46,6 +46,7 @@ SIGNATURES = {
     "kami_gemm_grouped_run": ([_vp, _vp, _vp, _vp, _d, _d, _i, _vp], _i),
     "kami_gemm_grouped_plan_info": ([_vp, ctypes.POINTER(_i64)], _i),
     "kami_gemm_grouped_plan_destroy": ([_vp], _i),
+    "kami_gemm_grouped_noalloc": ([_i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _d, _d, _i, _vp], _i),
     "kami_split_f64_gemm_batched": ([_i, _i, _i, _i, _i, _i64, _vp, _i64, _i64, _vp, _i64, _i64, _i,
                                      _vp, _i64, _i64, _d, _d, _i, _vp], _i),
     "kami_spgemm_bsr_symbolic": ([_i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(_i), _vp], _i),

@@ -792,3 +792,219 @@ int kami_gemm_grouped_plan_info(const kami_grouped_plan *plan, int64_t out[12])
 int kami_gemm_grouped_plan_destroy(kami_grouped_plan *plan) { return free_plan(plan); }
 
 } // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the grouped launch.
+//
+// Callers that cannot allocate device memory -- code running inside a CUDA
+// graph capture that must not call cudaMalloc, allocators that forbid
+// allocation after start-up, embedded and real-time hosts that preallocate
+// everything -- cannot create a plan, because a plan keeps its problem
+// descriptors and schedule in cudaMalloc'd memory.  This entry point keeps
+// them instead in one fixed array of device memory that belongs to the
+// library (a file-scope __device__ array, KAMI_NOALLOC_MAX_PROBLEMS
+// descriptors plus the CTA schedule, about 0.45 MB on every GPU that loads
+// the library, held until the process exits).  Each call rebuilds the
+// schedule on the host (static staging arrays, no heap), copies it into that
+// array with cudaMemcpyAsync on the caller's stream and launches the same
+// grouped kernel.  Every call shares the array and leaves its own contents
+// behind: calls whose work overlaps on the GPU (different streams, or a
+// second call before the first kernel has read its descriptors) race.
+// ---------------------------------------------------------------------------
+namespace kami {
+namespace {
+
+constexpr int kNoAllocMaxProblems = 8192; // KAMI_NOALLOC_MAX_PROBLEMS in kami.h
+constexpr int kNoAllocMaxCtas = 1024;
+constexpr size_t kNoAllocDescBytes = (size_t)kNoAllocMaxProblems * sizeof(GroupedDesc);
+constexpr size_t kNoAllocBytes = kNoAllocDescBytes + (size_t)(kNoAllocMaxCtas + 1) * sizeof(int);
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+struct NoAllocDevice
+{
+    bool ready = false;
+    void *scratch = nullptr; // device address of g_noalloc_scratch on this device
+    int ctas_max = 0;        // persistent CTAs the kernel can keep resident
+};
+std::mutex g_noalloc_mu;
+NoAllocDevice g_noalloc_dev[64][3]; // [device][precision class]
+
+// host staging (no heap allocation on this path)
+GroupedDesc g_na_desc[kNoAllocMaxProblems];
+int g_na_begin[kNoAllocMaxCtas + 1];
+int g_na_order[kNoAllocMaxProblems];
+int g_na_cta[kNoAllocMaxProblems];
+double g_na_cost[kNoAllocMaxProblems];
+double g_na_load[kNoAllocMaxCtas];
+int g_na_heap[kNoAllocMaxCtas];
+
+int noalloc_class(int in_type) { return in_type == KAMI_F64 ? 2 : in_type == KAMI_BF16 ? 1 : 0; }
+
+// once per device (with that device current): the device address of the
+// scratch array, the kernel's shared-memory limit and its resident CTAs
+int noalloc_setup(int in_type, NoAllocDevice **out)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess)
+        return cuda_fail(e, "cudaGetDevice");
+    if (dev < 0 || dev >= 64)
+        return fail(KAMI_ERR_UNSUPPORTED, "no-alloc grouped GEMM: device ordinal %d above 63", dev);
+    NoAllocDevice &d = g_noalloc_dev[dev][noalloc_class(in_type)];
+    if (!d.ready)
+    {
+        void *ptr = nullptr;
+        e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess)
+            return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+        const void *fn = grouped_fn(in_type);
+        const int smem = grouped_smem(in_type);
+        if ((e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
+            return cuda_fail(e, "cudaFuncSetAttribute(grouped_kernel)");
+        int sms = 0, occ = 0;
+        if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+            return cuda_fail(e, "cudaDeviceGetAttribute");
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kThreads, smem)) != cudaSuccess)
+            return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+        d.scratch = ptr;
+        d.ctas_max = std::min(kNoAllocMaxCtas, sms * std::max(occ, 1));
+        d.ready = true;
+    }
+    *out = &d;
+    return KAMI_OK;
+}
+
+void heap_sift_down(int n, int i)
+{
+    while (true)
+    {
+        int l = 2 * i + 1, r = l + 1, m = i;
+        if (l < n && g_na_load[g_na_heap[l]] < g_na_load[g_na_heap[m]])
+            m = l;
+        if (r < n && g_na_load[g_na_heap[r]] < g_na_load[g_na_heap[m]])
+            m = r;
+        if (m == i)
+            return;
+        std::swap(g_na_heap[i], g_na_heap[m]);
+        i = m;
+    }
+}
+
+} // namespace
+} // namespace kami
+
+extern "C" int kami_gemm_grouped_noalloc(kami_dtype_t in_type, kami_dtype_t out_type, int count, const int *M,
+                                         const int *N, const int *K, const int64_t *a_offsets,
+                                         const int64_t *b_offsets, const int64_t *c_offsets, const void *A,
+                                         const void *B, void *C, double alpha, double beta, int num_iter,
+                                         void *stream)
+{
+    if (in_type != KAMI_F16 && in_type != KAMI_BF16 && in_type != KAMI_F64)
+        return fail(KAMI_ERR_INVALID_VALUE, "no-alloc grouped GEMM: in_type must be KAMI_F16, KAMI_BF16 or KAMI_F64");
+    if ((in_type == KAMI_F64) != (out_type == KAMI_F64) ||
+        (out_type != KAMI_F64 && out_type != KAMI_F32 && out_type != KAMI_F16 && out_type != KAMI_BF16))
+        return fail(KAMI_ERR_UNSUPPORTED, "no-alloc grouped GEMM: output type does not match the input type");
+    if (count < 0 || num_iter < 1)
+        return fail(KAMI_ERR_INVALID_VALUE, "no-alloc grouped GEMM: bad count or num_iter");
+    if (count > kNoAllocMaxProblems)
+        return fail(KAMI_ERR_UNSUPPORTED,
+                    "no-alloc grouped GEMM: %d problems exceed the fixed device array of %d descriptors "
+                    "(KAMI_NOALLOC_MAX_PROBLEMS); split the call or use kami_gemm_grouped_plan_create",
+                    count, kNoAllocMaxProblems);
+    if (count == 0)
+        return KAMI_OK;
+    if (!M || !N || !K || !a_offsets || !b_offsets || !c_offsets || !A || !B || !C)
+        return fail(KAMI_ERR_INVALID_VALUE, "no-alloc grouped GEMM: null array or buffer");
+    if ((reinterpret_cast<uintptr_t>(A) & 15) || (reinterpret_cast<uintptr_t>(B) & 15) ||
+        (reinterpret_cast<uintptr_t>(C) & 15))
+        return fail(KAMI_ERR_MISALIGNED, "no-alloc grouped GEMM: A, B, C must be 16-byte aligned");
+    const int kq = in_type == KAMI_F64 ? 2 : 8;
+    for (int i = 0; i < count; ++i)
+    {
+        if (M[i] < 1 || N[i] < 1 || K[i] < 1 || M[i] > 128 || N[i] > 128 || K[i] > 128 || K[i] % kq)
+            return fail(KAMI_ERR_UNSUPPORTED, "no-alloc grouped GEMM: problem %d has M, N, K = %d, %d, %d", i, M[i],
+                        N[i], K[i]);
+        if (a_offsets[i] % kq || b_offsets[i] % kq || a_offsets[i] < 0 || b_offsets[i] < 0 || c_offsets[i] < 0)
+            return fail(KAMI_ERR_MISALIGNED, "no-alloc grouped GEMM: problem %d: bad offsets", i);
+    }
+
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    NoAllocDevice *dev = nullptr;
+    int st = noalloc_setup(in_type, &dev);
+    if (st)
+        return st;
+    const int ctas = std::max(1, std::min(count, dev->ctas_max));
+    const int esz = in_type == KAMI_F64 ? 8 : 2;
+    const int osz = out_type == KAMI_F64 ? 8 : out_type == KAMI_F32 ? 4 : 2;
+    const double balance = in_type == KAMI_F64 ? 6.0 : 150.0;
+    for (int i = 0; i < count; ++i)
+    {
+        const double fl = 2.0 * M[i] * N[i] * K[i];
+        const double by = (double)(M[i] + N[i]) * K[i] * esz + (double)M[i] * N[i] * osz;
+        g_na_cost[i] = std::max(fl / balance, by) + 2048.0;
+        g_na_order[i] = i;
+    }
+    std::sort(g_na_order, g_na_order + count, [](int a, int b) {
+        return g_na_cost[a] > g_na_cost[b] || (g_na_cost[a] == g_na_cost[b] && a < b);
+    });
+    // longest-first onto the least-loaded CTA (a min-heap over static arrays)
+    for (int c = 0; c < ctas; ++c)
+    {
+        g_na_load[c] = 0.0;
+        g_na_heap[c] = c;
+        g_na_begin[c] = 0;
+    }
+    for (int r = 0; r < count; ++r)
+    {
+        const int i = g_na_order[r];
+        const int c = g_na_heap[0];
+        g_na_cta[i] = c;
+        g_na_begin[c]++;
+        g_na_load[c] += g_na_cost[i];
+        heap_sift_down(ctas, 0);
+    }
+    int run = 0;
+    for (int c = 0; c < ctas; ++c)
+    {
+        const int n = g_na_begin[c];
+        g_na_begin[c] = run;
+        run += n;
+    }
+    g_na_begin[ctas] = run;
+    {
+        // place problems in LPT order inside each CTA's range (cursor per CTA in g_na_heap)
+        for (int c = 0; c < ctas; ++c)
+            g_na_heap[c] = g_na_begin[c];
+        for (int r = 0; r < count; ++r)
+        {
+            const int i = g_na_order[r];
+            const int slot = g_na_heap[g_na_cta[i]]++;
+            g_na_desc[slot] = GroupedDesc{M[i], N[i], K[i], cfg_heuristic(in_type, M[i], N[i], K[i]),
+                                          a_offsets[i], b_offsets[i], c_offsets[i], K[i], K[i], N[i], 0};
+        }
+    }
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    unsigned char *base = reinterpret_cast<unsigned char *>(dev->scratch);
+    cudaError_t e = cudaMemcpyAsync(base, g_na_desc, sizeof(GroupedDesc) * (size_t)count, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(base + kNoAllocDescBytes, g_na_begin, sizeof(int) * (size_t)(ctas + 1),
+                            cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess)
+        return cuda_fail(e, "cudaMemcpyAsync(no-alloc grouped schedule)");
+    GroupedParams p{};
+    p.desc = reinterpret_cast<const GroupedDesc *>(base);
+    p.cta_begin = reinterpret_cast<const int *>(base + kNoAllocDescBytes);
+    p.A = A;
+    p.B = B;
+    p.C = C;
+    p.out_type = out_type;
+    p.alpha = alpha;
+    p.beta = beta;
+    p.num_iter = num_iter;
+    void *args[] = {&p};
+    e = cudaLaunchKernel(grouped_fn(in_type), dim3(ctas), dim3(kThreads), args, (size_t)grouped_smem(in_type), s);
+    if (e != cudaSuccess)
+        return cuda_fail(e, "cudaLaunchKernel(grouped_kernel, no-alloc)");
+    return KAMI_OK;
+}
