@@ -35,6 +35,21 @@ sys.path.insert(0, ROOT)
 L2_FLUSH_BYTES = 256 << 20
 
 
+class L2Flush:
+    """Between timed steps: write a buffer larger than the 126 MB L2, then read
+    a second one, so the timed kernel finds neither its inputs in L2 nor
+    dirty flush lines it would have to write back (both outside the events)."""
+
+    def __init__(self, dev):
+        import torch
+        self.w = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+        self.r = torch.ones(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    def zero_(self):
+        self.w.zero_()
+        self.r.sum()
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -70,7 +85,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -207,7 +222,7 @@ def run_ours(args, rank, world):
     A = A_h.to(dev)
     B = B_h.to(dev)
     C = torch.empty((batch, M, N), dtype=torch.float32, device=dev)
-    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    flush = L2Flush(dev)
     stream = torch.cuda.current_stream(dev)
     plan = api.describe(M, N, K, batch, torch.float16, variant=args.variant, partition=args.partition)
 
@@ -262,6 +277,18 @@ def run_ours(args, rank, world):
         if i >= args.warmup:
             e2e_ms.append(e0.elapsed_time(e1))
     clocks = sampler.stop() if sampler else None
+    # context only: this box's cuBLAS bf16 rate right now (8192^3), to tell a
+    # slow box from a slow kernel; the roofline denominator stays the
+    # driver-measured peak
+    calib = None
+    try:
+        x = torch.randn(8192, 8192, device=dev, dtype=torch.bfloat16)
+        y = torch.randn(8192, 8192, device=dev, dtype=torch.bfloat16)
+        cm = _time_ms(lambda: torch.matmul(x, y), 3, 5)
+        calib = {"cublas_bf16_8192_tflops": 2 * 8192 ** 3 / (min(cm) * 1e-3) / 1e12}
+        del x, y
+    except Exception as e:  # pragma: no cover
+        calib = {"error": str(e)[:80]}
 
     step_ms = sum(ms) / len(ms)
     e2e_step = sum(e2e_ms) / len(e2e_ms)
@@ -291,13 +318,13 @@ def run_ours(args, rank, world):
                                   f"(4 x {sms} SMs), NUM_ITER {num_iter} in-register repeats",
                       "M": M, "N": N, "K": K, "batch": batch, "num_iter": num_iter,
                       "variant": plan["variant"], "partition": plan["partition"], "P": plan["P"],
-                      "threads": plan["threads"], "l2": "256 MiB buffer written between timed steps",
+                      "threads": plan["threads"], "l2": "256 MiB buffer written, then another 256 MiB read, between timed steps",
                       "parallelism": f"replicas x{world}"},
            "roofline": roof, "cpu_baseline": cpu,
            "e2e": {"value": e2e_value, "unit": "TFLOP/s",
                    "h2d_bytes_per_step": int(A_h.numel() * 2 + B_h.numel() * 2),
                    "d2h_bytes_per_step": int(C.numel() * 4)},
-           "gpu_launches": args.steps, "clocks": clocks, "check_rel_err": rel}
+           "gpu_launches": args.steps, "clocks": clocks, "check_rel_err": rel, "box_calibration": calib}
     print(json.dumps(out), flush=True)
 
 
@@ -338,7 +365,7 @@ def run_secondary(args):
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
-    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    flush = L2Flush(dev)
     peak_tf, peak_bw, src = measured_peaks()
     W, K_ = max(args.warmup, 3), args.steps
 

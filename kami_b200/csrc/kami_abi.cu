@@ -350,6 +350,7 @@ int kami_gemm_batched(kami_dtype_t in_type, kami_dtype_t out_type, kami_partitio
     g.out_type = out_type;
     const int osz = elem_size(out_type);
     g.c_vec = ((uintptr_t)C % (uintptr_t)(2 * osz)) == 0 && ldc % 2 == 0 && strideC % 2 == 0;
+    g.c_vec4 = ((uintptr_t)C % (uintptr_t)(4 * osz)) == 0 && ldc % 4 == 0 && strideC % 4 == 0;
     g.alpha = alpha;
     g.beta = beta;
     g.num_iter = num_iter;

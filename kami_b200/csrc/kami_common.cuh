@@ -24,6 +24,7 @@ struct GemmArgs {
     int64_t ldc, sC;
     int out_type;
     int c_vec;    // 1: pairs of C elements may be stored as one vector
+    int c_vec4;   // 1: groups of 4 C elements (4-aligned columns) may be stored as one vector
     double alpha, beta;
     int num_iter;
     int problems_per_cta;

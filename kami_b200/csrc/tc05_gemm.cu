@@ -24,6 +24,7 @@
 // Every mbarrier wait is bounded; on a timeout the kernel records an error
 // in g_tc05_error, waits (bounded) for its copies in flight, frees TMEM and
 // returns.
+#include <algorithm>
 #include <mutex>
 
 #include "kami_common.cuh"
@@ -52,6 +53,147 @@ struct Tc05Params
 
 __device__ __forceinline__ void tc05_flag(int code) { atomicExch(&g_tc05_error, code); }
 
+// The MMA issue loop of one problem (one thread).  A plain runtime loop
+// whose operand descriptors advance by addition (16-byte units of the
+// start-address field: +32 B per k-step along a K-major row, +2 KB down an
+// MN-major box, a jump to the next 64-element K box every 4 k-steps).  The
+// single issuing thread has to keep pace with 64-cycle MMAs, and this form
+// measured 0.85 of peak where a fully unrolled, predicated 16-step loop
+// reached 0.66.
+__device__ __forceinline__ uint64_t kdesc(uint32_t base, int box, int mn, int ks)
+{
+    const uint32_t addr = base + (uint32_t)((ks >> 2) * box + (ks & 3) * (mn ? 2048 : 32));
+    return mn ? tc::desc_mnmajor_sw128(addr, 8192) : tc::desc_kmajor_sw128(addr);
+}
+
+template <bool TS>
+__device__ __forceinline__ void issue_mmas(const Tc05Params &p, uint32_t tmem, uint32_t a0, uint32_t b0, int a_box,
+                                           int b_box)
+{
+    const int depth = p.part == 3 ? p.P : 1;
+    const int panels = p.part == 2 ? p.P : 1;
+    const int pn = p.bn / panels;
+    const uint64_t a_in = p.a_mn ? 128 : 2, b_in = p.b_mn ? 128 : 2;
+    const uint64_t a_wrap = (uint64_t)(a_box >> 4) - 3 * a_in, b_wrap = (uint64_t)(b_box >> 4) - 3 * b_in;
+    // descriptor step between B panels (2D), in 16-byte units
+    const uint64_t qstep = p.b_mn ? (uint64_t)(pn / 64) * (8192 >> 4) : (uint64_t)pn * (128 >> 4);
+    for (int it = 0; it < p.g.num_iter; ++it)
+    {
+        for (int d = 0; d < depth; ++d)
+        {
+            const int k_lo = p.ksteps * d / depth, k_hi = p.ksteps * (d + 1) / depth;
+            const uint32_t dcol = tmem + (uint32_t)(d * p.bn);
+            uint64_t ad = TS ? 0 : kdesc(a0, a_box, p.a_mn, k_lo);
+            uint64_t bd = kdesc(b0, b_box, p.b_mn, k_lo);
+            uint32_t at = tmem + p.a_col + (uint32_t)k_lo * 8;
+            for (int ks = k_lo; ks < k_hi; ++ks)
+            {
+                const uint32_t acc = (it > 0 || ks > k_lo) ? 1u : 0u;
+                if (panels == 1)
+                {
+                    if (TS)
+                        tc::mma_f16_ts(dcol, at, bd, p.idesc, acc);
+                    else
+                        tc::mma_f16_ss(dcol, ad, bd, p.idesc, acc);
+                }
+                else
+                {
+                    for (int q = 0; q < panels; ++q)
+                    {
+                        if (TS)
+                            tc::mma_f16_ts(dcol + q * pn, at, bd + q * qstep, p.idesc, acc);
+                        else
+                            tc::mma_f16_ss(dcol + q * pn, ad, bd + q * qstep, p.idesc, acc);
+                    }
+                }
+                const bool wrap = (ks & 3) == 3;
+                ad += wrap ? a_wrap : a_in;
+                bd += wrap ? b_wrap : b_in;
+                at += 8;
+            }
+        }
+    }
+}
+
+
+// ---------------------------------------------------------------------------
+// Coalesced epilogue.  tcgen05.ld leaves each thread 16 consecutive columns of
+// its own row; stored directly that is 32 rows touched per instruction with
+// half-used sectors.  Each warp transposes through a 32 x 20-float shared
+// tile so that every store instruction writes 8 rows x 64 contiguous bytes.
+// ---------------------------------------------------------------------------
+constexpr int kEpiStride = 20;                       // floats per staged row (16 + pad)
+constexpr int kEpiTileBytes = 32 * kEpiStride * 4;   // per warp
+
+__device__ __forceinline__ void store4(const GemmArgs &g, void *Cb, int r, int c, float4 x)
+{
+    if (g.c_vec4 && c + 3 < g.N)
+    {
+        const int64_t off = (int64_t)r * g.ldc + c;
+        const float a = (float)g.alpha, b = (float)g.beta;
+        if (g.out_type == KAMI_F32)
+        {
+            float4 *dst = reinterpret_cast<float4 *>(reinterpret_cast<float *>(Cb) + off);
+            if (g.alpha != 1.0 || g.beta != 0.0)
+            {
+                const float4 o = g.beta != 0.0 ? *dst : make_float4(0.f, 0.f, 0.f, 0.f);
+                x = make_float4(a * x.x + b * o.x, a * x.y + b * o.y, a * x.z + b * o.z, a * x.w + b * o.w);
+            }
+            *dst = x;
+        }
+        else
+        {
+            const bool bf = g.out_type == KAMI_BF16;
+            uint2 *dst = reinterpret_cast<uint2 *>(reinterpret_cast<uint16_t *>(Cb) + off);
+            float y[4] = {x.x, x.y, x.z, x.w};
+            if (g.alpha != 1.0 || g.beta != 0.0)
+            {
+                const uint2 o = g.beta != 0.0 ? *dst : make_uint2(0u, 0u);
+                const uint16_t ob[4] = {(uint16_t)(o.x & 0xffff), (uint16_t)(o.x >> 16), (uint16_t)(o.y & 0xffff),
+                                        (uint16_t)(o.y >> 16)};
+#pragma unroll
+                for (int e = 0; e < 4; ++e)
+                    y[e] = a * y[e] + (g.beta != 0.0 ? b * to_float(ob[e], bf) : 0.f);
+            }
+            uint32_t h[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+                h[e] = bf ? __bfloat16_as_ushort(__float2bfloat16_rn(y[e])) : __half_as_ushort(__float2half_rn(y[e]));
+            *dst = make_uint2(h[0] | (h[1] << 16), h[2] | (h[3] << 16));
+        }
+        return;
+    }
+    store_pair<float>(g, Cb, r, c, x.x, x.y);
+    store_pair<float>(g, Cb, r, c + 2, x.z, x.w);
+}
+
+// f: the calling thread's 16 values of row (row_base + lane), columns
+// c0..c0+15; nrows: rows this warp holds (32, or 16 for M = 64 MMAs).
+__device__ __forceinline__ void store_chunk(const GemmArgs &g, void *Cb, const float (&f)[16], int row_base,
+                                            int nrows, int c0, float *T)
+{
+    const int lane = threadIdx.x & 31;
+    float4 *t4 = reinterpret_cast<float4 *>(T + lane * kEpiStride);
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+        t4[q] = make_float4(f[4 * q], f[4 * q + 1], f[4 * q + 2], f[4 * q + 3]);
+    __syncwarp();
+    const int rr = lane >> 2, cq = (lane & 3) * 4;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+    {
+        const int lr = 8 * i + rr;
+        if (lr < nrows)
+        {
+            const int r = row_base + lr;
+            const int c = c0 + cq;
+            if (r < g.M && c < g.N)
+                store4(g, Cb, r, c, *reinterpret_cast<const float4 *>(T + lr * kEpiStride + cq));
+        }
+    }
+    __syncwarp();
+}
+
 template <bool BF16>
 __global__ void __launch_bounds__(128) tc05_block_kernel(const __grid_constant__ CUtensorMap tmA,
                                                          const __grid_constant__ CUtensorMap tmB,
@@ -63,7 +205,8 @@ __global__ void __launch_bounds__(128) tc05_block_kernel(const __grid_constant__
     const int a_box = p.a_tmem ? 0 : p.bm * 128, b_box = p.bn * 128;
     uint8_t *sA = smem;
     uint8_t *sB = sA + p.nkb * a_box;
-    uint64_t *bars = reinterpret_cast<uint64_t *>(sB + p.nkb * b_box); // [0] loads landed, [1] MMAs done
+    float *epi = reinterpret_cast<float *>(sB + p.nkb * b_box);            // 4 x kEpiTileBytes
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sB + p.nkb * b_box + 4 * kEpiTileBytes); // [0] loads, [1] MMAs
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2);
     int *ok_slot = reinterpret_cast<int *>(tmem_slot + 1);
 
@@ -152,36 +295,10 @@ __global__ void __launch_bounds__(128) tc05_block_kernel(const __grid_constant__
         else
         {
             tc::tc_fence_after();
-            const uint32_t a0 = tc::smem_u32(sA), b0 = tc::smem_u32(sB);
-            const int depth = p.part == 3 ? p.P : 1;
-            const int panels = p.part == 2 ? p.P : 1;
-            const int pn = p.bn / panels;
-            for (int it = 0; it < g.num_iter; ++it)
-            {
-                for (int d = 0; d < depth; ++d)
-                {
-                    const int k_lo = p.ksteps * d / depth, k_hi = p.ksteps * (d + 1) / depth;
-                    const uint32_t acc_col = (uint32_t)(d * p.bn);
-                    for (int ks = k_lo; ks < k_hi; ++ks)
-                    {
-                        const int kb = ks >> 2, kin = ks & 3;
-                        const uint64_t adesc = p.a_mn ? tc::desc_mnmajor_sw128(a0 + kb * a_box + kin * 2048, 8192)
-                                                      : tc::desc_kmajor_sw128(a0 + kb * a_box + kin * 32);
-                        const uint32_t acc = (it > 0 || ks > k_lo) ? 1u : 0u;
-                        const uint32_t a_tm = tmem + p.a_col + (uint32_t)ks * 8;
-                        for (int q = 0; q < panels; ++q)
-                        {
-                            const uint64_t bdesc =
-                                p.b_mn ? tc::desc_mnmajor_sw128(b0 + kb * b_box + (q * pn / 64) * 8192 + kin * 2048, 8192)
-                                       : tc::desc_kmajor_sw128(b0 + kb * b_box + q * pn * 128 + kin * 32);
-                            if (p.a_tmem)
-                                tc::mma_f16_ts(tmem + acc_col + q * pn, a_tm, bdesc, p.idesc, acc);
-                            else
-                                tc::mma_f16_ss(tmem + acc_col + q * pn, adesc, bdesc, p.idesc, acc);
-                        }
-                    }
-                }
-            }
+            if (p.a_tmem)
+                issue_mmas<true>(p, tmem, tc::smem_u32(sA), tc::smem_u32(sB), a_box, b_box);
+            else
+                issue_mmas<false>(p, tmem, tc::smem_u32(sA), tc::smem_u32(sB), a_box, b_box);
             tc::mma_commit(&bars[1]);
         }
     }
@@ -196,14 +313,12 @@ __global__ void __launch_bounds__(128) tc05_block_kernel(const __grid_constant__
     const bool ok = done && *reinterpret_cast<volatile int *>(ok_slot);
     if (ok)
     {
-        const int row = p.bm == 128 ? warp * 32 + lane : warp * 16 + lane;
-        const bool row_ok = (p.bm == 128 || lane < 16) && row < g.M;
         const uint32_t lane_addr = (uint32_t)(warp * 32) << 16;
         const int depth = p.part == 3 ? p.P : 1;
         const int osz = g.out_type == KAMI_F32 ? 4 : 2;
         void *Cb = reinterpret_cast<char *>(g.C) + (int64_t)prob * g.sC * osz;
-        const bool fast = g.out_type == KAMI_F32 && g.alpha == 1.0 && g.beta == 0.0 && g.c_vec &&
-                          (g.ldc % 4 == 0) && (g.sC % 4 == 0) && ((reinterpret_cast<uintptr_t>(g.C) & 15) == 0);
+        const int row_base = p.bm == 128 ? warp * 32 : warp * 16;
+        float *T = epi + warp * (kEpiTileBytes / 4);
         for (int c0 = 0; c0 < p.bn; c0 += 16)
         {
             uint32_t v[16];
@@ -222,27 +337,206 @@ __global__ void __launch_bounds__(128) tc05_block_kernel(const __grid_constant__
                 for (int e = 0; e < 16; ++e)
                     f[e] += __uint_as_float(w[e]);
             }
-            if (row_ok)
-            {
-                if (fast && c0 + 16 <= g.N)
-                {
-                    float4 *dst = reinterpret_cast<float4 *>(reinterpret_cast<float *>(Cb) + (int64_t)row * g.ldc + c0);
-#pragma unroll
-                    for (int e = 0; e < 4; ++e)
-                        dst[e] = make_float4(f[4 * e], f[4 * e + 1], f[4 * e + 2], f[4 * e + 3]);
-                }
-                else
-                {
-#pragma unroll
-                    for (int e = 0; e < 16; e += 2)
-                        store_pair<float>(g, Cb, row, c0 + e, f[e], f[e + 1]);
-                }
-            }
+            store_chunk(g, Cb, f, row_base, p.bm == 128 ? 32 : 16, c0, T);
         }
     }
     tc::tc_fence_before();
     __syncthreads();
     if (warp == 0)
+    {
+        __syncwarp();
+        tc::tc_fence_after();
+        tc::tmem_dealloc(tmem, p.tmem_cols);
+    }
+}
+
+
+// ---------------------------------------------------------------------------
+// Persistent streaming form (1D mapping) for the streamed regime: a fixed
+// grid of CTAs (one per SM) walks problems blockIdx.x, blockIdx.x + grid, ...
+// with three warp roles so that loads, MMAs and the epilogue of different
+// problems overlap:
+//   warp 0 (one lane)  TMA producer: a ring of `stages` shared-memory slots,
+//                      each holding one problem's A and B;
+//   warp 1 (one lane)  MMA issuer: one TMEM accumulator of two (double
+//                      buffered), commits free the slot and publish the
+//                      accumulator;
+//   warps 2..9         epilogue, two groups of four: group g drains the
+//                      accumulator of every problem j with j % 2 == g
+//                      (tcgen05.ld of its TMEM lane quadrant, coalesced C
+//                      stores), then releases it -- two problems drain at once.
+// Every wait is bounded like the per-problem kernel's.
+// ---------------------------------------------------------------------------
+struct Tc05StreamParams
+{
+    Tc05Params t;
+    int stages;
+    int stage_bytes; // A + B of one problem (1024-byte multiple)
+};
+
+template <bool BF16>
+__global__ void __launch_bounds__(320, 1) tc05_stream_kernel(const __grid_constant__ CUtensorMap tmA,
+                                                             const __grid_constant__ CUtensorMap tmB,
+                                                             const Tc05StreamParams sp)
+{
+    const Tc05Params &p = sp.t;
+    const GemmArgs &g = p.g;
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int S = sp.stages;
+    const int a_box = p.bm * 128, b_box = p.bn * 128;
+    float *epi = reinterpret_cast<float *>(smem + (size_t)S * sp.stage_bytes); // 8 x kEpiTileBytes
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + (size_t)S * sp.stage_bytes + 8 * kEpiTileBytes);
+    uint64_t *empty = full + S;
+    uint64_t *tfull = empty + S;  // [2]
+    uint64_t *tempty = tfull + 2; // [2]
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tempty + 2);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t nprob = g.batch;
+    if (threadIdx.x == 0)
+    {
+        for (int i = 0; i < S; ++i)
+        {
+            tc::mbar_init(&full[i], 1);
+            tc::mbar_init(&empty[i], 1);
+        }
+        for (int i = 0; i < 2; ++i)
+        {
+            tc::mbar_init(&tfull[i], 1);
+            tc::mbar_init(&tempty[i], 4);
+        }
+        tc::fence_mbar_init();
+    }
+    __syncwarp();
+    if (warp == 1)
+    {
+        tc::tmem_alloc(tmem_slot, p.tmem_cols);
+        tc::tmem_relinquish();
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const uint64_t limit = p.timeout_ns;
+
+    if (warp == 0)
+    {
+        if (lane == 0)
+        {
+            int j = 0;
+            for (int64_t prob = blockIdx.x; prob < nprob; prob += gridDim.x, ++j)
+            {
+                const int st = j % S;
+                if (j >= S && !tc::mbar_wait_bounded(&empty[st], ((j / S) - 1) & 1, limit))
+                {
+                    tc05_flag(5);
+                    break;
+                }
+                uint8_t *sA = smem + (size_t)st * sp.stage_bytes;
+                uint8_t *sB = sA + p.nkb * a_box;
+                tc::mbar_expect_tx(&full[st], (uint32_t)sp.stage_bytes);
+                for (int kb = 0; kb < p.nkb; ++kb)
+                {
+                    if (p.a_mn)
+                        for (int mc = 0; mc < p.bm / 64; ++mc)
+                            tc::tma_load_3d(sA + kb * a_box + mc * 8192, &tmA, &full[st], mc * 64, kb * 64, (int)prob);
+                    else
+                        tc::tma_load_3d(sA + kb * a_box, &tmA, &full[st], kb * 64, 0, (int)prob);
+                    if (p.b_mn)
+                        for (int nc = 0; nc < p.bn / 64; ++nc)
+                            tc::tma_load_3d(sB + kb * b_box + nc * 8192, &tmB, &full[st], nc * 64, kb * 64, (int)prob);
+                    else
+                        tc::tma_load_3d(sB + kb * b_box, &tmB, &full[st], kb * 64, 0, (int)prob);
+                }
+            }
+            // copies of the last slots still in flight complete before exit
+            const int jn = j;
+            for (int k = (jn > S ? jn - S : 0); k < jn; ++k)
+                tc::mbar_wait_bounded(&full[k % S], (k / S) & 1, limit);
+        }
+    }
+    else if (warp == 1)
+    {
+        if (lane == 0)
+        {
+            int j = 0;
+            for (int64_t prob = blockIdx.x; prob < nprob; prob += gridDim.x, ++j)
+            {
+                const int st = j % S, b = j & 1;
+                if (!tc::mbar_wait_bounded(&full[st], (j / S) & 1, limit))
+                {
+                    tc05_flag(6);
+                    break;
+                }
+                if (j >= 2 && !tc::mbar_wait_bounded(&tempty[b], ((j >> 1) - 1) & 1, limit))
+                {
+                    tc05_flag(7);
+                    break;
+                }
+                tc::tc_fence_after();
+                const uint32_t a0 = tc::smem_u32(smem + (size_t)st * sp.stage_bytes);
+                const uint32_t b0 = a0 + p.nkb * a_box;
+                const uint32_t acc_base = tmem + (uint32_t)(b * p.bn);
+                const uint64_t a_in = p.a_mn ? 128 : 2, b_in = p.b_mn ? 128 : 2;
+                const uint64_t a_wrap = (uint64_t)(a_box >> 4) - 3 * a_in, b_wrap = (uint64_t)(b_box >> 4) - 3 * b_in;
+                for (int it = 0; it < g.num_iter; ++it)
+                {
+                    uint64_t ad = kdesc(a0, a_box, p.a_mn, 0), bd = kdesc(b0, b_box, p.b_mn, 0);
+                    for (int ks = 0; ks < p.ksteps; ++ks)
+                    {
+                        tc::mma_f16_ss(acc_base, ad, bd, p.idesc, (it > 0 || ks > 0) ? 1u : 0u);
+                        const bool wrap = (ks & 3) == 3;
+                        ad += wrap ? a_wrap : a_in;
+                        bd += wrap ? b_wrap : b_in;
+                    }
+                }
+                tc::mma_commit(&empty[st]);
+                tc::mma_commit(&tfull[b]);
+            }
+        }
+    }
+    else
+    {
+        // epilogue group g = warps 2+4g .. 5+4g, covering TMEM lane quadrants 2, 3, 0, 1
+        const int quad = warp & 3;
+        const int grp = (warp - 2) >> 2;
+        const int row_base = p.bm == 128 ? quad * 32 : quad * 16;
+        const uint32_t lane_addr = (uint32_t)(quad * 32) << 16;
+        const int osz = g.out_type == KAMI_F32 ? 4 : 2;
+        float *T = epi + (warp - 2) * (kEpiTileBytes / 4);
+        int j = grp;
+        for (int64_t prob = blockIdx.x + (int64_t)grp * gridDim.x; prob < nprob; prob += 2 * (int64_t)gridDim.x, j += 2)
+        {
+            const int b = j & 1;
+            const bool ok = __all_sync(0xffffffffu, tc::mbar_wait_bounded(&tfull[b], (j >> 1) & 1, limit));
+            if (!ok)
+            {
+                tc05_flag(8);
+                break;
+            }
+            tc::tc_fence_after();
+            void *Cb = reinterpret_cast<char *>(g.C) + prob * g.sC * osz;
+            for (int c0 = 0; c0 < p.bn; c0 += 16)
+            {
+                uint32_t v[16];
+                tc::tmem_ld16(tmem + lane_addr + (uint32_t)(b * p.bn + c0), v);
+                tc::tmem_ld_wait();
+                float f[16];
+#pragma unroll
+                for (int e = 0; e < 16; ++e)
+                    f[e] = __uint_as_float(v[e]);
+                store_chunk(g, Cb, f, row_base, p.bm == 128 ? 32 : 16, c0, T);
+            }
+            tc::tc_fence_before();
+            __syncwarp();
+            if (lane == 0)
+                tc::mbar_arrive(&tempty[b]);
+        }
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == 1)
     {
         __syncwarp();
         tc::tc_fence_after();
@@ -321,7 +615,10 @@ struct Tc05Shape
     size_t smem;
 };
 
-static size_t smem_bytes(int bm, int bn, int nkb) { return (size_t)nkb * (bm + bn) * 128 + 1024 + 64; }
+static size_t smem_bytes(int bm, int bn, int nkb)
+{
+    return (size_t)nkb * (bm + bn) * 128 + 4 * kEpiTileBytes + 1024 + 64;
+}
 
 static int tc05_shape(int in_type, int out_type, int partition, int P, int M, int N, int K, int a_layout,
                       int b_layout, Tc05Shape *s, int a_tmem = 0)
@@ -418,6 +715,42 @@ int tc05_plan(int in_type, int out_type, int partition, int P, int M, int N, int
     return KAMI_OK;
 }
 
+// Launch the persistent streaming form: one CTA per SM, as many ring slots
+// as shared memory holds (2..6), two TMEM accumulators.
+static int stream_launch(CUtensorMap &ma, CUtensorMap &mb, Tc05Params &p, bool bf16, cudaStream_t stream)
+{
+    Tc05StreamParams sp{};
+    sp.t = p;
+    sp.stage_bytes = p.nkb * (p.bm + p.bn) * 128;
+    const int budget = 227 * 1024 - 1024 - 256 - 8 * kEpiTileBytes;
+    sp.stages = std::min(6, budget / sp.stage_bytes);
+    if (sp.stages < 2)
+        return fail(KAMI_ERR_UNSUPPORTED, "tcgen05 streaming form: a problem needs %d bytes of shared memory",
+                    sp.stage_bytes);
+    uint32_t cols = 32;
+    while ((int)cols < 2 * p.bn)
+        cols <<= 1;
+    sp.t.tmem_cols = cols;
+    sp.t.timeout_ns = p.timeout_ns + 500000000ull;
+    const size_t smem = (size_t)sp.stages * sp.stage_bytes + 8 * kEpiTileBytes + 1024 + 256;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const void *fn = bf16 ? (const void *)&tc05_stream_kernel<true> : (const void *)&tc05_stream_kernel<false>;
+    static std::once_flag once[2];
+    cudaError_t e = cudaSuccess;
+    std::call_once(once[bf16 ? 1 : 0],
+                   [&] { e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024); });
+    if (e != cudaSuccess)
+        return cuda_fail(e, "cudaFuncSetAttribute(tc05_stream_kernel)");
+    const int64_t grid = std::min<int64_t>(p.g.batch, sms);
+    void *args[] = {&ma, &mb, &sp};
+    e = cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(320), args, smem, stream);
+    if (e != cudaSuccess)
+        return cuda_fail(e, "cudaLaunchKernel(tc05_stream_kernel)");
+    return KAMI_OK;
+}
+
 int tc05_launch(const GemmArgs &g, int in_type, int partition, int P, void *, size_t, cudaStream_t stream,
                 int a_tmem)
 {
@@ -450,10 +783,19 @@ int tc05_launch(const GemmArgs &g, int in_type, int partition, int P, void *, si
     p.b_mn = s.b_mn;
     p.a_tmem = s.a_tmem;
     p.a_col = s.a_col;
+
     p.idesc = tc::idesc_f16(bf16, s.bm, s.part == KAMI_PARTITION_2D ? s.bn / s.P : s.bn, s.a_mn, s.b_mn);
     p.tmem_cols = s.tmem_cols;
     const double mmas = (double)g.num_iter * s.ksteps * (s.part == KAMI_PARTITION_2D ? s.P : 1);
     p.timeout_ns = (uint64_t)(5e8 + mmas * 2000.0);
+
+    // Streamed regime: the persistent form for problems of >= 32 KB of operands
+    // (measured on B200: 128^3 x 592 121 vs 105 TFLOP/s, x 8192 190 vs 150);
+    // smaller problems drain faster as one CTA each (64^3 x 8192: 84 vs 75).
+    const int stage_bytes = s.nkb * (s.bm + s.bn) * 128;
+    if (s.part == KAMI_PARTITION_1D && !s.a_tmem && g.num_iter <= 4 && stage_bytes >= 32768 &&
+        2 * stage_bytes <= 227 * 1024 - 1024 - 256 - 8 * kEpiTileBytes)
+        return stream_launch(ma, mb, p, bf16, stream);
 
     const void *fn = bf16 ? (const void *)&tc05_block_kernel<true> : (const void *)&tc05_block_kernel<false>;
     static std::once_flag once[2];
