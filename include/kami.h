@@ -184,8 +184,10 @@ int kami_gemm_grouped_plan_create(kami_dtype_t in_type, kami_dtype_t out_type, i
 int kami_gemm_grouped_run(const kami_grouped_plan *plan, const void *A, const void *B, void *C,
                           double alpha, double beta, int num_iter, void *stream);
 /* out[0] = problems, out[1] = persistent CTAs, out[2] = shared memory bytes,
- * out[3] = FLOPs, out[4] = bytes moved, out[5..11] = problems per partition. */
-int kami_gemm_grouped_plan_info(const kami_grouped_plan *plan, int64_t out[12]);
+ * out[3] = FLOPs, out[4] = bytes moved, out[5..12] = problems per partition
+ * (0-2: 1D/2D warp grids, 3-6: 3D warp grids with K depth, 7: one warp per
+ * problem), out[13..15] = 0. */
+int kami_gemm_grouped_plan_info(const kami_grouped_plan *plan, int64_t out[16]);
 int kami_gemm_grouped_plan_destroy(kami_grouped_plan *plan);
 
 /*

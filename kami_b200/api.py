@@ -135,11 +135,11 @@ class GroupedPlan:
         self._h = h
 
     def info(self) -> dict:
-        out = (ctypes.c_int64 * 12)()
+        out = (ctypes.c_int64 * 16)()
         check(load().kami_gemm_grouped_plan_info(self._h, out))
         v = list(out)
         return {"problems": v[0], "ctas": v[1], "smem": v[2], "flops": v[3], "bytes": v[4],
-                "partitions": v[5:12]}
+                "partitions": v[5:13]}
 
     def run(self, A: torch.Tensor, B: torch.Tensor, C: torch.Tensor, *, alpha=1.0, beta=0.0, num_iter=1,
             stream=None) -> torch.Tensor:

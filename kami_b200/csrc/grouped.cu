@@ -20,6 +20,11 @@
 //   cfg 4  1x1x8  3D: 8 depth ranks (M, N <= 32)
 //   cfg 5  2x1x4  3D (M <= 64, N <= 32)
 //   cfg 6  1x2x4  3D (M <= 32, N <= 64)
+//   cfg 7  one warp owns the whole problem (M, N <= 32): after its CTA's
+//          share of the larger problems, every warp of the grid takes small
+//          problems round-robin and runs them from registers -- all loads of
+//          a K chunk issued before its MMAs, no shared memory, no CTA
+//          barrier -- so hundreds of tiny problems per SM stream in parallel.
 // Depth partials are reduced on the device through shared memory.
 #include <algorithm>
 #include <cmath>
@@ -55,13 +60,14 @@ struct GroupedParams
     int out_type;
     double alpha, beta;
     int num_iter;
+    int small_begin, small_end; // desc range of problems run by single warps
 };
 
 namespace {
 
 constexpr int kWarps = 8;
 constexpr int kThreads = kWarps * 32;
-constexpr int kCfgs = 7;
+constexpr int kCfgs = 8; // cfg 7 = single-warp problems
 __host__ __device__ constexpr int cfg_R(int c) { return c == 0 ? 8 : c == 1 ? 4 : c == 2 ? 2 : c == 3 ? 2 : c == 4 ? 1 : c == 5 ? 2 : 1; }
 __host__ __device__ constexpr int cfg_C(int c) { return c == 0 ? 1 : c == 1 ? 2 : c == 2 ? 4 : c == 3 ? 2 : c == 4 ? 1 : c == 5 ? 1 : 2; }
 __host__ __device__ constexpr int cfg_D(int c) { return c <= 2 ? 1 : c == 3 ? 2 : c == 4 ? 8 : 4; }
@@ -278,17 +284,78 @@ __device__ __forceinline__ void run_chunk(const GroupedParams &p, const GroupedD
         finish_problem<Tr, MI, MJ>(p, d, t, red, acc);
 }
 
+// One warp computes one small problem (M, N <= 32) from registers.
 template <class Tr>
-__global__ void __launch_bounds__(kThreads, 1) grouped_kernel(const GroupedParams p)
+__device__ __forceinline__ void warp_problem(const GroupedParams &p, const GroupedDesc &d)
+{
+    using Unit = typename Tr::Unit;
+    using Acc = typename Tr::Acc;
+    using Elem = typename Tr::Elem;
+    constexpr int KC = Tr::EPU == 2 ? 8 : 4; // resident k-steps per chunk (K <= 128 in one chunk for FP16)
+    const int lane = threadIdx.x & 31, gq = lane >> 2, tq = lane & 3;
+    GemmArgs g{};
+    g.M = d.M;
+    g.N = d.N;
+    g.K = d.K;
+    g.lda = d.lda;
+    g.ldb = d.ldb;
+    g.a_layout = KAMI_A_ROW_MK;
+    g.b_layout = KAMI_B_REF_NK;
+    const Elem *A = reinterpret_cast<const Elem *>(p.A) + d.a_off;
+    const Elem *B = reinterpret_cast<const Elem *>(p.B) + d.b_off;
+    const int MF = (d.M + 15) >> 4, NF = (d.N + 7) >> 3;
+    const int lane_k = tq * 2 * Tr::EPU;
+    Acc acc[2][4][4];
+#pragma unroll
+    for (int ii = 0; ii < 2; ++ii)
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj)
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+                acc[ii][jj][e] = Acc(0);
+    for (int k0 = 0; k0 < d.K; k0 += KC * Tr::KSTEP)
+    {
+        Unit a[2][KC][4], b[4][KC][2];
+#pragma unroll
+        for (int ii = 0; ii < 2; ++ii)
+#pragma unroll
+            for (int kk = 0; kk < KC; ++kk)
+                load_a_frag<Tr>(g, A, (ii < MF ? ii * 16 : 1 << 20) + gq, k0 + kk * Tr::KSTEP + lane_k, a[ii][kk]);
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj)
+#pragma unroll
+            for (int kk = 0; kk < KC; ++kk)
+                load_b_frag<Tr>(g, B, (jj < NF ? jj * 8 : 1 << 20) + gq, k0 + kk * Tr::KSTEP + lane_k, b[jj][kk]);
+        for (int it = 0; it < p.num_iter; ++it)
+#pragma unroll
+            for (int kk = 0; kk < KC; ++kk)
+                if (k0 + kk * Tr::KSTEP < d.K)
+#pragma unroll
+                    for (int ii = 0; ii < 2; ++ii)
+#pragma unroll
+                        for (int jj = 0; jj < 4; ++jj)
+                            if (ii < MF && jj < NF)
+                                Tr::mma(acc[ii][jj], a[ii][kk], b[jj][kk][0], b[jj][kk][1]);
+    }
+#pragma unroll
+    for (int ii = 0; ii < 2; ++ii)
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj)
+            if (ii < MF && jj < NF)
+            {
+                const int r = ii * 16 + gq, c = jj * 8 + 2 * tq;
+                gstore_pair<Acc>(p, d, r, c, acc[ii][jj][0], acc[ii][jj][1]);
+                gstore_pair<Acc>(p, d, r + 8, c, acc[ii][jj][2], acc[ii][jj][3]);
+            }
+}
+
+// The CTA-wide pipeline over this CTA's larger problems.
+template <class Tr>
+__device__ __forceinline__ void cta_problems(const GroupedParams &p, int begin, int end, uint8_t *smem)
 {
     using G = GGeom<Tr>;
     using Acc = typename Tr::Acc;
-    extern __shared__ __align__(128) uint8_t smem[];
     uint8_t *red = smem + G::STAGES * G::STAGE;
-    const int begin = p.cta_begin[blockIdx.x], end = p.cta_begin[blockIdx.x + 1];
-    if (begin >= end)
-        return;
-
     // unit cursor for the loads (problem index, chunk start)
     int lp = begin, lk = 0;
     auto issue = [&](int slot) {
@@ -348,6 +415,21 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_kernel(const GroupedParam
     cp_async_wait<0>();
 }
 
+template <class Tr>
+__global__ void __launch_bounds__(kThreads, 1) grouped_kernel(const GroupedParams p)
+{
+    extern __shared__ __align__(128) uint8_t smem[];
+    const int begin = p.cta_begin[blockIdx.x], end = p.cta_begin[blockIdx.x + 1];
+    if (begin < end)
+        cta_problems<Tr>(p, begin, end, smem);
+    // then every warp of the grid takes single-warp problems round-robin
+    const int gw = blockIdx.x * kWarps + (threadIdx.x >> 5);
+    const int nw = gridDim.x * kWarps;
+    for (int i = p.small_begin + gw; i < p.small_end; i += nw)
+        warp_problem<Tr>(p, p.desc[i]);
+}
+
+
 } // namespace
 } // namespace kami
 
@@ -359,6 +441,7 @@ using namespace kami;
 struct kami_grouped_plan
 {
     int in_type, out_type, count, ctas, smem;
+    int small_begin = 0, small_end = 0; // desc range of single-warp problems
     GroupedDesc *d_desc = nullptr;
     int *d_begin = nullptr;
     int cfg_hist[kCfgs] = {0};
@@ -370,6 +453,8 @@ namespace {
 
 bool cfg_valid(int cfg, int M, int N)
 {
+    if (cfg == 7)
+        return M <= 32 && N <= 32;
     const int MF = (M + 15) / 16, NF = (N + 7) / 8;
     return (MF + cfg_R(cfg) - 1) / cfg_R(cfg) <= cfg_MI(cfg) && (NF + cfg_C(cfg) - 1) / cfg_C(cfg) <= cfg_MJ(cfg);
 }
@@ -379,9 +464,11 @@ int cfg_heuristic(int in_type, int M, int N, int K)
 {
     const int kstep = in_type == KAMI_F64 ? 8 : 16;
     const int MF = (M + 15) / 16, NF = (N + 7) / 8, KS = (K + kstep - 1) / kstep;
+    if (M <= 32 && N <= 32)
+        return 7; // single-warp problem
     int best = -1;
     double bc = 0;
-    for (int c = 0; c < kCfgs; ++c)
+    for (int c = 0; c < 7; ++c)
     {
         if (!cfg_valid(c, M, N))
             continue;
@@ -437,6 +524,8 @@ static int launch_grouped(const kami_grouped_plan *plan, const void *A, const vo
     p.alpha = alpha;
     p.beta = beta;
     p.num_iter = num_iter;
+    p.small_begin = plan->small_begin;
+    p.small_end = plan->small_end;
     void *args[] = {&p};
     cudaError_t e = cudaLaunchKernel(grouped_fn(plan->in_type), dim3(plan->ctas), dim3(kThreads), args,
                                      (size_t)plan->smem, s);
@@ -506,8 +595,14 @@ static int build_plan(int in_type, int out_type, int count, const int *M, const 
     for (int c = 0; c < ctas; ++c)
         heap.push(Load(0.0, c));
     std::vector<std::vector<int>> lists(ctas);
+    std::vector<int> smalls;
     for (int i : order)
     {
+        if (cfg[i] == 7)
+        {
+            smalls.push_back(i); // longest first, spread over all warps round-robin
+            continue;
+        }
         Load l = heap.top();
         heap.pop();
         lists[l.second].push_back(i);
@@ -524,6 +619,11 @@ static int build_plan(int in_type, int out_type, int count, const int *M, const 
                                        ldb ? ldb[i] : K[i], ldc ? ldc[i] : N[i], 0});
     }
     begin[ctas] = (int)desc.size();
+    pl->small_begin = (int)desc.size();
+    for (int i : smalls)
+        desc.push_back(GroupedDesc{M[i], N[i], K[i], cfg[i], ao[i], bo[i], co[i], lda ? lda[i] : K[i],
+                                   ldb ? ldb[i] : K[i], ldc ? ldc[i] : N[i], 0});
+    pl->small_end = (int)desc.size();
     if ((e = cudaMalloc(&pl->d_desc, sizeof(GroupedDesc) * std::max(count, 1))) != cudaSuccess ||
         (e = cudaMalloc(&pl->d_begin, sizeof(int) * (ctas + 1))) != cudaSuccess)
     {
@@ -775,7 +875,7 @@ int kami_gemm_grouped_run(const kami_grouped_plan *plan, const void *A, const vo
     return launch_grouped(plan, A, B, C, alpha, beta, num_iter, reinterpret_cast<cudaStream_t>(stream));
 }
 
-int kami_gemm_grouped_plan_info(const kami_grouped_plan *plan, int64_t out[12])
+int kami_gemm_grouped_plan_info(const kami_grouped_plan *plan, int64_t out[16])
 {
     if (!plan || !out)
         return fail(KAMI_ERR_INVALID_VALUE, "grouped: null plan or out");
@@ -786,6 +886,8 @@ int kami_gemm_grouped_plan_info(const kami_grouped_plan *plan, int64_t out[12])
     out[4] = plan->bytes;
     for (int c = 0; c < kCfgs; ++c)
         out[5 + c] = plan->cfg_hist[c];
+    for (int c = 5 + kCfgs; c < 16; ++c)
+        out[c] = 0;
     return KAMI_OK;
 }
 
@@ -958,6 +1060,11 @@ extern "C" int kami_gemm_grouped_noalloc(kami_dtype_t in_type, kami_dtype_t out_
     for (int r = 0; r < count; ++r)
     {
         const int i = g_na_order[r];
+        if (cfg_heuristic(in_type, M[i], N[i], K[i]) == 7)
+        {
+            g_na_cta[i] = -1; // single-warp problem: placed after the CTA lists
+            continue;
+        }
         const int c = g_na_heap[0];
         g_na_cta[i] = c;
         g_na_begin[c]++;
@@ -976,10 +1083,11 @@ extern "C" int kami_gemm_grouped_noalloc(kami_dtype_t in_type, kami_dtype_t out_
         // place problems in LPT order inside each CTA's range (cursor per CTA in g_na_heap)
         for (int c = 0; c < ctas; ++c)
             g_na_heap[c] = g_na_begin[c];
+        int small_slot = run;
         for (int r = 0; r < count; ++r)
         {
             const int i = g_na_order[r];
-            const int slot = g_na_heap[g_na_cta[i]]++;
+            const int slot = g_na_cta[i] < 0 ? small_slot++ : g_na_heap[g_na_cta[i]]++;
             g_na_desc[slot] = GroupedDesc{M[i], N[i], K[i], cfg_heuristic(in_type, M[i], N[i], K[i]),
                                           a_offsets[i], b_offsets[i], c_offsets[i], K[i], K[i], N[i], 0};
         }
@@ -995,6 +1103,8 @@ extern "C" int kami_gemm_grouped_noalloc(kami_dtype_t in_type, kami_dtype_t out_
     GroupedParams p{};
     p.desc = reinterpret_cast<const GroupedDesc *>(base);
     p.cta_begin = reinterpret_cast<const int *>(base + kNoAllocDescBytes);
+    p.small_begin = run;
+    p.small_end = count;
     p.A = A;
     p.B = B;
     p.C = C;
