@@ -3,28 +3,35 @@
 //
 // Per problem (one CTA, 128 threads), for C = A * op(B) with M, N, K <= 64:
 //   1. scaling: row i of A is scaled by 2^-eA[i] and row j of B (column j of
-//      op(B)) by 2^-eB[j], with eA/eB the binary exponents of the row
-//      maxima (frexp), so every scaled value r0 satisfies |r0| < 1;
-//   2. splitting: s integer digits per element, d_p = rint(r * 2^beta),
-//      r <- r * 2^beta - d_p (both steps exact in FP64), so that
-//      a = 2^eA * sum_p d_p 2^(-beta p) + (a remainder below 2^(-beta s));
-//      |d_1| <= 2^beta and |d_p| <= 2^(beta-1) for p >= 2.  Digits are exact
-//      binary16 (beta = 9) or bfloat16 (beta = 7) integers, written to
+//      op(B)) by 2^-eB[j], with eA/eB = floor(log2 of the row maximum) + 2
+//      (read from the exponent bits), so every scaled value r satisfies
+//      |r| < 1/2;
+//   2. splitting: each scaled value is rounded to the integer
+//      X = round(r * 2^(beta s)) (built from the mantissa bits with one
+//      shift) and X is written in balanced base 2^beta, least significant
+//      digit first: d = ((X + 2^(beta-1)) mod 2^beta) - 2^(beta-1),
+//      X <- (X - d) / 2^beta; the most significant digit d_1 takes what is
+//      left.  So a = 2^eA * sum_p d_p 2^(-beta p) + (at most half a unit of
+//      2^(eA - beta s)) and every |d_p| <= 2^(beta-1).  The digits are exact
+//      binary16 (beta = 9) or bfloat16 (beta = 7) integers, encoded from
+//      their leading-one position with integer instructions and written to
 //      shared memory in the 128-byte-swizzled K-major layout of the MMA;
-//   3. products: slices of A are stacked in pairs -- stack t holds digit
-//      2t+1 in rows 0..63 and digit 2t+2 in rows 64..127 -- so one M = 128
-//      MMA multiplies two A digits by one B digit q.  Stack t times digit q
-//      is accumulated (FP32, in TMEM) in column block c = 2t+1+q, so the top
-//      half of block c collects the digit pairs with p + q = c and the bottom
-//      half those with p + q = c + 1.  Products with 2t+1+q > s+1 are
-//      dropped (their weight is below 2^(-beta (s+2))).  With at most
-//      ceil(s/2) digit pairs per half, |d| <= 2^(beta-1) and K <= 64, every
-//      partial sum is an integer of magnitude <= ceil(s/2) * 2^(2 beta - 2) *
-//      64 <= 2^24 (beta = 9, s <= 7; beta = 7, s <= 8), so the FP32
+//   3. products: digits are stacked in pairs on both sides -- A stack t
+//      holds digit 2t+1 in rows 0..63 and 2t+2 in rows 64..127, B pair u
+//      digit 2u+1 in rows 0..63 and 2u+2 in rows 64..127 -- so one
+//      128 x 128 x 16 MMA multiplies four digit pairs at once.  Stack t times
+//      pair u accumulates (FP32, in TMEM) into column block b = t + u, whose
+//      four 64 x 64 quadrants then hold the digit products of weight
+//      2^(-beta (2b+2)) (top-left), 2^(-beta (2b+3)) (top-right and
+//      bottom-left) and 2^(-beta (2b+4)) (bottom-right).  Blocks with
+//      2b + 2 > s + 1 are dropped (weight below 2^(-beta (s+2))).  At most
+//      4 products share a quadrant and |d| <= 2^(beta-1), so with K <= 64
+//      every partial sum is an integer of magnitude <= 4 * 2^(2 beta - 2) *
+//      64 <= 2^24 (beta = 9 for FP16 digits, beta = 7 for BF16): the FP32
 //      accumulation is exact;
-//   4. recombination in FP64: C_ij = 2^(eA_i + eB_j) * sum_c (top_c 2^(-beta c)
-//      + bottom_c 2^(-beta (c+1))), smallest weights first.
-// FP64 is used only in steps 1, 2 and 4; all products run on the tensor
+//   4. recombination in FP64: C_ij = 2^(eA_i + eB_j) * sum_b (TL + TR + BL
+//      + BR with their weights), smallest weights first.
+// FP64 arithmetic is used only in step 4; all products run on the tensor
 // cores.  num_iter repeats step 3 on the resident digits (the in-register
 // repeat used to measure the block GEMM).
 #include <mutex>
@@ -49,8 +56,10 @@ struct SplitParams
     const double *B;
     double *C;
     int M, N, K;
+    int64_t batch;
     int64_t lda, sA, ldb, sB, ldc, sC;
     int b_layout;
+    int c_vec;    // 1: C rows may be written as 16-byte pairs (aligned base, even ldc and stride)
     int s;        // digits per element
     int beta;     // bits per digit
     double alpha, beta_c;
@@ -67,63 +76,322 @@ constexpr int kSliceBytes = 64 * 128;  // 64 rows x 64 K x 2 bytes
 // the 128-byte swizzle (16-byte chunk index XOR row % 8)
 __device__ __forceinline__ int swz(int row, int chunk) { return row * 128 + ((chunk ^ (row & 7)) << 4); }
 
-template <bool BF16S>
-__device__ __forceinline__ uint32_t pack2(double x, double y)
+
+// Digit encoding without conversion instructions.  A balanced digit is
+// d = f - 2^(beta-1) with f a field of beta (top digit: beta + 1) bits.  The
+// 16-bit pattern OFF + f is the binary16 (bfloat16) number 1280 + f (128 + f),
+// exact and linear in f over the whole range (the spacing is 1 there), so one
+// packed half-precision subtraction of 1536 (192) turns two patterns into the
+// two digits d exactly.
+template <bool BF16S> struct DigitCode;
+template <> struct DigitCode<false>
 {
-    if constexpr (BF16S)
+    static constexpr int kBeta = 9;
+    static constexpr uint32_t kOff = 0x6500u;  // binary16 1280
+    static constexpr uint32_t kBias = 0x6600u; // binary16 1536 = 1280 + 2^(beta-1)
+    static __device__ __forceinline__ uint32_t sub(uint32_t w)
     {
-        const uint32_t a = __bfloat16_as_ushort(__double2bfloat16(x));
-        const uint32_t b = __bfloat16_as_ushort(__double2bfloat16(y));
-        return a | (b << 16);
+        const __half2 r = __hsub2(*reinterpret_cast<const __half2 *>(&w), __halves2half2(__ushort_as_half((unsigned short)kBias), __ushort_as_half((unsigned short)kBias)));
+        return *reinterpret_cast<const uint32_t *>(&r);
+    }
+};
+template <> struct DigitCode<true>
+{
+    static constexpr int kBeta = 7;
+    static constexpr uint32_t kOff = 0x4300u;  // bfloat16 128
+    static constexpr uint32_t kBias = 0x4340u; // bfloat16 192 = 128 + 2^(beta-1)
+    static __device__ __forceinline__ uint32_t sub(uint32_t w)
+    {
+        const __nv_bfloat162 r = __hsub2(*reinterpret_cast<const __nv_bfloat162 *>(&w),
+                                         __halves2bfloat162(__ushort_as_bfloat16((unsigned short)kBias), __ushort_as_bfloat16((unsigned short)kBias)));
+        return *reinterpret_cast<const uint32_t *>(&r);
+    }
+};
+
+// sum over k < S of 2^(beta-1) 2^(beta k): adding it to X turns the balanced
+// digits of X into the plain base-2^beta fields of the sum
+template <int BETA, int S>
+__host__ __device__ constexpr uint64_t half_digits()
+{
+    uint64_t h = 0;
+    for (int k = 0; k < S; ++k)
+        h += (uint64_t)1 << (BETA * k + BETA - 1);
+    return h;
+}
+
+// Bits [lo, lo + width) of Y, moved to bit `up` (mask m = 2^width - 1);
+// lo and up are compile-time constants after unrolling.
+__device__ __forceinline__ uint32_t field_at(uint64_t Y, int lo, uint32_t m, int up)
+{
+    return lo >= up ? (uint32_t)(Y >> (lo - up)) & (m << up) : (uint32_t)(Y << (up - lo)) & (m << up);
+}
+
+// round(x 2^(BS - e)) + H as a uint64 (|x| 2^-e < 1/2, so the rounded value
+// is at most 2^(BS-1) in magnitude and the sum is non-negative).  A normal x
+// is a 53-bit integer m times 2^(be - 1075); its row exponent satisfies
+// e >= be - 1021, so the left shift BS - e + be - 1075 is at most BS - 54 <= 9
+// and one rounding right shift of m 2^10 suffices.  Zero, and subnormal x
+// (rare; only rows whose maximum is tiny), take a slower exact path.
+// round(x 2^(BS - e)) + H as a uint64 (|x| 2^-e < 1/2, so the rounded value
+// is at most 2^(BS-1) in magnitude and the sum is non-negative).  x is an
+// integer m < 2^53 times 2^(E - 1075) (E = the biased exponent, 1 for
+// subnormals), so the value is m 2^sh with sh = E + BS - e - 1075.  When the
+// row maximum is normal, e >= E - 1021 and sh <= BS - 54 <= 9: one rounding
+// (half away from zero) right shift of m 2^10 gives it.  Only rows whose
+// maximum is subnormal reach sh > 9, where the value is m 2^sh exactly.
+template <int BS>
+__device__ __forceinline__ uint64_t offset_fixed(double x, int e, uint64_t H)
+{
+    static_assert(BS <= 63, "fixed-point image must fit in 63 bits");
+    const uint64_t u = (uint64_t)__double_as_longlong(x);
+    const int be = (int)(u >> 52) & 0x7FF;
+    const uint64_t m = (u & 0xFFFFFFFFFFFFFull) | ((uint64_t)(be != 0) << 52);
+    const int sh = (be ? be : 1) + BS - e - 1075;
+    uint64_t a;
+    if (sh <= 9)
+    {
+        const int rs = 9 - sh < 63 ? 9 - sh : 63;
+        a = (((m << 10) >> rs) + 1) >> 1;
     }
     else
+        a = m << (sh < 63 ? sh : 63);
+    return ((u >> 63) ? (uint64_t)0 - a : a) + H;
+}
+
+// Split 32 values of one operand row (this thread's half of K) into S
+// balanced base-2^beta digits and write digit p (1 = most significant) to
+// tile_row(p).  Eight elements (one 16-byte chunk of each digit tile) at a
+// time: Y = round(x 2^(beta S - e)) + H, then digit p is field S - p of Y
+// minus 2^(beta-1) (the most significant field keeps its carry bit).
+template <bool BF16S, int S, class TileFn>
+__device__ __forceinline__ void split_row(const double (&r)[32], int e, int half, TileFn tile_row)
+{
+    using Code = DigitCode<BF16S>;
+    constexpr int BETA = Code::kBeta, BS = BETA * S;
+    constexpr uint64_t H = half_digits<BETA, S>();
+    constexpr uint32_t OFF2 = Code::kOff | (Code::kOff << 16);
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
     {
-        const uint32_t a = __half_as_ushort(__double2half(x));
-        const uint32_t b = __half_as_ushort(__double2half(y));
-        return a | (b << 16);
+        uint64_t Y[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+            Y[q] = offset_fixed<BS>(r[8 * c + q], e, H);
+#pragma unroll
+        for (int k = 0; k < S; ++k)
+        {
+            // the most significant field keeps its carry bit (f <= 2^beta)
+            const uint32_t fm = k == S - 1 ? (2u << BETA) - 1u : (1u << BETA) - 1u;
+            uint32_t w[4];
+#pragma unroll
+            for (int q = 0; q < 8; q += 2)
+                w[q >> 1] = Code::sub(field_at(Y[q], BETA * k, fm, 0) + field_at(Y[q + 1], BETA * k, fm, 16) + OFF2);
+            uint8_t *base;
+            int row;
+            tile_row(S - k, base, row);
+            *reinterpret_cast<uint4 *>(base + swz(row, half * 4 + c)) = make_uint4(w[0], w[1], w[2], w[3]);
+        }
     }
 }
 
-// Split 32 values of one operand row (this thread's half of K) into s
-// digits and write digit p to tile_of(p) at row row_of(p).
-template <bool BF16S, class TileFn>
-__device__ __forceinline__ void split_row(double (&r)[32], int e, int s, int beta, int half, TileFn tile_row)
+// Scale and split one row-half of an operand: `row` of A (is_b = false) or
+// row `row` of the N x K view of B (column `row` of op(B)), K elements
+// [32 half, 32 half + 32).  Writes the row's exponent (half 0) and its s
+// digits into the digit tiles at `dig` (A: digit p in stack (p-1)/2, row
+// ((p-1)%2)*64 + row; B: digit p in tile p-1).  The two threads of a row are
+// adjacent lanes (the row maximum is exchanged with one shuffle).
+template <bool BF16S, int S>
+__device__ __forceinline__ void split_operand(const SplitParams &p, const double *X, bool is_b, int row, int half,
+                                              uint8_t *dig, int *exps)
 {
-    const double two_beta = (double)(1 << beta);
+    const int rows = is_b ? p.N : p.M;
+    const int64_t ld = is_b ? p.ldb : p.lda;
+    const bool strided = is_b && p.b_layout != KAMI_B_REF_NK;
+    double r[32];
+    double mx = 0.0;
 #pragma unroll
-    for (int i = 0; i < 32; ++i)
-        r[i] = ldexp(r[i], -e);
-    for (int p = 1; p <= s; ++p)
+    for (int i = 0; i < 32; i += 2)
     {
-        uint32_t w[16];
-#pragma unroll
-        for (int i = 0; i < 32; i += 2)
+        const int k = half * 32 + i;
+        double x0 = 0.0, x1 = 0.0;
+        if (row < rows)
         {
-            const double y0 = r[i] * two_beta, y1 = r[i + 1] * two_beta;
-            const double d0 = rint(y0), d1 = rint(y1);
-            r[i] = y0 - d0;
-            r[i + 1] = y1 - d1;
-            w[i >> 1] = pack2<BF16S>(d0, d1);
+            if (!strided)
+            {
+                if (k + 1 < p.K)
+                {
+                    const double2 v = *reinterpret_cast<const double2 *>(X + row * ld + k);
+                    x0 = v.x;
+                    x1 = v.y;
+                }
+                else if (k < p.K)
+                    x0 = X[row * ld + k];
+            }
+            else
+            {
+                if (k < p.K)
+                    x0 = X[(int64_t)k * ld + row];
+                if (k + 1 < p.K)
+                    x1 = X[(int64_t)(k + 1) * ld + row];
+            }
         }
-        uint8_t *base;
-        int row;
-        tile_row(p, base, row);
+        r[i] = x0;
+        r[i + 1] = x1;
+        mx = fmax(mx, fmax(fabs(x0), fabs(x1)));
+    }
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
+    // e = floor(log2 max) + 2, so |x| 2^-e < 1/2 and every digit satisfies
+    // |d| <= 2^(beta-1); a zero row gets e = 0 (all digits zero)
+    int e = 0;
+    if (mx > 0.0)
+    {
+        const int be = (int)(((uint64_t)__double_as_longlong(mx) >> 52) & 0x7FF);
+        if (be > 0)
+            e = be - 1023 + 2;
+        else
+        {
+            frexp(mx, &e);
+            e += 1;
+        }
+    }
+    if (half == 0)
+        exps[row] = e;
+    // digit d of row `row`: A stack (d-1)/2 holds odd digits in rows 0..63 and
+    // even digits in rows 64..127 (8 KB further), B tile d-1 holds digit d;
+    // both place digit d at byte (d-1) * 8 KB + 128 row
+    split_row<BF16S, S>(r, e, half, [&](int d, uint8_t *&base, int &rr) {
+        base = dig + (d - 1) * kSliceBytes;
+        rr = row;
+    });
+    if constexpr (S & 1)
+    {
+        // odd digit count: digit S+1 of the last pair is zero
+        uint8_t *base = dig + S * kSliceBytes;
+        const int rr = row;
 #pragma unroll
         for (int c = 0; c < 4; ++c)
-            *reinterpret_cast<uint4 *>(base + swz(row, half * 4 + c)) =
-                make_uint4(w[4 * c], w[4 * c + 1], w[4 * c + 2], w[4 * c + 3]);
+            *reinterpret_cast<uint4 *>(base + swz(rr, half * 4 + c)) = make_uint4(0, 0, 0, 0);
     }
 }
 
-template <bool BF16S>
+// 2^n as a double for n >= -1074 (subnormal below -1022), 0 below
+__device__ __forceinline__ double pow2(int n)
+{
+    if (n >= -1022)
+        return __longlong_as_double((long long)(n + 1023) << 52);
+    return n >= -1074 ? __longlong_as_double(1ll << (n + 1074)) : 0.0;
+}
+
+// v * 2^n for |v| < 2^64 and |n| < 2300.  Exact while the result is normal
+// (a power-of-two factor); a result in the subnormal range may be rounded
+// twice when n < -1022.
+__device__ __forceinline__ double scale2(double v, int n)
+{
+    if (n >= -1022 && n <= 1023)
+        return v * pow2(n);
+    const int n1 = n < -1022 ? -1022 : 1023;
+    return v * pow2(n1) * pow2(n - n1 > 1023 ? 1023 : n - n1);
+}
+
+constexpr int kXferLd = 17; // row stride (doubles) of the recombination tile; odd against bank conflicts
+
+// Partial sums of one TMEM lane for output columns j0..j0+15: column block
+// b holds the left (columns j) and right (columns 64 + j) quadrants; lanes
+// 0..63 (top, rows i) carry weights 2b+2 (left) and 2b+3 (right), lanes
+// 64..127 (bottom, rows i - 64) 2b+3 and 2b+4, in units of 2^-beta.  Blocks
+// are read smallest weight first; the TMEM reads of block b-1 are in flight
+// while block b is converted and accumulated.  taddr = lane quadrant + j0.
+template <int BMAX>
+__device__ __forceinline__ void gather_chunk(uint32_t taddr, bool top, int beta, double (&acc)[16])
+{
+    uint32_t vl[2][16], vr[2][16];
+#pragma unroll
+    for (int e = 0; e < 16; ++e)
+        acc[e] = 0.0;
+    tc::tmem_ld16(taddr + (uint32_t)BMAX * 128, vl[0]);
+    tc::tmem_ld16(taddr + (uint32_t)BMAX * 128 + 64, vr[0]);
+#pragma unroll
+    for (int b = BMAX; b >= 0; --b)
+    {
+        const int cur = (BMAX - b) & 1;
+        tc::tmem_ld_wait();
+        tc::tmem_regs_ready(vl[cur]);
+        tc::tmem_regs_ready(vr[cur]);
+        if (b > 0)
+        {
+            tc::tmem_ld16(taddr + (uint32_t)(b - 1) * 128, vl[cur ^ 1]);
+            tc::tmem_ld16(taddr + (uint32_t)(b - 1) * 128 + 64, vr[cur ^ 1]);
+        }
+        const int wl = top ? 2 * b + 2 : 2 * b + 3;
+        const double sl = pow2(-beta * wl), sr = pow2(-beta * (wl + 1));
+#pragma unroll
+        for (int e = 0; e < 16; ++e)
+            acc[e] += (double)__uint_as_float(vr[cur][e]) * sr + (double)__uint_as_float(vl[cur][e]) * sl;
+    }
+}
+
+// Store the recombined 64 x 16 chunk j0..j0+15 of C.  The 128 calling
+// threads (one per TMEM lane L) stage their partial sums of row L % 64 in
+// xfer (tile L / 64, 64 x kXferLd doubles each); then every thread finishes
+// two adjacent columns of rows L / 8, L / 8 + 16, ...: top + bottom partial,
+// times 2^(eA[row] + eB[col]), alpha and beta, stored as one 16-byte pair, so
+// a warp writes whole 128-byte row segments of C.  Barrier 1 over the 128
+// threads orders xfer.
+__device__ __forceinline__ void recombine_store(const SplitParams &p, double *Cp, const int *eA, const int *eB,
+                                                double *xfer, const double (&part)[16], int L, int j0, bool valid)
+{
+    double *mine = xfer + (L >> 6) * (64 * kXferLd) + (L & 63) * kXferLd;
+    named_barrier(1, 128); // the previous chunk's stores are done with xfer
+#pragma unroll
+    for (int e = 0; e < 16; ++e)
+        mine[e] = part[e];
+    named_barrier(1, 128);
+    const int c = (L & 7) * 2, jj = j0 + c;
+    if (!valid || jj >= p.N)
+        return;
+    const bool two = jj + 1 < p.N;
+    const int eb0 = eB[jj], eb1 = two ? eB[jj + 1] : 0;
+    for (int r = L >> 3; r < p.M; r += 16)
+    {
+        const double *top = xfer + r * kXferLd + c, *bot = top + 64 * kXferLd;
+        const double t0 = top[0], t1 = top[1], b0 = bot[0], b1 = bot[1];
+        const int ea = eA[r];
+        double *dst = Cp + (int64_t)r * p.ldc + jj;
+        double v0 = p.alpha * scale2(t0 + b0, ea + eb0), v1 = p.alpha * scale2(t1 + b1, ea + eb1);
+        if (two && p.c_vec)
+        {
+            if (p.beta_c != 0.0)
+            {
+                const double2 o = *reinterpret_cast<const double2 *>(dst);
+                v0 += p.beta_c * o.x;
+                v1 += p.beta_c * o.y;
+            }
+            *reinterpret_cast<double2 *>(dst) = make_double2(v0, v1);
+        }
+        else
+        {
+            if (p.beta_c != 0.0)
+                v0 += p.beta_c * dst[0];
+            dst[0] = v0;
+            if (two)
+            {
+                if (p.beta_c != 0.0)
+                    v1 += p.beta_c * dst[1];
+                dst[1] = v1;
+            }
+        }
+    }
+}
+
+template <bool BF16S, int S>
 __global__ void __launch_bounds__(128) split_f64_kernel(const SplitParams p)
 {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    const int nstack = (p.s + 1) / 2;
-    uint8_t *sA = smem;                           // nstack x 16 KB
-    uint8_t *sB = sA + nstack * kStackBytes;      // s x 8 KB
-    int *eA = reinterpret_cast<int *>(sB + p.s * kSliceBytes);
+    constexpr int nstack = (S + 1) / 2;
+    uint8_t *sA = smem;                           // nstack x 16 KB (A digit pairs)
+    uint8_t *sB = sA + nstack * kStackBytes;      // nstack x 16 KB (B digit pairs)
+    int *eA = reinterpret_cast<int *>(sB + nstack * kStackBytes);
     int *eB = eA + 64;
     uint64_t *bar = reinterpret_cast<uint64_t *>(eB + 64);
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar + 1);
@@ -141,97 +409,11 @@ __global__ void __launch_bounds__(128) split_f64_kernel(const SplitParams p)
         *ok_slot = 1;
     }
 
-    // ---- 1 + 2: scale and split A (two threads per row, 32 k each) ----
+    // ---- 1 + 2: scale and split A and B (two threads per row, 32 k each) ----
     const int row = t >> 1, half = t & 1;
-    {
-        double r[32];
-        double mx = 0.0;
-#pragma unroll
-        for (int i = 0; i < 32; i += 2)
-        {
-            const int k = half * 32 + i;
-            double x0 = 0.0, x1 = 0.0;
-            if (row < p.M)
-            {
-                if (k + 1 < p.K)
-                {
-                    const double2 v = *reinterpret_cast<const double2 *>(A + row * p.lda + k);
-                    x0 = v.x;
-                    x1 = v.y;
-                }
-                else if (k < p.K)
-                    x0 = A[row * p.lda + k];
-            }
-            r[i] = x0;
-            r[i + 1] = x1;
-            mx = fmax(mx, fmax(fabs(x0), fabs(x1)));
-        }
-        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
-        int e = 0;
-        if (mx > 0.0)
-            frexp(mx, &e);
-        e += 1; // |scaled| < 1/2, so every digit satisfies |d| <= 2^(beta-1)
-        if (half == 0)
-            eA[row] = e;
-        split_row<BF16S>(r, e, p.s, p.beta, half, [&](int d, uint8_t *&base, int &rr) {
-            base = sA + ((d - 1) >> 1) * kStackBytes;
-            rr = ((d - 1) & 1) * 64 + row;
-        });
-        if (p.s & 1)
-        {
-            // odd digit count: the bottom half of the last stack is zero
-            uint8_t *base = sA + (nstack - 1) * kStackBytes;
-#pragma unroll
-            for (int c = 0; c < 4; ++c)
-                *reinterpret_cast<uint4 *>(base + swz(64 + row, half * 4 + c)) = make_uint4(0, 0, 0, 0);
-        }
-    }
-    // ---- B: row j of the N x K operand (column j of op(B)) ----
-    {
-        double r[32];
-        double mx = 0.0;
-#pragma unroll
-        for (int i = 0; i < 32; i += 2)
-        {
-            const int k = half * 32 + i;
-            double x0 = 0.0, x1 = 0.0;
-            if (row < p.N)
-            {
-                if (p.b_layout == KAMI_B_REF_NK)
-                {
-                    if (k + 1 < p.K)
-                    {
-                        const double2 v = *reinterpret_cast<const double2 *>(B + row * p.ldb + k);
-                        x0 = v.x;
-                        x1 = v.y;
-                    }
-                    else if (k < p.K)
-                        x0 = B[row * p.ldb + k];
-                }
-                else
-                {
-                    if (k < p.K)
-                        x0 = B[(int64_t)k * p.ldb + row];
-                    if (k + 1 < p.K)
-                        x1 = B[(int64_t)(k + 1) * p.ldb + row];
-                }
-            }
-            r[i] = x0;
-            r[i + 1] = x1;
-            mx = fmax(mx, fmax(fabs(x0), fabs(x1)));
-        }
-        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
-        int e = 0;
-        if (mx > 0.0)
-            frexp(mx, &e);
-        e += 1;
-        if (half == 0)
-            eB[row] = e;
-        split_row<BF16S>(r, e, p.s, p.beta, half, [&](int d, uint8_t *&base, int &rr) {
-            base = sB + (d - 1) * kSliceBytes;
-            rr = row;
-        });
-    }
+#pragma unroll 1
+    for (int op = 0; op < 2; ++op)
+        split_operand<BF16S, S>(p, op ? B : A, op != 0, row, half, op ? sB : sA, op ? eB : eA);
     // make the digit tiles visible to the tensor core (async proxy)
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
@@ -250,27 +432,23 @@ __global__ void __launch_bounds__(128) split_f64_kernel(const SplitParams p)
     // ---- 3: products on the tensor core ----
     if (t == 0)
     {
-        const uint32_t a0 = tc::smem_u32(sA), b0 = tc::smem_u32(sB);
+        constexpr int bmax = (S - 1) / 2; // last column block kept
+        const uint64_t ad0 = tc::desc_kmajor_sw128(tc::smem_u32(sA));
+        const uint64_t bd0 = tc::desc_kmajor_sw128(tc::smem_u32(sB));
+        const uint64_t pair16 = kStackBytes >> 4; // descriptor step between digit pairs
         for (int it = 0; it < p.num_iter; ++it)
-        {
-            uint32_t started = 0;
             for (int st = 0; st < nstack; ++st)
-                for (int q = 1; q <= p.s; ++q)
+                for (int u = 0; st + u <= bmax && u < nstack; ++u)
                 {
-                    const int c = 2 * st + 1 + q;
-                    if (c > p.s + 1)
-                        continue;
-                    const uint32_t col = (uint32_t)(c - 2) * 64;
-                    for (int kin = 0; kin < 4; ++kin)
-                    {
-                        const uint64_t ad = tc::desc_kmajor_sw128(a0 + st * kStackBytes + kin * 32);
-                        const uint64_t bd = tc::desc_kmajor_sw128(b0 + (q - 1) * kSliceBytes + kin * 32);
-                        const uint32_t acc = (it > 0 || kin > 0 || (started >> c & 1)) ? 1u : 0u;
-                        tc::mma_f16_ss(tmem + col, ad, bd, p.idesc, acc);
-                    }
-                    started |= 1u << c;
+                    const uint32_t col = tmem + (uint32_t)(st + u) * 128;
+                    const uint64_t ad = ad0 + st * pair16, bd = bd0 + u * pair16;
+                    // stack 0 opens every block; later stacks accumulate
+                    const uint32_t first = (it == 0 && st == 0) ? 0u : 1u;
+                    tc::mma_f16_ss(col, ad, bd, p.idesc, first);
+                    tc::mma_f16_ss(col, ad + 2, bd + 2, p.idesc, 1u);
+                    tc::mma_f16_ss(col, ad + 4, bd + 4, p.idesc, 1u);
+                    tc::mma_f16_ss(col, ad + 6, bd + 6, p.idesc, 1u);
                 }
-        }
         tc::mma_commit(bar);
     }
     __syncwarp();
@@ -281,62 +459,216 @@ __global__ void __launch_bounds__(128) split_f64_kernel(const SplitParams p)
 
     // ---- 4: recombination in FP64, 16 output columns at a time ----
     // lanes 0..63 of TMEM hold the top halves (rows i), lanes 64..127 the
-    // bottom halves (rows i - 64); the bottom threads hand their partial sums
-    // to the top threads through shared memory (the digit tiles are dead).
-    double *xfer = reinterpret_cast<double *>(smem); // 64 x 16 doubles
+    // bottom halves (rows i - 64); both stage their partial sums in shared
+    // memory (the digit tiles are dead once the products are done).
+    double *xfer = reinterpret_cast<double *>(smem); // 2 x 64 x kXferLd doubles
     const int L = warp * 32 + lane;
     const bool top = L < 64;
-    const int i = top ? L : L - 64;
     const uint32_t lane_addr = (uint32_t)(warp * 32) << 16;
-    const int64_t osz = 8;
     double *Cp = p.C + prob * p.sC;
+    constexpr int bmax = (S - 1) / 2;
     for (int j0 = 0; j0 < 64; j0 += 16)
     {
-        double S[16];
-#pragma unroll
-        for (int e = 0; e < 16; ++e)
-            S[e] = 0.0;
+        double acc[16];
         if (done)
-        {
-            for (int c = p.s + 1; c >= 2; --c)
-            {
-                uint32_t v[16];
-                tc::tmem_ld16(tmem + lane_addr + (uint32_t)(c - 2) * 64 + j0, v);
-                tc::tmem_ld_wait();
-                const int w = top ? c : c + 1;
-                const double scale = ldexp(1.0, -p.beta * w);
-#pragma unroll
-                for (int e = 0; e < 16; ++e)
-                    S[e] += (double)__uint_as_float(v[e]) * scale;
-            }
-        }
-        __syncthreads(); // previous chunk's readers are done with xfer
-        if (!top)
+            gather_chunk<bmax>(tmem + lane_addr + j0, top, p.beta, acc);
+        else
         {
 #pragma unroll
             for (int e = 0; e < 16; ++e)
-                xfer[i * 16 + e] = S[e];
+                acc[e] = 0.0;
         }
-        __syncthreads();
-        if (top && done && i < p.M)
-        {
-            const int ea = eA[i];
-            for (int e = 0; e < 16; ++e)
-            {
-                const int j = j0 + e;
-                if (j >= p.N)
-                    break;
-                double v = ldexp(xfer[i * 16 + e] + S[e], ea + eB[j]);
-                double *dst = Cp + (int64_t)i * p.ldc + j;
-                v = p.alpha * v + (p.beta_c != 0.0 ? p.beta_c * *dst : 0.0);
-                *dst = v;
-            }
-        }
+        recombine_store(p, Cp, eA, eB, xfer, acc, L, j0, done);
     }
-    (void)osz;
     tc::tc_fence_before();
     __syncthreads();
     if (warp == 0)
+    {
+        __syncwarp();
+        tc::tc_fence_after();
+        tc::tmem_dealloc(tmem, p.tmem_cols);
+    }
+}
+
+
+// ---------------------------------------------------------------------------
+// Persistent form for the streamed regime (one launch over all problems, one
+// CTA per SM, 13 warps), so the three phases of consecutive problems overlap:
+//   warps 0-7   split: 256 threads, one row-half of A or B each, into digit
+//               buffer j % nbuf (two buffers when they fit in shared memory);
+//   warp 12     MMA issue (one lane) once the digits of problem j are in and
+//               the accumulator of problem j-1 has been read out;
+//   warps 8-11  recombination of problem j from TMEM (lane quadrants 0-3),
+//               then release of the accumulator and of the digit buffer.
+// Barriers: dfull[b] (8 split warps), dempty[b] (the MMA commit + the 4
+// recombination warps, which still read the buffer's exponents), tfull (MMA
+// commit), tempty (4 recombination warps).  Every wait is bounded.
+// ---------------------------------------------------------------------------
+struct SplitStreamParams
+{
+    SplitParams p;
+    int nbuf;      // digit buffers (1 or 2)
+    int buf_bytes; // digits of A and B + exponents of one problem
+};
+
+template <bool BF16S, int S>
+__global__ void __launch_bounds__(416, 1) split_f64_persistent(const SplitStreamParams sp)
+{
+    const SplitParams &p = sp.p;
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    constexpr int nstack = (S + 1) / 2;
+    const int digit_bytes = 2 * nstack * kStackBytes;
+    double *xfer = reinterpret_cast<double *>(smem + (size_t)sp.nbuf * sp.buf_bytes); // 2 x 64 x kXferLd doubles
+    uint64_t *dfull = reinterpret_cast<uint64_t *>(xfer + 2 * 64 * kXferLd);
+    uint64_t *dempty = dfull + 2;
+    uint64_t *tfull = dempty + 2;
+    uint64_t *tempty = tfull + 1;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tempty + 1);
+
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int64_t nprob = p.batch;
+    const uint64_t limit = p.timeout_ns;
+    if (t == 0)
+    {
+        for (int i = 0; i < 2; ++i)
+        {
+            tc::mbar_init(&dfull[i], 8);
+            tc::mbar_init(&dempty[i], 5);
+        }
+        tc::mbar_init(tfull, 1);
+        tc::mbar_init(tempty, 4);
+        tc::fence_mbar_init();
+    }
+    __syncwarp();
+    if (warp == 12)
+    {
+        tc::tmem_alloc(tmem_slot, p.tmem_cols);
+        tc::tmem_relinquish();
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp < 8)
+    {
+        // ---- split role ----
+        const bool is_b = t >= 128;
+        const int row = (t & 127) >> 1, half = t & 1;
+        int j = 0;
+        for (int64_t prob = blockIdx.x; prob < nprob; prob += gridDim.x, ++j)
+        {
+            const int b = j % sp.nbuf;
+            if (j >= sp.nbuf &&
+                !__all_sync(0xffffffffu, tc::mbar_wait_bounded(&dempty[b], ((j / sp.nbuf) - 1) & 1, limit)))
+            {
+                atomicExch(&g_split_error, 5);
+                break;
+            }
+            // pull this thread's two 128-byte lines of the next problem into L2
+            if (prob + gridDim.x < nprob)
+            {
+                const double *nx = is_b ? p.B + (prob + gridDim.x) * p.sB : p.A + (prob + gridDim.x) * p.sA;
+                const int64_t ld = is_b ? p.ldb : p.lda;
+                const int tt = t & 127;
+                const bool rowmajor_rows = !(is_b && p.b_layout != KAMI_B_REF_NK);
+                const int nrows = rowmajor_rows ? (is_b ? p.N : p.M) : p.K;
+                const int rowbytes = (rowmajor_rows ? p.K : p.N) * 8;
+                const int off = (tt & 1) * 256;
+                const char *line = reinterpret_cast<const char *>(nx + (int64_t)(tt >> 1) * ld) + off;
+                if ((tt >> 1) < nrows && off < rowbytes)
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(line));
+                if ((tt >> 1) < nrows && off + 128 < rowbytes)
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(line + 128));
+            }
+            uint8_t *buf = smem + (size_t)b * sp.buf_bytes;
+            int *eA = reinterpret_cast<int *>(buf + digit_bytes);
+            split_operand<BF16S, S>(p, is_b ? p.B + prob * p.sB : p.A + prob * p.sA, is_b, row, half,
+                                    is_b ? buf + nstack * kStackBytes : buf, is_b ? eA + 64 : eA);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            if (lane == 0)
+                tc::mbar_arrive(&dfull[b]);
+        }
+    }
+    else if (warp == 12)
+    {
+        // ---- MMA role ----
+        if (lane == 0)
+        {
+            constexpr int bmax = (S - 1) / 2;
+            const uint64_t pair16 = kStackBytes >> 4;
+            int j = 0;
+            for (int64_t prob = blockIdx.x; prob < nprob; prob += gridDim.x, ++j)
+            {
+                const int b = j % sp.nbuf;
+                if (!tc::mbar_wait_bounded(&dfull[b], (j / sp.nbuf) & 1, limit) ||
+                    (j >= 1 && !tc::mbar_wait_bounded(tempty, (j - 1) & 1, limit)))
+                {
+                    atomicExch(&g_split_error, 6);
+                    break;
+                }
+                tc::tc_fence_after();
+                uint8_t *buf = smem + (size_t)b * sp.buf_bytes;
+                const uint64_t ad0 = tc::desc_kmajor_sw128(tc::smem_u32(buf));
+                const uint64_t bd0 = tc::desc_kmajor_sw128(tc::smem_u32(buf + nstack * kStackBytes));
+                for (int it = 0; it < p.num_iter; ++it)
+                    for (int st = 0; st < nstack; ++st)
+                        for (int u = 0; st + u <= bmax && u < nstack; ++u)
+                        {
+                            const uint32_t col = tmem + (uint32_t)(st + u) * 128;
+                            const uint64_t ad = ad0 + st * pair16, bd = bd0 + u * pair16;
+                            const uint32_t first = (it == 0 && st == 0) ? 0u : 1u;
+                            tc::mma_f16_ss(col, ad, bd, p.idesc, first);
+                            tc::mma_f16_ss(col, ad + 2, bd + 2, p.idesc, 1u);
+                            tc::mma_f16_ss(col, ad + 4, bd + 4, p.idesc, 1u);
+                            tc::mma_f16_ss(col, ad + 6, bd + 6, p.idesc, 1u);
+                        }
+                tc::mma_commit(&dempty[b]);
+                tc::mma_commit(tfull);
+            }
+        }
+    }
+    else
+    {
+        // ---- recombination role: warps 8..11 = TMEM lane quadrants 0..3 ----
+        const int quad = warp & 3;
+        const int L = quad * 32 + lane;
+        const bool top = L < 64;
+        const uint32_t lane_addr = (uint32_t)(quad * 32) << 16;
+        constexpr int bmax = (S - 1) / 2;
+        int j = 0;
+        for (int64_t prob = blockIdx.x; prob < nprob; prob += gridDim.x, ++j)
+        {
+            const int b = j % sp.nbuf;
+            if (!__all_sync(0xffffffffu, tc::mbar_wait_bounded(tfull, j & 1, limit)))
+            {
+                atomicExch(&g_split_error, 7);
+                break;
+            }
+            tc::tc_fence_after();
+            const int *eA = reinterpret_cast<const int *>(smem + (size_t)b * sp.buf_bytes + digit_bytes);
+            const int *eB = eA + 64;
+            double *Cp = p.C + prob * p.sC;
+            for (int j0 = 0; j0 < 64; j0 += 16)
+            {
+                double acc[16];
+                gather_chunk<bmax>(tmem + lane_addr + j0, top, p.beta, acc);
+                recombine_store(p, Cp, eA, eB, xfer, acc, L, j0, true);
+            }
+            tc::tc_fence_before();
+            __syncwarp();
+            if (lane == 0)
+            {
+                tc::mbar_arrive(tempty);
+                tc::mbar_arrive(&dempty[b]);
+            }
+        }
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == 12)
     {
         __syncwarp();
         tc::tc_fence_after();
@@ -360,7 +692,59 @@ int split_read_error(int *flag)
 
 namespace {
 
-size_t split_smem(int s) { return (size_t)((s + 1) / 2) * kStackBytes + (size_t)s * kSliceBytes + 1024 + 1024; }
+struct SplitFns
+{
+    const void *per_problem;
+    const void *persistent;
+};
+
+template <bool BF, int S>
+SplitFns split_fns()
+{
+    return {(const void *)&split_f64_kernel<BF, S>, (const void *)&split_f64_persistent<BF, S>};
+}
+
+// kernels per (digit type, digit count): FP16 digits 2..7, BF16 digits 2..8
+SplitFns split_lookup(bool bf, int s)
+{
+    if (bf)
+        switch (s)
+        {
+        case 2: return split_fns<true, 2>();
+        case 3: return split_fns<true, 3>();
+        case 4: return split_fns<true, 4>();
+        case 5: return split_fns<true, 5>();
+        case 6: return split_fns<true, 6>();
+        case 7: return split_fns<true, 7>();
+        case 8: return split_fns<true, 8>();
+        default: break;
+        }
+    else
+        switch (s)
+        {
+        case 2: return split_fns<false, 2>();
+        case 3: return split_fns<false, 3>();
+        case 4: return split_fns<false, 4>();
+        case 5: return split_fns<false, 5>();
+        case 6: return split_fns<false, 6>();
+        case 7: return split_fns<false, 7>();
+        default: break;
+        }
+    return {nullptr, nullptr};
+}
+
+// raise the dynamic shared memory limit of one kernel, once per process
+cudaError_t allow_smem(const void *fn, bool bf, int s, int which)
+{
+    static std::once_flag once[2][9][2];
+    static cudaError_t err[2][9][2];
+    std::call_once(once[bf][s][which], [&] {
+        err[bf][s][which] = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    });
+    return err[bf][s][which];
+}
+
+size_t split_smem(int s) { return (size_t)((s + 1) / 2) * 2 * kStackBytes + 1024 + 1024; }
 
 } // namespace
 } // namespace kami
@@ -405,6 +789,7 @@ extern "C" int kami_split_f64_gemm_batched(int nslices, kami_dtype_t slice_type,
     p.M = M;
     p.N = N;
     p.K = K;
+    p.batch = batch;
     p.lda = lda;
     p.sA = strideA;
     p.ldb = ldb;
@@ -412,27 +797,53 @@ extern "C" int kami_split_f64_gemm_batched(int nslices, kami_dtype_t slice_type,
     p.ldc = ldc;
     p.sC = strideC;
     p.b_layout = b_layout;
+    p.c_vec = !(reinterpret_cast<uintptr_t>(C) & 15) && !(ldc & 1) && !(strideC & 1);
     p.s = nslices;
     p.beta = bf ? 7 : 9;
     p.alpha = alpha;
     p.beta_c = beta;
     p.num_iter = num_iter;
-    p.idesc = tc::idesc_f16(bf, 128, 64);
+    p.idesc = tc::idesc_f16(bf, 128, 128);
     uint32_t cols = 32;
-    while ((int)cols < nslices * 64)
+    while ((int)cols < ((nslices - 1) / 2 + 1) * 128)
         cols <<= 1;
     p.tmem_cols = cols;
     p.timeout_ns = (uint64_t)(5e8 + (double)num_iter * nslices * nslices * 4 * 2000.0);
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const SplitFns fns = split_lookup(bf, nslices);
+    if (!fns.per_problem)
+        return fail(KAMI_ERR_UNSUPPORTED, "split-FP64: no kernel for %d slices", nslices);
+    if (num_iter <= 4)
+    {
+        // streamed regime: the persistent, phase-overlapped form
+        SplitStreamParams sp{};
+        sp.p = p;
+        const int nstack = (nslices + 1) / 2;
+        sp.buf_bytes = (2 * nstack * kStackBytes + 512 + 1023) / 1024 * 1024;
+        const size_t fixed = 2 * 64 * kXferLd * 8 + 128 + 1024;
+        sp.nbuf = (size_t)2 * sp.buf_bytes + fixed <= 227 * 1024 ? 2 : 1;
+        const size_t smem = (size_t)sp.nbuf * sp.buf_bytes + fixed;
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const void *fn = fns.persistent;
+        cudaError_t e2 = allow_smem(fn, bf, nslices, 1);
+        if (e2 != cudaSuccess)
+            return cuda_fail(e2, "cudaFuncSetAttribute(split_f64_persistent)");
+        const int64_t grid = batch < sms ? batch : sms;
+        void *args2[] = {&sp};
+        e2 = cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(416), args2, smem, st);
+        if (e2 != cudaSuccess)
+            return cuda_fail(e2, "cudaLaunchKernel(split_f64_persistent)");
+        return KAMI_OK;
+    }
     const size_t smem = split_smem(nslices);
-    const void *fn = bf ? (const void *)&split_f64_kernel<true> : (const void *)&split_f64_kernel<false>;
-    static std::once_flag once[2];
-    cudaError_t e = cudaSuccess;
-    std::call_once(once[bf ? 1 : 0],
-                   [&] { e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024); });
+    const void *fn = fns.per_problem;
+    cudaError_t e = allow_smem(fn, bf, nslices, 0);
     if (e != cudaSuccess)
         return cuda_fail(e, "cudaFuncSetAttribute(split_f64_kernel)");
     void *args[] = {&p};
-    e = cudaLaunchKernel(fn, dim3((unsigned)batch), dim3(128), args, smem, reinterpret_cast<cudaStream_t>(stream));
+    e = cudaLaunchKernel(fn, dim3((unsigned)batch), dim3(128), args, smem, st);
     if (e != cudaSuccess)
         return cuda_fail(e, "cudaLaunchKernel(split_f64_kernel)");
     return KAMI_OK;

@@ -142,6 +142,19 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16])
 
 __device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+// Order the uses of 16 registers filled by tcgen05.ld after a preceding
+// tcgen05.wait::ld: the empty statement reads and rewrites them, so the
+// compiler cannot hoist their uses above it.
+__device__ __forceinline__ void tmem_regs_ready(uint32_t (&v)[16])
+{
+    asm volatile(""
+                 : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7]),
+                   "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]), "+r"(v[12]), "+r"(v[13]), "+r"(v[14]),
+                   "+r"(v[15])
+                 :
+                 : "memory");
+}
+
 // thread t of the warp writes lane (base lane + t), columns [col, col+16)
 __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&v)[16])
 {
