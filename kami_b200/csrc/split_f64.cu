@@ -194,20 +194,17 @@ __device__ __forceinline__ void split_row(const double (&r)[32], int e, int half
     }
 }
 
-// Scale and split one row-half of an operand: `row` of A (is_b = false) or
-// row `row` of the N x K view of B (column `row` of op(B)), K elements
-// [32 half, 32 half + 32).  Writes the row's exponent (half 0) and its s
-// digits into the digit tiles at `dig` (A: digit p in stack (p-1)/2, row
-// ((p-1)%2)*64 + row; B: digit p in tile p-1).  The two threads of a row are
-// adjacent lanes (the row maximum is exchanged with one shuffle).
-template <bool BF16S, int S>
-__device__ __forceinline__ void split_operand(const SplitParams &p, const double *X, bool is_b, int row, int half,
-                                              uint8_t *dig, int *exps)
+// Load one row-half of an operand into r: `row` of A (is_b = false) or row
+// `row` of the N x K view of B (column `row` of op(B)), K elements
+// [32 half, 32 half + 32), zero outside the problem.  X / ld address the
+// operand in global memory or its staged copy in shared memory (same
+// layout, row stride ld).  Returns the maximum magnitude over the whole row
+// (the two threads of a row are adjacent lanes; one shuffle).
+__device__ __forceinline__ double load_row(const SplitParams &p, const double *X, int64_t ld, bool is_b, int row,
+                                           int half, double (&r)[32])
 {
     const int rows = is_b ? p.N : p.M;
-    const int64_t ld = is_b ? p.ldb : p.lda;
     const bool strided = is_b && p.b_layout != KAMI_B_REF_NK;
-    double r[32];
     double mx = 0.0;
 #pragma unroll
     for (int i = 0; i < 32; i += 2)
@@ -218,28 +215,39 @@ __device__ __forceinline__ void split_operand(const SplitParams &p, const double
         {
             if (!strided)
             {
+                const int64_t o = row * ld + k;
                 if (k + 1 < p.K)
                 {
-                    const double2 v = *reinterpret_cast<const double2 *>(X + row * ld + k);
+                    const double2 v = *reinterpret_cast<const double2 *>(X + o);
                     x0 = v.x;
                     x1 = v.y;
                 }
                 else if (k < p.K)
-                    x0 = X[row * ld + k];
+                    x0 = X[o];
             }
             else
             {
+                const int64_t o = (int64_t)k * ld + row;
                 if (k < p.K)
-                    x0 = X[(int64_t)k * ld + row];
+                    x0 = X[o];
                 if (k + 1 < p.K)
-                    x1 = X[(int64_t)(k + 1) * ld + row];
+                    x1 = X[o + ld];
             }
         }
         r[i] = x0;
         r[i + 1] = x1;
         mx = fmax(mx, fmax(fabs(x0), fabs(x1)));
     }
-    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
+    return fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
+}
+
+// Scale and split one loaded row-half (row maximum mx).  Writes the row's
+// exponent (half 0) and its S digits into the digit tiles at `dig` (A: digit
+// p in stack (p-1)/2, row ((p-1)%2)*64 + row; B: digit p in tile p-1).
+template <bool BF16S, int S>
+__device__ __forceinline__ void split_loaded(const double (&r)[32], double mx, int row, int half, uint8_t *dig,
+                                             int *exps)
+{
     // e = floor(log2 max) + 2, so |x| 2^-e < 1/2 and every digit satisfies
     // |d| <= 2^(beta-1); a zero row gets e = 0 (all digits zero)
     int e = 0;
@@ -267,11 +275,19 @@ __device__ __forceinline__ void split_operand(const SplitParams &p, const double
     {
         // odd digit count: digit S+1 of the last pair is zero
         uint8_t *base = dig + S * kSliceBytes;
-        const int rr = row;
 #pragma unroll
         for (int c = 0; c < 4; ++c)
-            *reinterpret_cast<uint4 *>(base + swz(rr, half * 4 + c)) = make_uint4(0, 0, 0, 0);
+            *reinterpret_cast<uint4 *>(base + swz(row, half * 4 + c)) = make_uint4(0, 0, 0, 0);
     }
+}
+
+template <bool BF16S, int S>
+__device__ __forceinline__ void split_operand(const SplitParams &p, const double *X, bool is_b, int row, int half,
+                                              uint8_t *dig, int *exps)
+{
+    double r[32];
+    const double mx = load_row(p, X, is_b ? p.ldb : p.lda, is_b, row, half, r);
+    split_loaded<BF16S, S>(r, mx, row, half, dig, exps);
 }
 
 // 2^n as a double for n >= -1074 (subnormal below -1022), 0 below
@@ -293,71 +309,83 @@ __device__ __forceinline__ double scale2(double v, int n)
     return v * pow2(n1) * pow2(n - n1 > 1023 ? 1023 : n - n1);
 }
 
-constexpr int kXferLd = 17; // row stride (doubles) of the recombination tile; odd against bank conflicts
+// Row stride (doubles) of the recombination tile for chunks of W columns:
+// W + 2 keeps rows 16-byte aligned and spreads 16-byte accesses of
+// consecutive rows over all bank groups.
+template <int W>
+constexpr int xfer_ld()
+{
+    return W + 2;
+}
 
-// Partial sums of one TMEM lane for output columns j0..j0+15: column block
+// Partial sums of one TMEM lane for output columns j0..j0+W-1: column block
 // b holds the left (columns j) and right (columns 64 + j) quadrants; lanes
 // 0..63 (top, rows i) carry weights 2b+2 (left) and 2b+3 (right), lanes
 // 64..127 (bottom, rows i - 64) 2b+3 and 2b+4, in units of 2^-beta.  Blocks
-// are read smallest weight first; the TMEM reads of block b-1 are in flight
-// while block b is converted and accumulated.  taddr = lane quadrant + j0.
-template <int BMAX>
-__device__ __forceinline__ void gather_chunk(uint32_t taddr, bool top, int beta, double (&acc)[16])
+// are read smallest weight first, 16 columns at a time; the TMEM reads of
+// the next 16 columns are in flight while the current ones are converted
+// and accumulated.  taddr = lane quadrant + j0.
+template <int BMAX, int W>
+__device__ __forceinline__ void gather_chunk(uint32_t taddr, bool top, int beta, double (&acc)[W])
 {
+    constexpr int H = W / 16, NU = (BMAX + 1) * H; // units of 16 columns
     uint32_t vl[2][16], vr[2][16];
 #pragma unroll
-    for (int e = 0; e < 16; ++e)
+    for (int e = 0; e < W; ++e)
         acc[e] = 0.0;
     tc::tmem_ld16(taddr + (uint32_t)BMAX * 128, vl[0]);
     tc::tmem_ld16(taddr + (uint32_t)BMAX * 128 + 64, vr[0]);
 #pragma unroll
-    for (int b = BMAX; b >= 0; --b)
+    for (int u = 0; u < NU; ++u)
     {
-        const int cur = (BMAX - b) & 1;
+        const int b = BMAX - u / H, h = u % H, cur = u & 1;
         tc::tmem_ld_wait();
         tc::tmem_regs_ready(vl[cur]);
         tc::tmem_regs_ready(vr[cur]);
-        if (b > 0)
+        if (u + 1 < NU)
         {
-            tc::tmem_ld16(taddr + (uint32_t)(b - 1) * 128, vl[cur ^ 1]);
-            tc::tmem_ld16(taddr + (uint32_t)(b - 1) * 128 + 64, vr[cur ^ 1]);
+            const int bn = BMAX - (u + 1) / H, hn = (u + 1) % H;
+            tc::tmem_ld16(taddr + (uint32_t)bn * 128 + 16 * hn, vl[cur ^ 1]);
+            tc::tmem_ld16(taddr + (uint32_t)bn * 128 + 64 + 16 * hn, vr[cur ^ 1]);
         }
         const int wl = top ? 2 * b + 2 : 2 * b + 3;
         const double sl = pow2(-beta * wl), sr = pow2(-beta * (wl + 1));
 #pragma unroll
         for (int e = 0; e < 16; ++e)
-            acc[e] += (double)__uint_as_float(vr[cur][e]) * sr + (double)__uint_as_float(vl[cur][e]) * sl;
+            acc[16 * h + e] += (double)__uint_as_float(vr[cur][e]) * sr + (double)__uint_as_float(vl[cur][e]) * sl;
     }
 }
 
-// Store the recombined 64 x 16 chunk j0..j0+15 of C.  The 128 calling
+// Store the recombined 64 x W chunk j0..j0+W-1 of C.  The 128 calling
 // threads (one per TMEM lane L) stage their partial sums of row L % 64 in
-// xfer (tile L / 64, 64 x kXferLd doubles each); then every thread finishes
-// two adjacent columns of rows L / 8, L / 8 + 16, ...: top + bottom partial,
-// times 2^(eA[row] + eB[col]), alpha and beta, stored as one 16-byte pair, so
-// a warp writes whole 128-byte row segments of C.  Barrier 1 over the 128
-// threads orders xfer.
+// xfer (tile L / 64, 64 x xfer_ld<W>() doubles each, 16-byte stores); then
+// every thread finishes two adjacent columns of rows L / (W/2), ... : top +
+// bottom partial, times 2^(eA[row] + eB[col]), alpha and beta, stored as one
+// 16-byte pair, so a warp writes whole row segments of C.  Barrier 1 over
+// the 128 threads orders xfer.
+template <int W>
 __device__ __forceinline__ void recombine_store(const SplitParams &p, double *Cp, const int *eA, const int *eB,
-                                                double *xfer, const double (&part)[16], int L, int j0, bool valid)
+                                                double *xfer, const double (&part)[W], int L, int j0, bool valid)
 {
-    double *mine = xfer + (L >> 6) * (64 * kXferLd) + (L & 63) * kXferLd;
+    constexpr int LD = xfer_ld<W>(), TPR = W / 2, RSTEP = 128 / TPR; // threads per row, rows per pass
+    double *mine = xfer + (L >> 6) * (64 * LD) + (L & 63) * LD;
     named_barrier(1, 128); // the previous chunk's stores are done with xfer
 #pragma unroll
-    for (int e = 0; e < 16; ++e)
-        mine[e] = part[e];
+    for (int e = 0; e < W; e += 2)
+        *reinterpret_cast<double2 *>(mine + e) = make_double2(part[e], part[e + 1]);
     named_barrier(1, 128);
-    const int c = (L & 7) * 2, jj = j0 + c;
+    const int c = (L % TPR) * 2, jj = j0 + c;
     if (!valid || jj >= p.N)
         return;
     const bool two = jj + 1 < p.N;
     const int eb0 = eB[jj], eb1 = two ? eB[jj + 1] : 0;
-    for (int r = L >> 3; r < p.M; r += 16)
+    for (int r = L / TPR; r < p.M; r += RSTEP)
     {
-        const double *top = xfer + r * kXferLd + c, *bot = top + 64 * kXferLd;
-        const double t0 = top[0], t1 = top[1], b0 = bot[0], b1 = bot[1];
+        const double2 tp = *reinterpret_cast<const double2 *>(xfer + r * LD + c);
+        const double2 bt = *reinterpret_cast<const double2 *>(xfer + (64 + r) * LD + c);
         const int ea = eA[r];
         double *dst = Cp + (int64_t)r * p.ldc + jj;
-        double v0 = p.alpha * scale2(t0 + b0, ea + eb0), v1 = p.alpha * scale2(t1 + b1, ea + eb1);
+        double v0 = p.alpha * scale2(tp.x + bt.x, ea + eb0), v1 = p.alpha * scale2(tp.y + bt.y, ea + eb1);
         if (two && p.c_vec)
         {
             if (p.beta_c != 0.0)
@@ -387,7 +415,9 @@ template <bool BF16S, int S>
 __global__ void __launch_bounds__(128) split_f64_kernel(const SplitParams p)
 {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    // 1024-byte aligned base, derived from smem_raw by an offset so that the
+    // compiler still knows every derived pointer addresses shared memory
+    uint8_t *smem = smem_raw + ((1024u - (uint32_t)(reinterpret_cast<uintptr_t>(smem_raw) & 1023u)) & 1023u);
     constexpr int nstack = (S + 1) / 2;
     uint8_t *sA = smem;                           // nstack x 16 KB (A digit pairs)
     uint8_t *sB = sA + nstack * kStackBytes;      // nstack x 16 KB (B digit pairs)
@@ -461,24 +491,25 @@ __global__ void __launch_bounds__(128) split_f64_kernel(const SplitParams p)
     // lanes 0..63 of TMEM hold the top halves (rows i), lanes 64..127 the
     // bottom halves (rows i - 64); both stage their partial sums in shared
     // memory (the digit tiles are dead once the products are done).
-    double *xfer = reinterpret_cast<double *>(smem); // 2 x 64 x kXferLd doubles
+    double *xfer = reinterpret_cast<double *>(smem); // 2 x 64 x xfer_ld<W>() doubles
     const int L = warp * 32 + lane;
     const bool top = L < 64;
     const uint32_t lane_addr = (uint32_t)(warp * 32) << 16;
     double *Cp = p.C + prob * p.sC;
     constexpr int bmax = (S - 1) / 2;
-    for (int j0 = 0; j0 < 64; j0 += 16)
+    constexpr int W = S >= 3 ? 32 : 16; // the 2-digit form has only 32 KB of dead digit tiles
+    for (int j0 = 0; j0 < 64; j0 += W)
     {
-        double acc[16];
+        double acc[W];
         if (done)
-            gather_chunk<bmax>(tmem + lane_addr + j0, top, p.beta, acc);
+            gather_chunk<bmax, W>(tmem + lane_addr + j0, top, p.beta, acc);
         else
         {
 #pragma unroll
-            for (int e = 0; e < 16; ++e)
+            for (int e = 0; e < W; ++e)
                 acc[e] = 0.0;
         }
-        recombine_store(p, Cp, eA, eB, xfer, acc, L, j0, done);
+        recombine_store<W>(p, Cp, eA, eB, xfer, acc, L, j0, done);
     }
     tc::tc_fence_before();
     __syncthreads();
@@ -493,38 +524,117 @@ __global__ void __launch_bounds__(128) split_f64_kernel(const SplitParams p)
 
 // ---------------------------------------------------------------------------
 // Persistent form for the streamed regime (one launch over all problems, one
-// CTA per SM, 13 warps), so the three phases of consecutive problems overlap:
-//   warps 0-7   split: 256 threads, one row-half of A or B each, into digit
-//               buffer j % nbuf (two buffers when they fit in shared memory);
-//   warp 12     MMA issue (one lane) once the digits of problem j are in and
-//               the accumulator of problem j-1 has been read out;
-//   warps 8-11  recombination of problem j from TMEM (lane quadrants 0-3),
-//               then release of the accumulator and of the digit buffer.
-// Barriers: dfull[b] (8 split warps), dempty[b] (the MMA commit + the 4
-// recombination warps, which still read the buffer's exponents), tfull (MMA
-// commit), tempty (4 recombination warps).  Every wait is bounded.
+// CTA per SM, 12 warps), so the phases of consecutive problems overlap:
+//   warps 0-7   split: 256 threads, one row-half of A or B each.  With
+//               16-byte aligned rows the inputs of problem j are staged in
+//               shared memory by bulk copies (TMA engine) that the split
+//               warps issued for it while working on problem j-1; once all
+//               eight warps have read problem j out of the stage they issue
+//               the copies of problem j+1, then write the digits of problem
+//               j into buffer j % nbuf once the MMAs of the problem that
+//               last used it have completed;
+//   warps 8-11  recombination of problem j from TMEM (lane quadrants 0-3).
+//               After the last TMEM read of problem j, lane 0 of warp 8
+//               issues the MMAs of problem j+1 (its digits complete), then
+//               the four warps store the last columns of problem j.
+// Row and column exponents live in a ring of four entries apart from the
+// digit buffers.  Barriers: sfull (bulk copies, by bytes), dfull[b] (8 split
+// warps), dempty[b] and tfull (MMA commits).
+// Every mbarrier wait is bounded; each warp group agrees on the outcome of
+// its waits with a barrier reduction before acting on it, so a timeout
+// ends the whole group together.
 // ---------------------------------------------------------------------------
+constexpr int kStageLd = 66;                            // staged row stride (doubles): 528 bytes
+constexpr int kStageBytes = 2 * 64 * kStageLd * 8;      // A rows, then B rows
+constexpr int kExpRing = 4;
+
+// Output columns per recombination chunk of the persistent form: 32, except
+// where the 128 KB digit buffer of 7 or 8 digits leaves no room for it.
+template <int S>
+constexpr int persistent_chunk()
+{
+    return S <= 6 ? 32 : 16;
+}
+
 struct SplitStreamParams
 {
     SplitParams p;
     int nbuf;      // digit buffers (1 or 2)
-    int buf_bytes; // digits of A and B + exponents of one problem
+    int buf_bytes; // digits of A and B of one problem
+    int staged;    // 1: inputs are staged by bulk copies (16-byte aligned rows)
 };
 
+// AND of `pred` over the `n` threads of named barrier `id` (whole warps)
+__device__ __forceinline__ bool barrier_and(int id, int n, bool pred)
+{
+    uint32_t out;
+    asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.and.pred q, %2, %3, p;\n\t"
+                 "selp.u32 %0, 1, 0, q;\n\t}"
+                 : "=r"(out)
+                 : "r"((uint32_t)pred), "r"(id), "r"(n)
+                 : "memory");
+    return out != 0;
+}
+
+// Bulk copies of problem `prob`'s A rows (threads 0..63 of the split group)
+// and B rows (threads 64..127) into the stage; thread 0 first announces the
+// byte count on sfull.
+__device__ __forceinline__ void stage_problem(const SplitParams &p, int64_t prob, int tt, uint8_t *stage,
+                                              uint64_t *sfull)
+{
+    const bool refnk = p.b_layout == KAMI_B_REF_NK;
+    const uint32_t a_bytes = (uint32_t)p.K * 8, b_bytes = (uint32_t)(refnk ? p.K : p.N) * 8;
+    const int b_rows = refnk ? p.N : p.K;
+    if (tt == 0)
+        tc::mbar_expect_tx(sfull, (uint32_t)p.M * a_bytes + (uint32_t)b_rows * b_bytes);
+    if (tt < 64 && tt < p.M)
+        tc::bulk_g2s(stage + (size_t)tt * kStageLd * 8, p.A + prob * p.sA + tt * p.lda, a_bytes, sfull);
+    else if (tt >= 64 && tt < 128 && tt - 64 < b_rows)
+        tc::bulk_g2s(stage + (size_t)tt * kStageLd * 8, p.B + prob * p.sB + (tt - 64) * p.ldb, b_bytes, sfull);
+}
+
+template <int S>
+__device__ __forceinline__ void issue_products(const SplitParams &p, uint32_t tmem, uint8_t *buf, uint64_t *dempty,
+                                               uint64_t *tfull)
+{
+    constexpr int nstack = (S + 1) / 2, bmax = (S - 1) / 2;
+    const uint64_t pair16 = kStackBytes >> 4;
+    const uint64_t ad0 = tc::desc_kmajor_sw128(tc::smem_u32(buf));
+    const uint64_t bd0 = tc::desc_kmajor_sw128(tc::smem_u32(buf + nstack * kStackBytes));
+    for (int it = 0; it < p.num_iter; ++it)
+        for (int st = 0; st < nstack; ++st)
+            for (int u = 0; st + u <= bmax && u < nstack; ++u)
+            {
+                const uint32_t col = tmem + (uint32_t)(st + u) * 128;
+                const uint64_t ad = ad0 + st * pair16, bd = bd0 + u * pair16;
+                const uint32_t first = (it == 0 && st == 0) ? 0u : 1u;
+                tc::mma_f16_ss(col, ad, bd, p.idesc, first);
+                tc::mma_f16_ss(col, ad + 2, bd + 2, p.idesc, 1u);
+                tc::mma_f16_ss(col, ad + 4, bd + 4, p.idesc, 1u);
+                tc::mma_f16_ss(col, ad + 6, bd + 6, p.idesc, 1u);
+            }
+    tc::mma_commit(dempty);
+    tc::mma_commit(tfull);
+}
+
 template <bool BF16S, int S>
-__global__ void __launch_bounds__(416, 1) split_f64_persistent(const SplitStreamParams sp)
+__global__ void __launch_bounds__(384, 1) split_f64_persistent(const SplitStreamParams sp)
 {
     const SplitParams &p = sp.p;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    // 1024-byte aligned base, derived from smem_raw by an offset so that the
+    // compiler still knows every derived pointer addresses shared memory
+    uint8_t *smem = smem_raw + ((1024u - (uint32_t)(reinterpret_cast<uintptr_t>(smem_raw) & 1023u)) & 1023u);
     constexpr int nstack = (S + 1) / 2;
-    const int digit_bytes = 2 * nstack * kStackBytes;
-    double *xfer = reinterpret_cast<double *>(smem + (size_t)sp.nbuf * sp.buf_bytes); // 2 x 64 x kXferLd doubles
-    uint64_t *dfull = reinterpret_cast<uint64_t *>(xfer + 2 * 64 * kXferLd);
+    uint8_t *stage = smem + (size_t)sp.nbuf * sp.buf_bytes;
+    constexpr int W = persistent_chunk<S>();
+    double *xfer = reinterpret_cast<double *>(stage + (sp.staged ? kStageBytes : 0)); // 2 x 64 x xfer_ld<W>()
+    int *exps = reinterpret_cast<int *>(xfer + 2 * 64 * xfer_ld<W>());               // kExpRing x 128
+    uint64_t *dfull = reinterpret_cast<uint64_t *>(exps + kExpRing * 128);
     uint64_t *dempty = dfull + 2;
     uint64_t *tfull = dempty + 2;
-    uint64_t *tempty = tfull + 1;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tempty + 1);
+    uint64_t *sfull = tfull + 1;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(sfull + 1);
 
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const int64_t nprob = p.batch;
@@ -534,14 +644,14 @@ __global__ void __launch_bounds__(416, 1) split_f64_persistent(const SplitStream
         for (int i = 0; i < 2; ++i)
         {
             tc::mbar_init(&dfull[i], 8);
-            tc::mbar_init(&dempty[i], 5);
+            tc::mbar_init(&dempty[i], 1);
         }
         tc::mbar_init(tfull, 1);
-        tc::mbar_init(tempty, 4);
+        tc::mbar_init(sfull, 1);
         tc::fence_mbar_init();
     }
     __syncwarp();
-    if (warp == 12)
+    if (warp == 8)
     {
         tc::tmem_alloc(tmem_slot, p.tmem_cols);
         tc::tmem_relinquish();
@@ -553,122 +663,125 @@ __global__ void __launch_bounds__(416, 1) split_f64_persistent(const SplitStream
 
     if (warp < 8)
     {
-        // ---- split role ----
+        // ---- split role (named barrier 2 over its 256 threads) ----
         const bool is_b = t >= 128;
         const int row = (t & 127) >> 1, half = t & 1;
+        int issued = 0, consumed = 0; // stage phases started / completed and read
+        if (sp.staged && blockIdx.x < nprob)
+        {
+            if (t < 128)
+                stage_problem(p, blockIdx.x, t, stage, sfull);
+            issued = 1;
+        }
         int j = 0;
         for (int64_t prob = blockIdx.x; prob < nprob; prob += gridDim.x, ++j)
         {
+            double r[32], mx;
+            if (sp.staged)
+            {
+                if (!barrier_and(2, 256, tc::mbar_wait_bounded(sfull, j & 1, limit)))
+                {
+                    atomicExch(&g_split_error, 8);
+                    break;
+                }
+                consumed = j + 1;
+                mx = load_row(p, reinterpret_cast<const double *>(stage) + (is_b ? 64 * kStageLd : 0), kStageLd,
+                              is_b, row, half, r);
+                // all eight warps have read the stage: refill it with the next problem
+                named_barrier(2, 256);
+                if (prob + gridDim.x < nprob)
+                {
+                    if (t < 128)
+                        stage_problem(p, prob + gridDim.x, t, stage, sfull);
+                    issued = j + 2;
+                }
+            }
+            else
+                mx = load_row(p, is_b ? p.B + prob * p.sB : p.A + prob * p.sA, is_b ? p.ldb : p.lda, is_b, row,
+                              half, r);
             const int b = j % sp.nbuf;
-            if (j >= sp.nbuf &&
-                !__all_sync(0xffffffffu, tc::mbar_wait_bounded(&dempty[b], ((j / sp.nbuf) - 1) & 1, limit)))
+            if (!barrier_and(2, 256,
+                             j < sp.nbuf || tc::mbar_wait_bounded(&dempty[b], ((j / sp.nbuf) - 1) & 1, limit)))
             {
                 atomicExch(&g_split_error, 5);
                 break;
             }
-            // pull this thread's two 128-byte lines of the next problem into L2
-            if (prob + gridDim.x < nprob)
-            {
-                const double *nx = is_b ? p.B + (prob + gridDim.x) * p.sB : p.A + (prob + gridDim.x) * p.sA;
-                const int64_t ld = is_b ? p.ldb : p.lda;
-                const int tt = t & 127;
-                const bool rowmajor_rows = !(is_b && p.b_layout != KAMI_B_REF_NK);
-                const int nrows = rowmajor_rows ? (is_b ? p.N : p.M) : p.K;
-                const int rowbytes = (rowmajor_rows ? p.K : p.N) * 8;
-                const int off = (tt & 1) * 256;
-                const char *line = reinterpret_cast<const char *>(nx + (int64_t)(tt >> 1) * ld) + off;
-                if ((tt >> 1) < nrows && off < rowbytes)
-                    asm volatile("prefetch.global.L2 [%0];" ::"l"(line));
-                if ((tt >> 1) < nrows && off + 128 < rowbytes)
-                    asm volatile("prefetch.global.L2 [%0];" ::"l"(line + 128));
-            }
             uint8_t *buf = smem + (size_t)b * sp.buf_bytes;
-            int *eA = reinterpret_cast<int *>(buf + digit_bytes);
-            split_operand<BF16S, S>(p, is_b ? p.B + prob * p.sB : p.A + prob * p.sA, is_b, row, half,
-                                    is_b ? buf + nstack * kStackBytes : buf, is_b ? eA + 64 : eA);
+            int *ex = exps + (j % kExpRing) * 128;
+            split_loaded<BF16S, S>(r, mx, row, half, is_b ? buf + nstack * kStackBytes : buf, is_b ? ex + 64 : ex);
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
             if (lane == 0)
                 tc::mbar_arrive(&dfull[b]);
         }
-    }
-    else if (warp == 12)
-    {
-        // ---- MMA role ----
-        if (lane == 0)
-        {
-            constexpr int bmax = (S - 1) / 2;
-            const uint64_t pair16 = kStackBytes >> 4;
-            int j = 0;
-            for (int64_t prob = blockIdx.x; prob < nprob; prob += gridDim.x, ++j)
-            {
-                const int b = j % sp.nbuf;
-                if (!tc::mbar_wait_bounded(&dfull[b], (j / sp.nbuf) & 1, limit) ||
-                    (j >= 1 && !tc::mbar_wait_bounded(tempty, (j - 1) & 1, limit)))
-                {
-                    atomicExch(&g_split_error, 6);
-                    break;
-                }
-                tc::tc_fence_after();
-                uint8_t *buf = smem + (size_t)b * sp.buf_bytes;
-                const uint64_t ad0 = tc::desc_kmajor_sw128(tc::smem_u32(buf));
-                const uint64_t bd0 = tc::desc_kmajor_sw128(tc::smem_u32(buf + nstack * kStackBytes));
-                for (int it = 0; it < p.num_iter; ++it)
-                    for (int st = 0; st < nstack; ++st)
-                        for (int u = 0; st + u <= bmax && u < nstack; ++u)
-                        {
-                            const uint32_t col = tmem + (uint32_t)(st + u) * 128;
-                            const uint64_t ad = ad0 + st * pair16, bd = bd0 + u * pair16;
-                            const uint32_t first = (it == 0 && st == 0) ? 0u : 1u;
-                            tc::mma_f16_ss(col, ad, bd, p.idesc, first);
-                            tc::mma_f16_ss(col, ad + 2, bd + 2, p.idesc, 1u);
-                            tc::mma_f16_ss(col, ad + 4, bd + 4, p.idesc, 1u);
-                            tc::mma_f16_ss(col, ad + 6, bd + 6, p.idesc, 1u);
-                        }
-                tc::mma_commit(&dempty[b]);
-                tc::mma_commit(tfull);
-            }
-        }
+        // no bulk copy may still be landing when the CTA exits (possible only
+        // after a failed wait): wait for the phase of the copies not yet read
+        if (issued > consumed && !tc::mbar_wait_bounded(sfull, consumed & 1, limit))
+            atomicExch(&g_split_error, 9);
     }
     else
     {
-        // ---- recombination role: warps 8..11 = TMEM lane quadrants 0..3 ----
+        // ---- recombination role: warps 8..11 = TMEM lane quadrants 0..3
+        //      (named barrier 1 over its 128 threads); lane 0 of warp 8 also
+        //      issues the MMAs ----
         const int quad = warp & 3;
         const int L = quad * 32 + lane;
         const bool top = L < 64;
+        const bool issuer = warp == 8 && lane == 0;
         const uint32_t lane_addr = (uint32_t)(quad * 32) << 16;
         constexpr int bmax = (S - 1) / 2;
+        if (issuer && blockIdx.x < nprob)
+        {
+            if (tc::mbar_wait_bounded(&dfull[0], 0, limit))
+            {
+                tc::tc_fence_after();
+                issue_products<S>(p, tmem, smem, &dempty[0], tfull);
+            }
+            else
+                atomicExch(&g_split_error, 6);
+        }
+        __syncwarp();
         int j = 0;
         for (int64_t prob = blockIdx.x; prob < nprob; prob += gridDim.x, ++j)
         {
-            const int b = j % sp.nbuf;
-            if (!__all_sync(0xffffffffu, tc::mbar_wait_bounded(tfull, j & 1, limit)))
+            if (!barrier_and(1, 128, tc::mbar_wait_bounded(tfull, j & 1, limit)))
             {
                 atomicExch(&g_split_error, 7);
                 break;
             }
             tc::tc_fence_after();
-            const int *eA = reinterpret_cast<const int *>(smem + (size_t)b * sp.buf_bytes + digit_bytes);
+            const int *eA = exps + (j % kExpRing) * 128;
             const int *eB = eA + 64;
             double *Cp = p.C + prob * p.sC;
-            for (int j0 = 0; j0 < 64; j0 += 16)
+            for (int j0 = 0; j0 < 64; j0 += W)
             {
-                double acc[16];
-                gather_chunk<bmax>(tmem + lane_addr + j0, top, p.beta, acc);
-                recombine_store(p, Cp, eA, eB, xfer, acc, L, j0, true);
-            }
-            tc::tc_fence_before();
-            __syncwarp();
-            if (lane == 0)
-            {
-                tc::mbar_arrive(tempty);
-                tc::mbar_arrive(&dempty[b]);
+                double acc[W];
+                gather_chunk<bmax, W>(tmem + lane_addr + j0, top, p.beta, acc);
+                if (j0 == 64 - W)
+                {
+                    // every TMEM read of problem j is done: start problem j+1
+                    tc::tc_fence_before();
+                    named_barrier(1, 128);
+                    if (issuer && prob + gridDim.x < nprob)
+                    {
+                        const int jn = j + 1, bn = jn % sp.nbuf;
+                        if (tc::mbar_wait_bounded(&dfull[bn], (jn / sp.nbuf) & 1, limit))
+                        {
+                            tc::tc_fence_after();
+                            issue_products<S>(p, tmem, smem + (size_t)bn * sp.buf_bytes, &dempty[bn], tfull);
+                        }
+                        else
+                            atomicExch(&g_split_error, 6); // the next tfull wait then times out for all
+                    }
+                    __syncwarp();
+                }
+                recombine_store<W>(p, Cp, eA, eB, xfer, acc, L, j0, true);
             }
         }
     }
     tc::tc_fence_before();
     __syncthreads();
-    if (warp == 12)
+    if (warp == 8)
     {
         __syncwarp();
         tc::tc_fence_after();
@@ -819,8 +932,15 @@ extern "C" int kami_split_f64_gemm_batched(int nslices, kami_dtype_t slice_type,
         SplitStreamParams sp{};
         sp.p = p;
         const int nstack = (nslices + 1) / 2;
-        sp.buf_bytes = (2 * nstack * kStackBytes + 512 + 1023) / 1024 * 1024;
-        const size_t fixed = 2 * 64 * kXferLd * 8 + 128 + 1024;
+        sp.buf_bytes = 2 * nstack * kStackBytes;
+        // bulk copies need 16-byte aligned rows whose length is a multiple of 16 bytes
+        const bool a_ok = !(reinterpret_cast<uintptr_t>(A) & 15) && !(lda & 1) && !(strideA & 1) && !(K & 1);
+        const bool b_ok = !(reinterpret_cast<uintptr_t>(B) & 15) && !(ldb & 1) && !(strideB & 1) &&
+                          !((b_layout == KAMI_B_REF_NK ? K : N) & 1);
+        sp.staged = a_ok && b_ok ? 1 : 0;
+        const int xld = (nslices <= 6 ? 32 : 16) + 2; // xfer_ld<persistent_chunk<S>()>()
+        const size_t fixed = (size_t)2 * 64 * xld * 8 + kExpRing * 128 * 4 + 128 + 1024 +
+                             (sp.staged ? kStageBytes : 0);
         sp.nbuf = (size_t)2 * sp.buf_bytes + fixed <= 227 * 1024 ? 2 : 1;
         const size_t smem = (size_t)sp.nbuf * sp.buf_bytes + fixed;
         int dev = 0, sms = 148;
@@ -832,7 +952,7 @@ extern "C" int kami_split_f64_gemm_batched(int nslices, kami_dtype_t slice_type,
             return cuda_fail(e2, "cudaFuncSetAttribute(split_f64_persistent)");
         const int64_t grid = batch < sms ? batch : sms;
         void *args2[] = {&sp};
-        e2 = cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(416), args2, smem, st);
+        e2 = cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(384), args2, smem, st);
         if (e2 != cudaSuccess)
             return cuda_fail(e2, "cudaLaunchKernel(split_f64_persistent)");
         return KAMI_OK;

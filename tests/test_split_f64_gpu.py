@@ -85,3 +85,20 @@ def test_num_iter_repeats_products(cuda):
     B = rng.integers(-50, 51, (4, 64, 64)).astype(np.float64)
     C = api.split_f64_gemm(torch.tensor(A, device="cuda"), torch.tensor(B, device="cuda"), nslices=3, num_iter=5)
     assert np.array_equal(C.cpu().numpy(), 5 * oracle.gemm(A, B))
+
+
+@pytest.mark.parametrize("slice_dtype,s,b_layout,N", [(torch.float16, 3, "ref_nk", 64), (torch.float16, 6, "ref_nk", 64),
+                                                       (torch.bfloat16, 8, "ref_nk", 64),
+                                                       (torch.float16, 6, "row_kn", 63)])
+def test_streamed_many_problems_exact(cuda, slice_dtype, s, b_layout, N):
+    """Many problems per CTA (the persistent form's buffer rings and phases),
+    staged (aligned rows) and unstaged (row_kn with an odd N) inputs; integer
+    inputs make every digit product exact, so the result must be exact."""
+    rng = np.random.default_rng(s + N)
+    batch = 1500
+    A = rng.integers(-2000, 2001, (batch, 64, 64)).astype(np.float64)
+    Bt = rng.integers(-2000, 2001, (batch, 64, N)).astype(np.float64)
+    B = np.ascontiguousarray(Bt.transpose(0, 2, 1)) if b_layout == "ref_nk" else Bt
+    C = api.split_f64_gemm(torch.tensor(A, device="cuda"), torch.tensor(B, device="cuda"), nslices=s,
+                           slice_dtype=slice_dtype, b_layout=b_layout)
+    assert np.array_equal(C.cpu().numpy(), np.matmul(A, Bt))
