@@ -63,7 +63,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="bounded CPU-baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="block",
-                    choices=["block", "block-sweep", "fp64", "split", "uneven", "spgemm", "bmm"],
+                    choices=["block", "block-sweep", "fp64", "split", "uneven", "spgemm", "spmm", "bmm"],
                     help="block (default, the headline line) or one of the other configurations; "
                          "non-default workloads print one JSON line per measured case")
     return ap.parse_args()
@@ -513,6 +513,50 @@ def run_secondary(args):
                    "symbolic_ms": min(ms_sym), "tflops_numeric": fl / t / 1e9,
                    "hbm_gbs_numeric": by / t / 1e6, "frac_hbm": by / t / 1e6 / peak_bw,
                    "tflops_end_to_end": fl / (t + min(ms_sym)) / 1e9})
+        return
+
+    if args.workload == "spmm":
+        # (a) the reference programs' own shape and method: one 64 x 64 BSR block
+        # (4 x 4 tiles, the reference generator at sparsity 0.5) times a dense
+        # 64 x 64 B per CTA, 16384 CTAs sharing A and B, NUM_ITER 1000
+        #  (spmm/1d/block_spmm_1d_half_mma.cu:229-285; FLOPs 2 * nnz * N).
+        rp, ci, vals = oracle.bsr_generate(4, 4, 0.5, rule="spmm1d")
+        rng = np.random.default_rng(0)
+        Bh = torch.tensor(rng.integers(0, 3, (64, 64)), dtype=torch.float16, device=dev)
+        d_rp, d_ci = torch.tensor(rp, device=dev), torch.tensor(ci, device=dev)
+        d_v = torch.tensor(vals, device=dev)
+        for batch, it in [(16384, 1000), (16384, 1)]:
+            Cb = torch.empty((batch, 64, 64), dtype=torch.float32, device=dev)
+            ms = _time_ms(lambda: api.spmm_batched(d_rp, d_ci, d_v, 4, Bh, Cb, b_layout="ref_nk", num_iter=it),
+                          W, K_, flush)
+            t = min(ms)
+            fl = 2.0 * ci.size * 256 * 64 * batch * it
+            ref = oracle.spmm(rp, ci, vals.astype(np.float64), 4, Bh.double().cpu().numpy(), "ref_nk")
+            err = float(np.abs(Cb[batch - 1].double().cpu().numpy() / it - ref).max())
+            _emit({"workload": "spmm", "case": "reference block 64x64x64, 50 % tiles, shared A/B",
+                   "nnz_blocks": int(ci.size), "batch": batch, "num_iter": it, "ms": t, "tflops": fl / t / 1e9,
+                   "frac_tensor_peak": fl / t / 1e9 / peak_tf, "max_abs_err_vs_oracle": err})
+        # (b) a large SpMM, streamed: n = 16384 (1024 x 1024 tiles), 1 % tiles,
+        # dense B 16384 x 256, FP16 in, FP32 out
+        nb, Nd = 1024, 256
+        rp, ci = oracle.bsr_pattern(nb, nb, 0.01, 1)
+        va = torch.tensor(rng.uniform(-1, 1, (len(ci), 16, 16)), dtype=torch.float16, device=dev)
+        A = api.BSR(torch.tensor(rp, device=dev), torch.tensor(ci, device=dev), va, nb)
+        for lay in ("row_kn", "ref_nk"):
+            Bd = torch.tensor(rng.uniform(-1, 1, (nb * 16, Nd) if lay == "row_kn" else (Nd, nb * 16)),
+                              dtype=torch.float16, device=dev)
+            C = torch.empty((nb * 16, Nd), dtype=torch.float32, device=dev)
+            ms = _time_ms(lambda: api.spmm(A, Bd, C, b_layout=lay), W, K_, flush)
+            t = min(ms)
+            fl = 2.0 * len(ci) * 256 * Nd
+            by = len(ci) * (512 + 4) + (nb + 1) * 4 + nb * 16 * Nd * 2 + nb * 16 * Nd * 4
+            rows = slice(0, 64 * 16)
+            ref = oracle.spmm(rp[:65], ci[: rp[64]], va[: rp[64]].double().cpu().numpy(), nb,
+                              Bd.double().cpu().numpy(), lay)
+            err = float(np.abs(C[rows].double().cpu().numpy() - ref).max())
+            _emit({"workload": "spmm", "case": f"n=16384, 1 % tiles, dense {Nd} columns, B {lay}",
+                   "nnz_blocks": int(len(ci)), "ms": t, "tflops": fl / t / 1e9, "hbm_gbs": by / t / 1e6,
+                   "frac_hbm": by / t / 1e6 / peak_bw, "max_abs_err_first_64_block_rows": err})
         return
 
     if args.workload == "bmm":

@@ -286,6 +286,62 @@ int kami_spgemm_bsr_numeric(kami_dtype_t in_type, kami_dtype_t out_type, int bsr
                             int64_t nnz_c, double alpha, double beta, int num_iter,
                             void *stream);
 
+/* ------------------------------------------------------------------------ */
+/* Block SpMM: BSR (16 x 16 tiles) times dense                              */
+/* ------------------------------------------------------------------------ */
+/*
+ * C (M x N, M = 16 mb) = alpha * num_iter * (A * op(B)) + beta * C, with A an
+ * mb x kb-block BSR matrix (row_ptr mb + 1 entries, col_idx, vals as
+ * row-major 16 x 16 tiles in entry order: vals[e*256 + r*16 + c]) and B
+ * dense: KAMI_B_REF_NK = N x K row-major (the reference's B, read as
+ * B[n*K + k] in block_spmm_1d_half_mma.cu:121-127, so C = A * B^T) or
+ * KAMI_B_ROW_KN = K x N row-major (C = A * B).  FP16 or BF16 tiles and B,
+ * FP32 accumulation, C in KAMI_F32, KAMI_F16 or KAMI_BF16.  batch problems
+ * at the given strides (a stride of 0 shares that operand, as the
+ * reference's 16384-CTA launch shares A, B and C); row_ptr entries index
+ * col_idx / vals of the same problem.  Replaces block_spmm_1d_half_mma
+ * (src/sparse/spmm/1d/block_spmm_1d_half_mma.cu:78, arguments bsr_rowptr,
+ * bsr_colidx, bsr_vals, B, C, alpha, beta; NUM_ITER -> num_iter).
+ * Block columns outside [0, kb) are skipped. */
+int kami_spmm_bsr(kami_dtype_t in_type, kami_dtype_t out_type, int bsr, int mb, int kb, int N,
+                  int64_t batch, const int *row_ptr, const int *col_idx,
+                  int64_t stride_row_ptr, int64_t stride_col_idx,
+                  const void *vals, int64_t stride_vals,
+                  const void *B, int64_t ldb, int64_t strideB, kami_b_layout_t b_layout,
+                  void *C, int64_t ldc, int64_t strideC,
+                  double alpha, double beta, int num_iter, void *stream);
+
+/* The same product with A in the reference's tiled-BSR form (built by
+ * bsr2tilebsr, src/sparse/spmm/2d/block_spmm_2d_half_mma.cu:264-293 and
+ * 3d/...:268-294): row tiles of tile_rows block-rows (the reference's
+ * NUMS_ROW) and column tiles of tile_cols block-columns (NUMS_COL);
+ * blk_row_ptr has (mb / tile_rows) * (kb / tile_cols) * tile_rows + 1
+ * entries, entry ((i * (kb / tile_cols) + j) * tile_rows + ii) starting
+ * block-row i * tile_rows + ii of column tile j; blk_col_idx is relative to
+ * the column tile; vals are tiles in blk entry order.  Replaces
+ * block_spmm_2d_half_mma (2d/...:72) and block_spmm_3d_half_mma
+ * (3d/...:73), whose argument order (blk_rowptr, blk_colidx, bsr_vals, B,
+ * C, alpha, beta) is kept; the 3D form's P partial C slices are reduced
+ * here (C is M x N). */
+int kami_spmm_tilebsr(kami_dtype_t in_type, kami_dtype_t out_type, int bsr, int mb, int kb, int N,
+                      int64_t batch, int tile_rows, int tile_cols,
+                      const int *blk_row_ptr, const int *blk_col_idx,
+                      int64_t stride_row_ptr, int64_t stride_col_idx,
+                      const void *vals, int64_t stride_vals,
+                      const void *B, int64_t ldb, int64_t strideB, kami_b_layout_t b_layout,
+                      void *C, int64_t ldc, int64_t strideC,
+                      double alpha, double beta, int num_iter, void *stream);
+
+/* Host conversion BSR -> tiled-BSR, the reference's bsr2tilebsr
+ * (2d/...:264-293) on host arrays: fills blk_row_ptr / blk_col_idx exactly
+ * as the reference does and, when perm is not NULL, perm[e] = the BSR entry
+ * that tiled entry e came from (the reference leaves the values in BSR
+ * order; gather vals through perm to multiply the same matrix).  Returns
+ * the number of entries (or a negative status). */
+int kami_bsr_to_tilebsr(int mb, int kb, int tile_rows, int tile_cols,
+                        const int *row_ptr, const int *col_idx,
+                        int *blk_row_ptr, int *blk_col_idx, int *perm);
+
 #ifdef __cplusplus
 }
 #endif

@@ -53,6 +53,11 @@ SIGNATURES = {
     "kami_spgemm_bsr_fill_colidx": ([_i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp], _i),
     "kami_spgemm_bsr_numeric": ([_i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64,
                                  _d, _d, _i, _vp], _i),
+    "kami_spmm_bsr": ([_i, _i, _i, _i, _i, _i, _i64, _vp, _vp, _i64, _i64, _vp, _i64,
+                       _vp, _i64, _i64, _i, _vp, _i64, _i64, _d, _d, _i, _vp], _i),
+    "kami_spmm_tilebsr": ([_i, _i, _i, _i, _i, _i, _i64, _i, _i, _vp, _vp, _i64, _i64, _vp, _i64,
+                           _vp, _i64, _i64, _i, _vp, _i64, _i64, _d, _d, _i, _vp], _i),
+    "kami_bsr_to_tilebsr": ([_i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp], _i),
 }
 
 

@@ -239,5 +239,90 @@ def spgemm(A: BSR, B: BSR, out_dtype=torch.float32, *, num_iter=1, stream=None) 
     return BSR(rpc, cic, vals, B.block_cols)
 
 
+def spmm(A: BSR, B: torch.Tensor, C: torch.Tensor | None = None, *, b_layout: str = "row_kn",
+         out_dtype=torch.float32, alpha: float = 1.0, beta: float = 0.0, num_iter: int = 1,
+         stream=None) -> torch.Tensor:
+    """Block SpMM (kami_spmm_bsr): C [16 mb, N] = A * B for a BSR matrix A and
+    a dense B, [K, N] (row_kn, torch's A @ B) or [N, K] (ref_nk, the
+    reference's layout: C = A * B^T).  FP16/BF16 operands, FP32 accumulation."""
+    K = A.block_cols * 16
+    if B.dim() != 2:
+        raise ValueError("B must be 2-D")
+    N = B.shape[1] if b_layout == "row_kn" else B.shape[0]
+    if (B.shape[0] if b_layout == "row_kn" else B.shape[1]) != K:
+        raise ValueError(f"B does not match K = {K}")
+    if B.stride(1) != 1:
+        B = B.contiguous()
+    if C is None:
+        C = torch.empty((A.block_rows * 16, N), dtype=out_dtype, device=B.device)
+    check(load().kami_spmm_bsr(_DT[A.values.dtype], _DT[C.dtype], 16, A.block_rows, A.block_cols, N, 1,
+                               A.row_ptr.data_ptr(), _ptr(A.col_idx), 0, 0, _ptr(A.values), 0,
+                               B.data_ptr(), _ld(B[None]), 0, _BL[b_layout], C.data_ptr(), _ld(C[None]), 0,
+                               float(alpha), float(beta), int(num_iter), _stream_ptr(stream)))
+    return C
+
+
+def spmm_batched(row_ptr: torch.Tensor, col_idx: torch.Tensor, values: torch.Tensor, block_cols: int,
+                 B: torch.Tensor, C: torch.Tensor | None = None, *, b_layout: str = "ref_nk",
+                 out_dtype=torch.float32, alpha: float = 1.0, beta: float = 0.0, num_iter: int = 1,
+                 tile_rows: int = 0, tile_cols: int = 0, stream=None) -> torch.Tensor:
+    """Batched block SpMM (kami_spmm_bsr / kami_spmm_tilebsr).  row_ptr
+    [batch, rows+1] or [rows+1] (shared), col_idx [batch, e] or [e], values
+    [batch, e, 16, 16] or [e, 16, 16]; B [batch, N, K] (ref_nk) or
+    [batch, K, N] (row_kn), or 2-D (shared); the batch is the largest
+    leading dimension among them and C [batch, 16 rows, N] (when given), so
+    fully shared operands with a batched C repeat one problem, as the
+    reference's 16384-CTA launch does.  tile_rows / tile_cols > 0 select the
+    reference's tiled-BSR index form."""
+    def _b(t, nd):
+        return (t.shape[0], t.stride(0)) if t.dim() == nd else (1, 0)
+    nb_r, s_r = _b(row_ptr, 2)
+    nb_c, s_c = _b(col_idx, 2)
+    nb_v, s_v = _b(values, 4)
+    nb_b, s_b = _b(B, 3)
+    batch = max(nb_r, nb_c, nb_v, nb_b, C.shape[0] if C is not None and C.dim() == 3 else 1)
+    if not (tile_rows and tile_cols):
+        tile_rows = tile_cols = 0
+    mb = row_ptr.shape[-1] - 1
+    B2 = B if B.dim() == 2 else B[0]
+    N = B2.shape[0] if b_layout == "ref_nk" else B2.shape[1]
+    if tile_rows:
+        nct = block_cols // tile_cols
+        mb = (row_ptr.shape[-1] - 1) // nct
+    if C is None:
+        C = torch.empty((batch, mb * 16, N), dtype=out_dtype, device=B.device)
+    s_cc = _bs(C) if C.dim() == 3 else 0
+    ldc = _ld(C if C.dim() == 3 else C[None])
+    ldb = _ld(B if B.dim() == 3 else B[None])
+    L = load()
+    common_tail = (_ptr(values), s_v, B.data_ptr(), ldb, s_b, _BL[b_layout], C.data_ptr(), ldc, s_cc,
+                   float(alpha), float(beta), int(num_iter), _stream_ptr(stream))
+    if tile_rows:
+        check(L.kami_spmm_tilebsr(_DT[values.dtype], _DT[C.dtype], 16, mb, block_cols, N, batch, tile_rows,
+                                  tile_cols, row_ptr.data_ptr(), _ptr(col_idx), s_r, s_c, *common_tail))
+    else:
+        check(L.kami_spmm_bsr(_DT[values.dtype], _DT[C.dtype], 16, mb, block_cols, N, batch,
+                              row_ptr.data_ptr(), _ptr(col_idx), s_r, s_c, *common_tail))
+    return C
+
+
+def bsr_to_tilebsr(row_ptr, col_idx, block_cols: int, tile_rows: int, tile_cols: int):
+    """The reference's bsr2tilebsr on host arrays (numpy int32): returns
+    (blk_row_ptr, blk_col_idx, perm) with perm[e] = the BSR entry of tiled
+    entry e."""
+    import numpy as np
+    rp = np.ascontiguousarray(row_ptr, dtype=np.int32)
+    ci = np.ascontiguousarray(col_idx, dtype=np.int32)
+    mb = rp.size - 1
+    nct = block_cols // tile_cols
+    brp = np.zeros((mb // tile_rows) * nct * tile_rows + 1, dtype=np.int32)
+    bci = np.zeros(max(ci.size, 1), dtype=np.int32)
+    perm = np.zeros(max(ci.size, 1), dtype=np.int32)
+    n = load().kami_bsr_to_tilebsr(mb, block_cols, tile_rows, tile_cols, rp.ctypes.data, ci.ctypes.data,
+                                   brp.ctypes.data, bci.ctypes.data, perm.ctypes.data)
+    check(n if n < 0 else 0)
+    return brp, bci[:n], perm[:n]
+
+
 def _ptr(t: torch.Tensor) -> int:
     return t.data_ptr() if t.numel() else 0

@@ -19,6 +19,7 @@
  *   src/block_gemm/KAMI/1d/fp16/block_gemm_1d_half_mma.cu
  *   src/block_gemm/KAMI/3d/fp16/block_gemm_3d_half_mma.cu
  *   src/sparse/spgemm/2d/block_spgemm_2d_half_mma.cu
+ *   src/sparse/spmm/{1d,2d,3d}/block_spmm_{1d,2d,3d}_half_mma.cu
  */
 #define _GNU_SOURCE
 #include <stdint.h>
@@ -76,13 +77,16 @@ void kami_oracle_fill_rand_r_mod(double *x, int64_t n, int mod)
     }
 }
 
-/* Block-BSR generator of block_spgemm_2d_half_mma.cu:648-673: srand(0), then
- * one rand() per block position (kept when rand()/RAND_MAX > sparsity) and
- * BSR_M*BSR_K values rand()%3+1 per kept block, row by row.  Values are
- * written as binary16 bits.  Returns the number of nonzero blocks. */
-int kami_oracle_bsr_generate(int rows, int cols, float sparsity, int bsr_m,
-                             int bsr_k, int *row_ptr, int *col_idx,
-                             uint16_t *values)
+/* Block-BSR generator shared by the reference's sparse programs: srand(0),
+ * then one rand() per block position (kept when rand()/RAND_MAX > sparsity)
+ * and BSR_M*BSR_K values rand() % mod + add per kept block, row by row:
+ *   block_spgemm_2d_half_mma.cu:648-673   rand() % 3 + 1
+ *   spmm/1d/block_spmm_1d_half_mma.cu:197-222   rand() % 3
+ *   spmm/2d/...:236-262, spmm/3d/...:241-266   rand() % 2 + 1
+ * Values are written as binary16 bits.  Returns the number of nonzero
+ * blocks. */
+int kami_oracle_bsr_generate_rule(int rows, int cols, float sparsity, int bsr_m, int bsr_k, int mod, int add,
+                                  int *row_ptr, int *col_idx, uint16_t *values)
 {
     int count = 0;
     srand(0);
@@ -96,13 +100,20 @@ int kami_oracle_bsr_generate(int rows, int cols, float sparsity, int bsr_m,
             {
                 col_idx[count] = j;
                 for (int len = 0; len < bsr_m * bsr_k; len++)
-                    values[(int64_t)count * bsr_m * bsr_k + len] = d2h((double)(rand() % 3) + 1.0);
+                    values[(int64_t)count * bsr_m * bsr_k + len] = d2h((double)(rand() % mod) + (double)add);
                 count++;
             }
         }
         row_ptr[i + 1] = count;
     }
     return count;
+}
+
+int kami_oracle_bsr_generate(int rows, int cols, float sparsity, int bsr_m,
+                             int bsr_k, int *row_ptr, int *col_idx,
+                             uint16_t *values)
+{
+    return kami_oracle_bsr_generate_rule(rows, cols, sparsity, bsr_m, bsr_k, 3, 1, row_ptr, col_idx, values);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -435,4 +446,75 @@ int kami_oracle_bsr_pattern(int rows, int cols, double density, uint64_t seed,
         row_ptr[i + 1] = count;
     }
     return count;
+}
+
+/* ------------------------------------------------------------------------ */
+/* block SpMM (BSR or tiled-BSR A, dense B)                                 */
+/* ------------------------------------------------------------------------ */
+
+/* bsr2tilebsr of spmm/2d/block_spmm_2d_half_mma.cu:264-293 (the same code
+ * in spmm/3d/...:268-294): for each row tile i (row_tiles of them, tile_rows
+ * block-rows each), each column tile j (tile_cols block-columns), each
+ * block-row ii of the tile: the entries of BSR row i*tile_rows + ii whose
+ * column falls in tile j, column kept relative to the tile.  Returns the
+ * number of entries. */
+int kami_oracle_bsr2tilebsr(int row_tiles, int tile_rows, int cols, int tile_cols, const int *bsr_rowptr,
+                            const int *bsr_colidx, int *blk_rowptr, int *blk_colidx)
+{
+    int count = 0;
+    blk_rowptr[0] = 0;
+    for (int i = 0; i < row_tiles; i++)
+        for (int j = 0; j < cols / tile_cols; j++)
+        {
+            int start = j * tile_cols, end = (j + 1) * tile_cols;
+            for (int ii = 0; ii < tile_rows; ii++)
+            {
+                for (int jj = bsr_rowptr[i * tile_rows + ii]; jj < bsr_rowptr[i * tile_rows + ii + 1]; jj++)
+                {
+                    int col = bsr_colidx[jj];
+                    if (col >= start && col < end)
+                        blk_colidx[count++] = col % tile_cols;
+                }
+                blk_rowptr[i * tile_rows * (cols / tile_cols) + j * tile_rows + ii + 1] = count;
+            }
+        }
+    return count;
+}
+
+/* Host check of the block SpMM programs, in their loop order and with a
+ * double accumulator: for each row tile i, column tile j, block-row ii of
+ * the tile and entry jj, C[(row) * ldc + n] += a[r*16 + c] * B(n, k)
+ * (spmm/1d/...:305-326 for plain BSR, which is tile_rows = 1 and one column
+ * tile; spmm/2d/...:385-408 and 3d/...:398-419 for the tiled form).  vals
+ * are the tiles as doubles; B(n, k) = B[n*ldb + k] (b_layout 0, the
+ * reference's N x K) or B[k*ldb + n] (b_layout 1, K x N).  C is zeroed
+ * first (mb*16 x N, row stride ldc). */
+void kami_oracle_spmm(int mb, int kb, int N, int tile_rows, int tile_cols, const int *rowptr, const int *colidx,
+                      const double *vals, const double *B, int64_t ldb, int b_layout, double *C, int64_t ldc)
+{
+    const int ntiles = tile_cols > 0 ? kb / tile_cols : 1;
+    const int tc = tile_cols > 0 ? tile_cols : 0;
+    for (int r = 0; r < mb * 16; r++)
+        for (int n = 0; n < N; n++)
+            C[(int64_t)r * ldc + n] = 0.0;
+    for (int i = 0; i < mb / tile_rows; i++)
+        for (int j = 0; j < ntiles; j++)
+            for (int ii = 0; ii < tile_rows; ii++)
+            {
+                int q = i * tile_rows * ntiles + j * tile_rows + ii;
+                for (int jj = rowptr[q]; jj < rowptr[q + 1]; jj++)
+                {
+                    int col = colidx[jj] + j * tc;
+                    const double *a = vals + (int64_t)jj * 256;
+                    for (int iii = 0; iii < 16; iii++)
+                        for (int jjj = 0; jjj < 16; jjj++)
+                        {
+                            int k = col * 16 + jjj;
+                            double av = a[iii * 16 + jjj];
+                            double *crow = C + (int64_t)((i * tile_rows + ii) * 16 + iii) * ldc;
+                            for (int n = 0; n < N; n++)
+                                crow[n] += av * (b_layout == 0 ? B[(int64_t)n * ldb + k] : B[(int64_t)k * ldb + n]);
+                        }
+                }
+            }
 }

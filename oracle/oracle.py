@@ -52,6 +52,12 @@ def lib():
         L.kami_oracle_fill_rand_r_mod.argtypes = [_dp, _i64, _i32]
         L.kami_oracle_bsr_generate.argtypes = [_i32, _i32, ctypes.c_float, _i32, _i32, _ip, _ip, _u16p]
         L.kami_oracle_bsr_generate.restype = _i32
+        L.kami_oracle_bsr_generate_rule.argtypes = [_i32, _i32, ctypes.c_float, _i32, _i32, _i32, _i32, _ip, _ip,
+                                                    _u16p]
+        L.kami_oracle_bsr_generate_rule.restype = _i32
+        L.kami_oracle_bsr2tilebsr.argtypes = [_i32, _i32, _i32, _i32, _ip, _ip, _ip, _ip]
+        L.kami_oracle_bsr2tilebsr.restype = _i32
+        L.kami_oracle_spmm.argtypes = [_i32, _i32, _i32, _i32, _i32, _ip, _ip, _dp, _dp, _i64, _i32, _dp, _i64]
         L.kami_oracle_gemm_f64.argtypes = [_i64, _i32, _i32, _i32, _dp, _i64, _i64, _dp, _i64, _i64, _i32,
                                            _dp, _i64, _i64]
         L.kami_oracle_gemm_h16.argtypes = [_i64, _i32, _i32, _i32, _u16p, _i64, _i64, _u16p, _i64, _i64, _i32,
@@ -88,15 +94,64 @@ def fill_rand_r_mod(n: int, mod: int = 3) -> np.ndarray:
     return x
 
 
-def bsr_generate(rows: int, cols: int, sparsity: float, bsr: int = 16):
-    """generate_random_bsr_matrix (block_spgemm_2d_half_mma.cu:648-673):
-    returns (row_ptr int32, col_idx int32, values float16 [nnz, bsr, bsr])."""
+# value rules of the reference's generate_random_bsr_matrix copies
+BSR_RULES = {
+    "spgemm": (3, 1),  # block_spgemm_2d_half_mma.cu:648-673: rand() % 3 + 1
+    "spmm1d": (3, 0),  # spmm/1d/block_spmm_1d_half_mma.cu:197-222: rand() % 3
+    "spmm2d": (2, 1),  # spmm/2d/...:236-262 and spmm/3d/...:241-266: rand() % 2 + 1
+}
+
+
+def bsr_generate(rows: int, cols: int, sparsity: float, bsr: int = 16, rule: str = "spgemm"):
+    """generate_random_bsr_matrix of the reference's sparse programs (srand(0),
+    one rand() per block position, values by `rule`): returns (row_ptr int32,
+    col_idx int32, values float16 [nnz, bsr, bsr])."""
+    mod, add = BSR_RULES[rule]
     row_ptr = np.zeros(rows + 1, dtype=np.int32)
     col_idx = np.zeros(max(rows * cols, 1), dtype=np.int32)
     vals = np.zeros(max(rows * cols, 1) * bsr * bsr, dtype=np.uint16)
-    nnz = lib().kami_oracle_bsr_generate(rows, cols, sparsity, bsr, bsr, _p(row_ptr, _ip), _p(col_idx, _ip),
-                                         _p(vals, _u16p))
+    nnz = lib().kami_oracle_bsr_generate_rule(rows, cols, sparsity, bsr, bsr, mod, add, _p(row_ptr, _ip),
+                                              _p(col_idx, _ip), _p(vals, _u16p))
     return row_ptr, col_idx[:nnz].copy(), vals[: nnz * bsr * bsr].view(np.float16).reshape(nnz, bsr, bsr).copy()
+
+
+def bsr2tilebsr(row_ptr, col_idx, cols: int, row_tiles: int, tile_cols: int):
+    """bsr2tilebsr (spmm/2d/block_spmm_2d_half_mma.cu:264-293): returns
+    (blk_row_ptr, blk_col_idx) for row_tiles row tiles of
+    (rows / row_tiles) block-rows and column tiles of tile_cols columns."""
+    rp = np.ascontiguousarray(row_ptr, dtype=np.int32)
+    ci = np.ascontiguousarray(col_idx, dtype=np.int32)
+    rows = rp.size - 1
+    tile_rows = rows // row_tiles
+    brp = np.zeros(row_tiles * (cols // tile_cols) * tile_rows + 1, dtype=np.int32)
+    bci = np.zeros(max(ci.size, 1), dtype=np.int32)
+    if ci.size == 0:
+        ci = np.zeros(1, dtype=np.int32)
+    n = lib().kami_oracle_bsr2tilebsr(row_tiles, tile_rows, cols, tile_cols, _p(rp, _ip), _p(ci, _ip),
+                                      _p(brp, _ip), _p(bci, _ip))
+    return brp, bci[:n].copy()
+
+
+def spmm(row_ptr, col_idx, values, block_cols: int, B, b_layout: str = "ref_nk", tile_rows: int = 1,
+         tile_cols: int = 0) -> np.ndarray:
+    """Host check of the block SpMM programs (spmm/1d/...:305-326; tiled form
+    spmm/2d/...:385-408): C [16 rows, N] in double, values as given (tiles in
+    entry order), B [N, K] (ref_nk) or [K, N] (row_kn)."""
+    rp = np.ascontiguousarray(row_ptr, dtype=np.int32)
+    ci = np.ascontiguousarray(col_idx, dtype=np.int32)
+    if ci.size == 0:
+        ci = np.zeros(1, dtype=np.int32)
+    v = np.ascontiguousarray(np.asarray(values, dtype=np.float64).reshape(-1))
+    if v.size == 0:
+        v = np.zeros(256)
+    Bd = np.ascontiguousarray(np.asarray(B, dtype=np.float64))
+    N = Bd.shape[0] if b_layout == "ref_nk" else Bd.shape[1]
+    ntiles = block_cols // tile_cols if tile_cols else 1
+    mb = (rp.size - 1) // ntiles
+    C = np.zeros((mb * 16, N))
+    lib().kami_oracle_spmm(mb, block_cols, N, tile_rows, tile_cols, _p(rp, _ip), _p(ci, _ip), _p(v, _dp),
+                           _p(Bd, _dp), Bd.shape[1], 0 if b_layout == "ref_nk" else 1, _p(C, _dp), N)
+    return C
 
 
 def bsr_pattern(rows: int, cols: int, density: float, seed: int):
@@ -249,6 +304,15 @@ def ref_lib(name: str):
         L.kami_ref_launch.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _i32]
         L.kami_ref_launch.restype = _i32
         L.kami_ref_config.argtypes = [_ip]
+    if hasattr(L, "kami_ref_spmm_launch"):
+        L.kami_ref_spmm_launch.argtypes = [ctypes.c_void_p] * 5 + [_i32]
+        L.kami_ref_spmm_launch.restype = _i32
+        L.kami_ref_spmm_config.argtypes = [_ip]
+        L.kami_ref_bsr_generate.argtypes = [_i32, _i32, ctypes.c_float, _ip, _ip, _u16p]
+        L.kami_ref_bsr_generate.restype = _i32
+        L.kami_ref_bsr_size.restype = _i32
+        if hasattr(L, "kami_ref_bsr2tilebsr"):
+            L.kami_ref_bsr2tilebsr.argtypes = [_i32, _i32, _i32, _ip, _ip, _ip, _ip]
     if hasattr(L, "kami_ref_spgemm_spa"):
         L.kami_ref_bsr_generate.argtypes = [_i32, _i32, ctypes.c_float, _ip, _ip, _u16p]
         L.kami_ref_bsr_generate.restype = _i32
@@ -263,6 +327,27 @@ def ref_config(L) -> dict:
     L.kami_ref_config(cfg)
     keys = ["M", "N", "K", "P", "num_iter", "threads", "slices", "smem"]
     return dict(zip(keys, list(cfg)))
+
+
+def ref_spmm_config(L) -> dict:
+    cfg = (ctypes.c_int * 9)()
+    L.kami_ref_spmm_config(cfg)
+    keys = ["M", "N", "K", "P", "num_iter", "threads", "slices", "tile_rows", "tile_cols"]
+    return dict(zip(keys, list(cfg)))
+
+
+def ref_bsr2tilebsr(L, row_ptr, col_idx, cols: int, row_tiles: int, tile_cols: int):
+    """The reference's own bsr2tilebsr (compiled from its 2D/3D SpMM file)."""
+    rp = np.ascontiguousarray(row_ptr, dtype=np.int32)
+    ci = np.ascontiguousarray(col_idx, dtype=np.int32)
+    rows = rp.size - 1
+    tile_rows = rows // row_tiles
+    brp = np.zeros(row_tiles * (cols // tile_cols) * tile_rows + 1, dtype=np.int32)
+    bci = np.zeros(max(ci.size, 1), dtype=np.int32)
+    if ci.size == 0:
+        ci = np.zeros(1, dtype=np.int32)
+    L.kami_ref_bsr2tilebsr(rows, cols, int(rp[-1]) * 256, _p(rp, _ip), _p(ci, _ip), _p(brp, _ip), _p(bci, _ip))
+    return brp, bci[: int(brp[-1])].copy()
 
 
 def ref_bsr_generate(L, rows, cols, sparsity):

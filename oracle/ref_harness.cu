@@ -14,7 +14,10 @@
 //     the file's own dynamic shared-memory size and block size
 //     (the launch of batched_gemm_2d_double_mma.cu:303-307 and friends);
 //   * KAMI_REF_SPGEMM_HOST set: the host functions generate_random_bsr_matrix
-//     and spgemm_spa of the block SpGEMM files (CPU only).
+//     and spgemm_spa of the block SpGEMM files (CPU only);
+//   * KAMI_REF_SPMM set: a launcher for the block SpMM kernel of that file
+//     (block_spmm_{1d,2d,3d}_half_mma) with the file's own launch geometry,
+//     plus its generate_random_bsr_matrix and (2D/3D) bsr2tilebsr.
 // Oracle/Makefile.ref lists the variants and their -D macros.
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -23,14 +26,14 @@
 #include KAMI_REF_SOURCE
 #undef main
 
+#ifndef KAMI_REF_SLICES
+#define KAMI_REF_SLICES 1
+#endif
+
 #if defined(KAMI_REF_KERNEL)
 
 #ifndef KAMI_REF_T
 #error "KAMI_REF_T (the element type of the kernel) must be defined"
-#endif
-
-#ifndef KAMI_REF_SLICES
-#define KAMI_REF_SLICES 1
 #endif
 
 extern "C" int kami_ref_launch(const void *A, const void *B, void *C, int grid)
@@ -93,6 +96,63 @@ extern "C" int kami_ref_spgemm_spa(int mA, int nA, const int *RowPtrA, const int
 
 extern "C" int kami_ref_bsr_size(void) { return BSR_M; }
 
+#elif defined(KAMI_REF_SPMM)
+
+// The file's kernel on its own launch geometry (e.g. spmm/1d/...:283-285):
+// index arrays as the kernel takes them (BSR for 1D, tiled BSR for 2D/3D).
+extern "C" int kami_ref_spmm_launch(const int *rowptr, const int *colidx, const void *vals, const void *B, void *C,
+                                    int grid)
+{
+    cudaError_t e =
+        cudaFuncSetAttribute(KAMI_REF_SPMM, cudaFuncAttributeMaxDynamicSharedMemorySize, shmem_size_block_spmm);
+    if (e != cudaSuccess)
+        return (int)e;
+    KAMI_REF_SPMM<<<grid, KAMI_REF_SPMM_THREADS, shmem_size_block_spmm>>>(
+        rowptr, colidx, (const half *)vals, (const half *)B, (half *)C, (half)1.0, (half)0.0);
+    e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return (int)e;
+    return (int)cudaDeviceSynchronize();
+}
+
+// {M, N, K, P, NUM_ITER, threads per block, C slices, tile rows, tile cols}
+extern "C" void kami_ref_spmm_config(int *cfg)
+{
+    cfg[0] = M_BLOCK;
+    cfg[1] = N_BLOCK;
+    cfg[2] = K_BLOCK;
+    cfg[3] = NUM_RANK_BLOCK;
+    cfg[4] = NUM_ITER;
+    cfg[5] = KAMI_REF_SPMM_THREADS;
+    cfg[6] = KAMI_REF_SLICES;
+#ifdef NUMS_ROW
+    cfg[7] = NUMS_ROW;
+    cfg[8] = NUMS_COL;
 #else
-#error "define KAMI_REF_KERNEL or KAMI_REF_SPGEMM_HOST"
+    cfg[7] = 0;
+    cfg[8] = 0;
+#endif
+}
+
+extern "C" int kami_ref_bsr_generate(int rows, int cols, float sparsity, int *row_ptr, int *col_idx,
+                                     uint16_t *values)
+{
+    int nnz = 0;
+    generate_random_bsr_matrix(rows, cols, sparsity, row_ptr, col_idx, reinterpret_cast<half *>(values), &nnz);
+    return nnz / (BSR_M * BSR_K);
+}
+
+extern "C" int kami_ref_bsr_size(void) { return BSR_M; }
+
+#ifdef NUMS_ROW
+extern "C" void kami_ref_bsr2tilebsr(int rows, int cols, int bsr_nnz, const int *bsr_rowptr, const int *bsr_colidx,
+                                     int *blk_rowptr, int *blk_colidx)
+{
+    bsr2tilebsr(rows, cols, bsr_nnz, 0.5f, const_cast<int *>(bsr_rowptr), const_cast<int *>(bsr_colidx), blk_rowptr,
+                blk_colidx);
+}
+#endif
+
+#else
+#error "define KAMI_REF_KERNEL, KAMI_REF_SPGEMM_HOST or KAMI_REF_SPMM"
 #endif

@@ -7,7 +7,7 @@ import re
 
 import pytest
 
-from kami_b200 import _lib
+from kami_b200 import _lib, api
 from kami_b200._lib import KamiError
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -79,3 +79,44 @@ def test_describe_is_host_only():
     assert d["problems_per_cta"] == 4 and d["grid"] == 250
     with pytest.raises(KamiError):
         api.describe(200, 200, 200, 1, torch.float16, variant="mma_sync")
+
+
+def _spmm(**kw):
+    a = dict(it=_lib.F16, ot=_lib.F32, bsr=16, mb=4, kb=4, N=64, batch=1, rp=16, ci=16, srp=0, sci=0, v=16, sv=0,
+             B=16, ldb=64, sB=0, bl=0, C=16, ldc=64, sC=0, alpha=1.0, beta=0.0, iters=1)
+    a.update(kw)
+    return _lib.load().kami_spmm_bsr(a["it"], a["ot"], a["bsr"], a["mb"], a["kb"], a["N"], a["batch"], a["rp"],
+                                     a["ci"], a["srp"], a["sci"], a["v"], a["sv"], a["B"], a["ldb"], a["sB"],
+                                     a["bl"], a["C"], a["ldc"], a["sC"], a["alpha"], a["beta"], a["iters"], None)
+
+
+@pytest.mark.parametrize("kw,status", [
+    (dict(batch=0), 0),
+    (dict(N=0), 0),
+    (dict(bsr=32), -2),
+    (dict(it=_lib.F64), -2),
+    (dict(ot=_lib.F64), -2),
+    (dict(kb=0), -1),
+    (dict(iters=0), -1),
+    (dict(v=None), -1),
+    (dict(v=18), -3),
+    (dict(ldb=63), -1),
+    (dict(bl=1, ldb=32), -1),
+    (dict(ldc=8), -1),
+])
+def test_spmm_host_validation(kw, status):
+    """Rejected before any launch (no GPU needed)."""
+    assert _spmm(**kw) == status
+
+
+def test_bsr_to_tilebsr_host_conversion():
+    import numpy as np
+    rp = np.array([0, 2, 3, 3, 5], dtype=np.int32)
+    ci = np.array([0, 3, 2, 1, 2], dtype=np.int32)
+    brp, bci, perm = api.bsr_to_tilebsr(rp, ci, 4, 2, 2)
+    # row tile 0 (rows 0, 1): column tile 0 holds (0,0); tile 1 holds (0,3), (1,2)
+    assert brp.tolist() == [0, 1, 1, 2, 3, 3, 4, 4, 5]
+    assert bci.tolist() == [0, 1, 0, 1, 0]
+    assert perm.tolist() == [0, 1, 2, 3, 4]
+    with pytest.raises(Exception):
+        api.bsr_to_tilebsr(rp, ci, 4, 3, 2)

@@ -135,3 +135,58 @@ def test_double_double_against_mpmath():
             got = mpmath.mpf(hi[0, i, j]) + mpmath.mpf(lo[0, i, j])
             scale = mpmath.fsum(abs(mpmath.mpf(a) * mpmath.mpf(b)) for a, b in zip(A[0, i], B[0, j]))
             assert abs(got - exact) <= scale * mpmath.mpf(2) ** -100
+
+
+# --------------------------------------------------------------------------
+# block SpMM
+# --------------------------------------------------------------------------
+
+def _spmm_cases():
+    return sorted(glob.glob(os.path.join(GOLDEN, "spmm_*.npz")))
+
+
+@pytest.mark.parametrize("path", _spmm_cases(), ids=os.path.basename)
+def test_spmm_oracle_matches_reference_kernel_golden(path):
+    """The restated SpMM host check reproduces the outputs of the
+    reference's own block_spmm_{1d,2d,3d}_half_mma kernels (exact small
+    integers; tiled-BSR indices for 2D / 3D)."""
+    g = np.load(path)
+    M, N, K, P, tile_rows, tile_cols, _ = (int(x) for x in g["cfg"])
+    C = oracle.spmm(g["row_ptr"], g["col_idx"], g["vals"].astype(np.float64), K // 16, g["B"].astype(np.float64),
+                    "ref_nk", tile_rows=tile_rows, tile_cols=tile_cols)
+    assert np.array_equal(C, g["C"])
+
+
+@pytest.mark.parametrize("lib,rule", [("spmm1d_64p4", "spmm1d"), ("spmm2d_64p2", "spmm2d"),
+                                      ("spmm3d_64p2", "spmm2d")])
+@pytest.mark.parametrize("rows,cols,sp", [(4, 4, 0.5), (8, 6, 0.3), (6, 8, 0.9)])
+def test_spmm_generator_and_tiling_match_reference_library(lib, rule, rows, cols, sp):
+    if not oracle.ref_available(lib):
+        pytest.skip("oracle/_ref not built")
+    L = oracle.ref_lib(lib)
+    a = oracle.ref_bsr_generate(L, rows, cols, sp)
+    b = oracle.bsr_generate(rows, cols, sp, rule=rule)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+    cfg = oracle.ref_spmm_config(L)
+    if cfg["tile_rows"] and (rows, cols) == (cfg["M"] // 16, cfg["K"] // 16):
+        # bsr2tilebsr tiles with its compile-time geometry (BSR_ROWS, BSR_COLS,
+        # NUMS_ROW, NUMS_COL), so it is compared at the compiled shape only
+        r1 = oracle.ref_bsr2tilebsr(L, a[0], a[1], cols, cfg["P"], cfg["tile_cols"])
+        r2 = oracle.bsr2tilebsr(a[0], a[1], cols, cfg["P"], cfg["tile_cols"])
+        for x, y in zip(r1, r2):
+            assert np.array_equal(x, y)
+
+
+def test_spmm_oracle_against_numpy():
+    rng = np.random.default_rng(5)
+    rp, ci = oracle.bsr_pattern(6, 5, 0.4, 11)
+    vals = rng.uniform(-1, 1, (ci.size, 16, 16))
+    dense = np.zeros((96, 80))
+    for r in range(6):
+        for e in range(rp[r], rp[r + 1]):
+            dense[16 * r:16 * r + 16, 16 * ci[e]:16 * ci[e] + 16] = vals[e]
+    B = rng.uniform(-1, 1, (80, 33))
+    assert np.allclose(oracle.spmm(rp, ci, vals, 5, B, "row_kn"), dense @ B, rtol=0, atol=1e-12)
+    assert np.allclose(oracle.spmm(rp, ci, vals, 5, np.ascontiguousarray(B.T), "ref_nk"), dense @ B, rtol=0,
+                       atol=1e-12)
