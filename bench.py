@@ -445,12 +445,14 @@ def run_secondary(args):
             _emit({"workload": "split", "kernel": "native-fp64 (DMMA mma.sync)", "num_iter": it, "ms": t,
                    "tflops_fp64_equiv": fl1 * it / t / 1e9, "hbm_gbs": by / t / 1e6, "normwise_err_dd": e_nat})
             for s_, sdt in [(3, torch.float16), (4, torch.float16), (5, torch.float16), (6, torch.float16),
-                            (7, torch.float16), (8, torch.bfloat16)]:
+                            (7, torch.float16), (8, torch.bfloat16), (6, torch.int8), (7, torch.int8),
+                            (8, torch.int8)]:
                 ms = _time_ms(lambda: api.split_f64_gemm(A, B, C, nslices=s_, slice_dtype=sdt, num_iter=it),
                               W, K_, flush)
                 e = oracle.normwise_error_dd(C[:sub].cpu().numpy() / it, hi, lo) if it == 1 else None
                 t = min(ms)
-                _emit({"workload": "split", "kernel": f"split {s_} x {'bf16' if sdt == torch.bfloat16 else 'fp16'}",
+                sname = {torch.bfloat16: "bf16", torch.float16: "fp16", torch.int8: "int8"}[sdt]
+                _emit({"workload": "split", "kernel": f"split {s_} x {sname}",
                        "num_iter": it, "ms": t, "tflops_fp64_equiv": fl1 * it / t / 1e9,
                        "hbm_gbs": by / t / 1e6, "normwise_err_dd": e})
         return

@@ -52,7 +52,8 @@ typedef enum kami_dtype {
     KAMI_F16 = 0,
     KAMI_BF16 = 1,
     KAMI_F64 = 2,
-    KAMI_F32 = 3
+    KAMI_F32 = 3,
+    KAMI_S8 = 4 /* signed 8-bit integer: digit slices of kami_split_f64_gemm_batched only */
 } kami_dtype_t;
 
 typedef enum kami_partition {
@@ -219,16 +220,17 @@ int kami_gemm_grouped_noalloc(kami_dtype_t in_type, kami_dtype_t out_type, int c
                               double alpha, double beta, int num_iter, void *stream);
 
 /* ------------------------------------------------------------------------ */
-/* FP64-accurate batched GEMM on the FP16/BF16 tensor cores                 */
+/* FP64-accurate batched GEMM on the FP16/BF16/INT8 tensor cores            */
 /* ------------------------------------------------------------------------ */
 /*
  * C[b] = alpha * A[b] * op(B[b]) + beta * C[b] in FP64, M, N, K <= 64, computed
  * by splitting each row of A and each column of op(B) into `nslices` exact
- * integer digits (power-of-two row/column scaling; 9-bit digits in binary16
- * or 7-bit digits in bfloat16), multiplying digit pairs on the tensor cores
- * with exact FP32 accumulation, and recombining in FP64.  FP64 arithmetic is
- * used only for scaling/splitting and recombination.  nslices: 2..7
- * (KAMI_F16) or 2..8 (KAMI_BF16).  A is M x K row-major; B is N x K
+ * integer digits (power-of-two row/column scaling; 9-bit digits in binary16,
+ * 7-bit digits in bfloat16 or 8-bit digits in int8), multiplying digit pairs
+ * on the tensor cores with exact accumulation (FP32 for the 16-bit digits,
+ * INT32 for int8), and recombining in FP64.  FP64 arithmetic is used only for
+ * the recombination.  nslices: 2..7 (KAMI_F16), 2..8 (KAMI_BF16) or 2..8
+ * (KAMI_S8; 8 int8 digits carry 62 bits).  A is M x K row-major; B is N x K
  * (KAMI_B_REF_NK) or K x N (KAMI_B_ROW_KN).  No counterpart in the
  * reference; its FP64 comparator is kami_gemm_batched with in_type KAMI_F64
  * (batched_gemm_{1d,2d,3d}_double_mma.cu).  num_iter repeats the tensor-core

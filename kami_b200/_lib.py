@@ -13,7 +13,7 @@ LIB_PATH = os.path.join(HERE, "libkami_b200.so")
 
 # enums of include/kami.h
 KAMI_OK = 0
-F16, BF16, F64, F32 = 0, 1, 2, 3
+F16, BF16, F64, F32, S8 = 0, 1, 2, 3, 4
 PARTITION_AUTO, PARTITION_1D, PARTITION_2D, PARTITION_3D = 0, 1, 2, 3
 VARIANT_AUTO, VARIANT_MMA_SYNC, VARIANT_TCGEN05, VARIANT_TCGEN05_TS = 0, 1, 2, 3
 A_ROW_MK, A_COL_MK = 0, 1

@@ -160,9 +160,11 @@ class GroupedPlan:
 def split_f64_gemm(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = None, *, nslices: int = 6,
                    slice_dtype=torch.float16, b_layout: str = "ref_nk", alpha: float = 1.0, beta: float = 0.0,
                    num_iter: int = 1, stream=None) -> torch.Tensor:
-    """FP64 C = A op(B) via exact FP16/BF16 digit slices on the tensor cores
-    (kami_split_f64_gemm_batched).  A: [batch, M, K] float64; B: [batch, N, K]
-    (ref_nk) or [batch, K, N] (row_kn)."""
+    """FP64 C = A op(B) via exact digit slices on the tensor cores
+    (kami_split_f64_gemm_batched): slice_dtype torch.float16 (2-7 slices),
+    torch.bfloat16 (2-8) or torch.int8 (2-8; 8 slices carry 62 bits).
+    A: [batch, M, K] float64; B: [batch, N, K] (ref_nk) or [batch, K, N]
+    (row_kn)."""
     squeeze = A.dim() == 2
     A3, B3 = _as3(A), _as3(B)
     if A3.dtype != torch.float64 or B3.dtype != torch.float64:
@@ -173,7 +175,8 @@ def split_f64_gemm(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = No
     N = B3.shape[1] if b_layout == "ref_nk" else B3.shape[2]
     C3 = torch.empty((batch, M, N), dtype=torch.float64, device=A3.device) if C is None else _as3(C)
     check(load().kami_split_f64_gemm_batched(
-        int(nslices), _DT[slice_dtype], M, N, K, batch, A3.data_ptr(), _ld(A3), _bs(A3),
+        int(nslices), _lib.S8 if slice_dtype == torch.int8 else _DT[slice_dtype], M, N, K, batch,
+        A3.data_ptr(), _ld(A3), _bs(A3),
         B3.data_ptr(), _ld(B3), _bs(B3), _BL[b_layout], C3.data_ptr(), _ld(C3), _bs(C3),
         float(alpha), float(beta), int(num_iter), _stream_ptr(stream)))
     if C is not None:

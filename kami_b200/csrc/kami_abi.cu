@@ -85,10 +85,11 @@ static const MmaInstance *select_mma(int in_type, int part, int P, int M, int N,
         double cost = (double)c.BM * c.BN * c.BK;
         int w = c.nwarps > 16 ? 32 - c.nwarps : c.nwarps;
         cost -= w * 1e-3;
-        // equal tiles and warps: the 1D mapping (no exchange of C slices)
-        // measured fastest, streamed and repeated (FP64 64^3: 0.26 vs 0.34 ms)
+        // equal tiles: the 1D mapping (no exchange of C slices) measured
+        // fastest for FP64, streamed and repeated (64^3: 0.26 ms vs 0.34 ms
+        // for 2D); for 16-bit inputs it only breaks ties of warp count
         if (c.part == KAMI_PARTITION_1D)
-            cost -= 0.5e-3;
+            cost -= in_type == KAMI_F64 ? 0.5 : 0.5e-3; // FP64: before any warp count
         if (!best || cost < best_cost)
         {
             best = &c;

@@ -83,8 +83,17 @@ __device__ __forceinline__ int swz(int row, int chunk) { return row * 128 + ((ch
 // exact and linear in f over the whole range (the spacing is 1 there), so one
 // packed half-precision subtraction of 1536 (192) turns two patterns into the
 // two digits d exactly.
-template <bool BF16S> struct DigitCode;
-template <> struct DigitCode<false>
+// Slice kinds: binary16 digits (beta = 9), bfloat16 digits (beta = 7),
+// int8 digits (beta = 8, exact INT32 accumulation).
+enum SliceKind
+{
+    kSliceF16 = 0,
+    kSliceBF16 = 1,
+    kSliceI8 = 2
+};
+
+template <int SK> struct DigitCode;
+template <> struct DigitCode<kSliceF16>
 {
     static constexpr int kBeta = 9;
     static constexpr uint32_t kOff = 0x6500u;  // binary16 1280
@@ -95,7 +104,7 @@ template <> struct DigitCode<false>
         return *reinterpret_cast<const uint32_t *>(&r);
     }
 };
-template <> struct DigitCode<true>
+template <> struct DigitCode<kSliceBF16>
 {
     static constexpr int kBeta = 7;
     static constexpr uint32_t kOff = 0x4300u;  // bfloat16 128
@@ -132,17 +141,19 @@ __device__ __forceinline__ uint32_t field_at(uint64_t Y, int lo, uint32_t m, int
 // e >= be - 1021, so the left shift BS - e + be - 1075 is at most BS - 54 <= 9
 // and one rounding right shift of m 2^10 suffices.  Zero, and subnormal x
 // (rare; only rows whose maximum is tiny), take a slower exact path.
-// round(x 2^(BS - e)) + H as a uint64 (|x| 2^-e < 1/2, so the rounded value
-// is at most 2^(BS-1) in magnitude and the sum is non-negative).  x is an
-// integer m < 2^53 times 2^(E - 1075) (E = the biased exponent, 1 for
-// subnormals), so the value is m 2^sh with sh = E + BS - e - 1075.  When the
-// row maximum is normal, e >= E - 1021 and sh <= BS - 54 <= 9: one rounding
-// (half away from zero) right shift of m 2^10 gives it.  Only rows whose
-// maximum is subnormal reach sh > 9, where the value is m 2^sh exactly.
+// round(x 2^(BS - e)) + H as a uint64.  x is an integer m < 2^53 times
+// 2^(E - 1075) (E = the biased exponent, 1 for subnormals), so the value is
+// m 2^sh with sh = E + BS - e - 1075.  With e = floor(log2 max) + G
+// (G = 2 for the 16-bit digits, |x| 2^-e < 1/2 and BS <= 63; G = 3 for the
+// int8 digits, |x| 2^-e < 1/4 and BS <= 64), a normal row maximum gives
+// e >= E - 1023 + G and sh <= BS - 52 - G <= 9: one rounding (half away from
+// zero) right shift of m 2^10 gives the value.  Only rows whose maximum is
+// subnormal reach sh > 9, where the value is m 2^sh exactly.  The result
+// stays below 2^(BS - G + 1) in magnitude; H makes it non-negative.
 template <int BS>
 __device__ __forceinline__ uint64_t offset_fixed(double x, int e, uint64_t H)
 {
-    static_assert(BS <= 63, "fixed-point image must fit in 63 bits");
+    static_assert(BS <= 64, "fixed-point image must fit in 64 bits");
     const uint64_t u = (uint64_t)__double_as_longlong(x);
     const int be = (int)(u >> 52) & 0x7FF;
     const uint64_t m = (u & 0xFFFFFFFFFFFFFull) | ((uint64_t)(be != 0) << 52);
@@ -163,10 +174,10 @@ __device__ __forceinline__ uint64_t offset_fixed(double x, int e, uint64_t H)
 // tile_row(p).  Eight elements (one 16-byte chunk of each digit tile) at a
 // time: Y = round(x 2^(beta S - e)) + H, then digit p is field S - p of Y
 // minus 2^(beta-1) (the most significant field keeps its carry bit).
-template <bool BF16S, int S, class TileFn>
+template <int SK, int S, class TileFn>
 __device__ __forceinline__ void split_row(const double (&r)[32], int e, int half, TileFn tile_row)
 {
-    using Code = DigitCode<BF16S>;
+    using Code = DigitCode<SK>;
     constexpr int BETA = Code::kBeta, BS = BETA * S;
     constexpr uint64_t H = half_digits<BETA, S>();
     constexpr uint32_t OFF2 = Code::kOff | (Code::kOff << 16);
@@ -241,25 +252,82 @@ __device__ __forceinline__ double load_row(const SplitParams &p, const double *X
     return fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
 }
 
+// Bytes of four 32-bit words transposed: out[p] = byte p of in[0..3] (in
+// byte order).
+__device__ __forceinline__ void byte_transpose4(const uint32_t (&in)[4], uint32_t (&out)[4])
+{
+    const uint32_t a = __byte_perm(in[0], in[1], 0x5140), b = __byte_perm(in[2], in[3], 0x5140);
+    const uint32_t c = __byte_perm(in[0], in[1], 0x7362), d = __byte_perm(in[2], in[3], 0x7362);
+    out[0] = __byte_perm(a, b, 0x5410);
+    out[1] = __byte_perm(a, b, 0x7632);
+    out[2] = __byte_perm(c, d, 0x5410);
+    out[3] = __byte_perm(c, d, 0x7632);
+}
+
+// Int8 digits of 32 values of one row (this thread's half of K): with
+// Y = round(x 2^(8S - e)) + H (H = 0x80 in each of the S-1 low bytes), the
+// low S bytes of Y ^ H are the S balanced base-256 digits themselves, least
+// significant first (low digits in [-128, 127], the top one within +-65).
+// Digit p (1 = most significant) is byte S - p; eight values (8 bytes of one
+// digit tile row) are transposed and stored at a time.
+template <int S, class TileFn>
+__device__ __forceinline__ void split_row_i8(const double (&r)[32], int e, int half, TileFn tile_row)
+{
+    constexpr uint64_t H = half_digits<8, S - 1>();
+#pragma unroll
+    for (int c8 = 0; c8 < 4; ++c8)
+    {
+        uint32_t lo[8], hi[8]; // digits 0-3 / 4-7 (from the least significant) of 8 values
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+        {
+            const uint64_t D = offset_fixed<8 * S>(r[8 * c8 + q], e, H) ^ H;
+            lo[q] = (uint32_t)D;
+            hi[q] = (uint32_t)(D >> 32);
+        }
+        uint32_t t0[4], t1[4], u0[4], u1[4];
+        byte_transpose4(*reinterpret_cast<const uint32_t(*)[4]>(&lo[0]), t0); // values 0-3, digits 0-3
+        byte_transpose4(*reinterpret_cast<const uint32_t(*)[4]>(&lo[4]), t1); // values 4-7, digits 0-3
+        if constexpr (S > 4)
+        {
+            byte_transpose4(*reinterpret_cast<const uint32_t(*)[4]>(&hi[0]), u0);
+            byte_transpose4(*reinterpret_cast<const uint32_t(*)[4]>(&hi[4]), u1);
+        }
+        // K index of the first value: 32 half + 8 c8 -> 16-byte chunk and offset
+        const int chunk = half * 2 + (c8 >> 1), off = (c8 & 1) * 8;
+#pragma unroll
+        for (int k = 0; k < S; ++k)
+        {
+            const uint32_t w0 = k < 4 ? t0[k & 3] : u0[k & 3], w1 = k < 4 ? t1[k & 3] : u1[k & 3];
+            uint8_t *base;
+            int row;
+            tile_row(S - k, base, row);
+            *reinterpret_cast<uint2 *>(base + swz(row, chunk) + off) = make_uint2(w0, w1);
+        }
+    }
+}
+
 // Scale and split one loaded row-half (row maximum mx).  Writes the row's
 // exponent (half 0) and its S digits into the digit tiles at `dig` (A: digit
 // p in stack (p-1)/2, row ((p-1)%2)*64 + row; B: digit p in tile p-1).
-template <bool BF16S, int S>
+template <int SK, int S>
 __device__ __forceinline__ void split_loaded(const double (&r)[32], double mx, int row, int half, uint8_t *dig,
                                              int *exps)
 {
-    // e = floor(log2 max) + 2, so |x| 2^-e < 1/2 and every digit satisfies
-    // |d| <= 2^(beta-1); a zero row gets e = 0 (all digits zero)
+    // e = floor(log2 max) + G, so |x| 2^-e < 2^(1-G): G = 2 keeps every
+    // 16-bit digit within 2^(beta-1); G = 3 keeps the top int8 digit within
+    // +-65.  A zero row gets e = 0 (all digits zero).
+    constexpr int G = SK == kSliceI8 ? 3 : 2;
     int e = 0;
     if (mx > 0.0)
     {
         const int be = (int)(((uint64_t)__double_as_longlong(mx) >> 52) & 0x7FF);
         if (be > 0)
-            e = be - 1023 + 2;
+            e = be - 1023 + G;
         else
         {
             frexp(mx, &e);
-            e += 1;
+            e += G - 1;
         }
     }
     if (half == 0)
@@ -267,27 +335,33 @@ __device__ __forceinline__ void split_loaded(const double (&r)[32], double mx, i
     // digit d of row `row`: A stack (d-1)/2 holds odd digits in rows 0..63 and
     // even digits in rows 64..127 (8 KB further), B tile d-1 holds digit d;
     // both place digit d at byte (d-1) * 8 KB + 128 row
-    split_row<BF16S, S>(r, e, half, [&](int d, uint8_t *&base, int &rr) {
+    auto tile_row = [&](int d, uint8_t *&base, int &rr) {
         base = dig + (d - 1) * kSliceBytes;
         rr = row;
-    });
+    };
+    if constexpr (SK == kSliceI8)
+        split_row_i8<S>(r, e, half, tile_row);
+    else
+        split_row<SK, S>(r, e, half, tile_row);
     if constexpr (S & 1)
     {
-        // odd digit count: digit S+1 of the last pair is zero
+        // odd digit count: digit S+1 of the last pair is zero (int8 rows use
+        // the first 64 bytes: two 16-byte chunks per row-half)
         uint8_t *base = dig + S * kSliceBytes;
+        constexpr int nch = SK == kSliceI8 ? 2 : 4;
 #pragma unroll
-        for (int c = 0; c < 4; ++c)
-            *reinterpret_cast<uint4 *>(base + swz(row, half * 4 + c)) = make_uint4(0, 0, 0, 0);
+        for (int c = 0; c < nch; ++c)
+            *reinterpret_cast<uint4 *>(base + swz(row, half * nch + c)) = make_uint4(0, 0, 0, 0);
     }
 }
 
-template <bool BF16S, int S>
+template <int SK, int S>
 __device__ __forceinline__ void split_operand(const SplitParams &p, const double *X, bool is_b, int row, int half,
                                               uint8_t *dig, int *exps)
 {
     double r[32];
     const double mx = load_row(p, X, is_b ? p.ldb : p.lda, is_b, row, half, r);
-    split_loaded<BF16S, S>(r, mx, row, half, dig, exps);
+    split_loaded<SK, S>(r, mx, row, half, dig, exps);
 }
 
 // 2^n as a double for n >= -1074 (subnormal below -1022), 0 below
@@ -325,7 +399,7 @@ constexpr int xfer_ld()
 // are read smallest weight first, 16 columns at a time; the TMEM reads of
 // the next 16 columns are in flight while the current ones are converted
 // and accumulated.  taddr = lane quadrant + j0.
-template <int BMAX, int W>
+template <int BMAX, int W, int SK>
 __device__ __forceinline__ void gather_chunk(uint32_t taddr, bool top, int beta, double (&acc)[W])
 {
     constexpr int H = W / 16, NU = (BMAX + 1) * H; // units of 16 columns
@@ -349,10 +423,29 @@ __device__ __forceinline__ void gather_chunk(uint32_t taddr, bool top, int beta,
             tc::tmem_ld16(taddr + (uint32_t)bn * 128 + 64 + 16 * hn, vr[cur ^ 1]);
         }
         const int wl = top ? 2 * b + 2 : 2 * b + 3;
-        const double sl = pow2(-beta * wl), sr = pow2(-beta * (wl + 1));
+        if constexpr (SK == kSliceI8)
+        {
+            // INT32 quadrants: left * 2^8 + right is exact (|.| < 2^31, at most
+            // four products of |d| <= 128 per quadrant and K = 64), converted
+            // with the 2^52 + 2^51 bias (integer and FP64 add, no conversion
+            // unit) and weighted as the right quadrant
+            const double sr = pow2(-beta * (wl + 1));
+            constexpr double kBias = 6755399441055744.0; // 2^52 + 2^51
 #pragma unroll
-        for (int e = 0; e < 16; ++e)
-            acc[16 * h + e] += (double)__uint_as_float(vr[cur][e]) * sr + (double)__uint_as_float(vl[cur][e]) * sl;
+            for (int e = 0; e < 16; ++e)
+            {
+                const int v = (int)(vl[cur][e] << 8) + (int)vr[cur][e];
+                const double d = __hiloint2double(0x43380000 + (v >> 31), v) - kBias;
+                acc[16 * h + e] = fma(d, sr, acc[16 * h + e]);
+            }
+        }
+        else
+        {
+            const double sl = pow2(-beta * wl), sr = pow2(-beta * (wl + 1));
+#pragma unroll
+            for (int e = 0; e < 16; ++e)
+                acc[16 * h + e] += (double)__uint_as_float(vr[cur][e]) * sr + (double)__uint_as_float(vl[cur][e]) * sl;
+        }
     }
 }
 
@@ -411,7 +504,27 @@ __device__ __forceinline__ void recombine_store(const SplitParams &p, double *Cp
     }
 }
 
-template <bool BF16S, int S>
+// One digit-pair product over K = 64: four kind::f16 MMAs of K = 16 (16-bit
+// digits) or two kind::i8 MMAs of K = 32 (int8 digits); each K-step
+// advances the descriptors by 32 bytes (2 in their 16-byte units).
+template <int SK>
+__device__ __forceinline__ void issue_pair(uint32_t col, uint64_t ad, uint64_t bd, uint32_t idesc, uint32_t first)
+{
+    if constexpr (SK == kSliceI8)
+    {
+        tc::mma_i8_ss(col, ad, bd, idesc, first);
+        tc::mma_i8_ss(col, ad + 2, bd + 2, idesc, 1u);
+    }
+    else
+    {
+        tc::mma_f16_ss(col, ad, bd, idesc, first);
+        tc::mma_f16_ss(col, ad + 2, bd + 2, idesc, 1u);
+        tc::mma_f16_ss(col, ad + 4, bd + 4, idesc, 1u);
+        tc::mma_f16_ss(col, ad + 6, bd + 6, idesc, 1u);
+    }
+}
+
+template <int SK, int S>
 __global__ void __launch_bounds__(128) split_f64_kernel(const SplitParams p)
 {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -443,7 +556,7 @@ __global__ void __launch_bounds__(128) split_f64_kernel(const SplitParams p)
     const int row = t >> 1, half = t & 1;
 #pragma unroll 1
     for (int op = 0; op < 2; ++op)
-        split_operand<BF16S, S>(p, op ? B : A, op != 0, row, half, op ? sB : sA, op ? eB : eA);
+        split_operand<SK, S>(p, op ? B : A, op != 0, row, half, op ? sB : sA, op ? eB : eA);
     // make the digit tiles visible to the tensor core (async proxy)
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
@@ -474,10 +587,7 @@ __global__ void __launch_bounds__(128) split_f64_kernel(const SplitParams p)
                     const uint64_t ad = ad0 + st * pair16, bd = bd0 + u * pair16;
                     // stack 0 opens every block; later stacks accumulate
                     const uint32_t first = (it == 0 && st == 0) ? 0u : 1u;
-                    tc::mma_f16_ss(col, ad, bd, p.idesc, first);
-                    tc::mma_f16_ss(col, ad + 2, bd + 2, p.idesc, 1u);
-                    tc::mma_f16_ss(col, ad + 4, bd + 4, p.idesc, 1u);
-                    tc::mma_f16_ss(col, ad + 6, bd + 6, p.idesc, 1u);
+                    issue_pair<SK>(col, ad, bd, p.idesc, first);
                 }
         tc::mma_commit(bar);
     }
@@ -502,7 +612,7 @@ __global__ void __launch_bounds__(128) split_f64_kernel(const SplitParams p)
     {
         double acc[W];
         if (done)
-            gather_chunk<bmax, W>(tmem + lane_addr + j0, top, p.beta, acc);
+            gather_chunk<bmax, W, SK>(tmem + lane_addr + j0, top, p.beta, acc);
         else
         {
 #pragma unroll
@@ -593,7 +703,7 @@ __device__ __forceinline__ void stage_problem(const SplitParams &p, int64_t prob
         tc::bulk_g2s(stage + (size_t)tt * kStageLd * 8, p.B + prob * p.sB + (tt - 64) * p.ldb, b_bytes, sfull);
 }
 
-template <int S>
+template <int SK, int S>
 __device__ __forceinline__ void issue_products(const SplitParams &p, uint32_t tmem, uint8_t *buf, uint64_t *dempty,
                                                uint64_t *tfull)
 {
@@ -608,16 +718,13 @@ __device__ __forceinline__ void issue_products(const SplitParams &p, uint32_t tm
                 const uint32_t col = tmem + (uint32_t)(st + u) * 128;
                 const uint64_t ad = ad0 + st * pair16, bd = bd0 + u * pair16;
                 const uint32_t first = (it == 0 && st == 0) ? 0u : 1u;
-                tc::mma_f16_ss(col, ad, bd, p.idesc, first);
-                tc::mma_f16_ss(col, ad + 2, bd + 2, p.idesc, 1u);
-                tc::mma_f16_ss(col, ad + 4, bd + 4, p.idesc, 1u);
-                tc::mma_f16_ss(col, ad + 6, bd + 6, p.idesc, 1u);
+                issue_pair<SK>(col, ad, bd, p.idesc, first);
             }
     tc::mma_commit(dempty);
     tc::mma_commit(tfull);
 }
 
-template <bool BF16S, int S>
+template <int SK, int S>
 __global__ void __launch_bounds__(384, 1) split_f64_persistent(const SplitStreamParams sp)
 {
     const SplitParams &p = sp.p;
@@ -708,7 +815,7 @@ __global__ void __launch_bounds__(384, 1) split_f64_persistent(const SplitStream
             }
             uint8_t *buf = smem + (size_t)b * sp.buf_bytes;
             int *ex = exps + (j % kExpRing) * 128;
-            split_loaded<BF16S, S>(r, mx, row, half, is_b ? buf + nstack * kStackBytes : buf, is_b ? ex + 64 : ex);
+            split_loaded<SK, S>(r, mx, row, half, is_b ? buf + nstack * kStackBytes : buf, is_b ? ex + 64 : ex);
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
             if (lane == 0)
@@ -735,7 +842,7 @@ __global__ void __launch_bounds__(384, 1) split_f64_persistent(const SplitStream
             if (tc::mbar_wait_bounded(&dfull[0], 0, limit))
             {
                 tc::tc_fence_after();
-                issue_products<S>(p, tmem, smem, &dempty[0], tfull);
+                issue_products<SK, S>(p, tmem, smem, &dempty[0], tfull);
             }
             else
                 atomicExch(&g_split_error, 6);
@@ -756,7 +863,7 @@ __global__ void __launch_bounds__(384, 1) split_f64_persistent(const SplitStream
             for (int j0 = 0; j0 < 64; j0 += W)
             {
                 double acc[W];
-                gather_chunk<bmax, W>(tmem + lane_addr + j0, top, p.beta, acc);
+                gather_chunk<bmax, W, SK>(tmem + lane_addr + j0, top, p.beta, acc);
                 if (j0 == 64 - W)
                 {
                     // every TMEM read of problem j is done: start problem j+1
@@ -768,7 +875,7 @@ __global__ void __launch_bounds__(384, 1) split_f64_persistent(const SplitStream
                         if (tc::mbar_wait_bounded(&dfull[bn], (jn / sp.nbuf) & 1, limit))
                         {
                             tc::tc_fence_after();
-                            issue_products<S>(p, tmem, smem + (size_t)bn * sp.buf_bytes, &dempty[bn], tfull);
+                            issue_products<SK, S>(p, tmem, smem + (size_t)bn * sp.buf_bytes, &dempty[bn], tfull);
                         }
                         else
                             atomicExch(&g_split_error, 6); // the next tfull wait then times out for all
@@ -811,50 +918,54 @@ struct SplitFns
     const void *persistent;
 };
 
-template <bool BF, int S>
+template <int SK, int S>
 SplitFns split_fns()
 {
-    return {(const void *)&split_f64_kernel<BF, S>, (const void *)&split_f64_persistent<BF, S>};
+    return {(const void *)&split_f64_kernel<SK, S>, (const void *)&split_f64_persistent<SK, S>};
 }
 
-// kernels per (digit type, digit count): FP16 digits 2..7, BF16 digits 2..8
-SplitFns split_lookup(bool bf, int s)
+// kernels per (digit kind, digit count): FP16 digits 2..7, BF16 and int8
+// digits 2..8
+SplitFns split_lookup(int sk, int s)
 {
-    if (bf)
+#define KAMI_SPLIT_CASE(K, N) \
+    case N: return split_fns<K, N>();
+    if (sk == kSliceF16)
         switch (s)
         {
-        case 2: return split_fns<true, 2>();
-        case 3: return split_fns<true, 3>();
-        case 4: return split_fns<true, 4>();
-        case 5: return split_fns<true, 5>();
-        case 6: return split_fns<true, 6>();
-        case 7: return split_fns<true, 7>();
-        case 8: return split_fns<true, 8>();
+            KAMI_SPLIT_CASE(kSliceF16, 2) KAMI_SPLIT_CASE(kSliceF16, 3) KAMI_SPLIT_CASE(kSliceF16, 4)
+            KAMI_SPLIT_CASE(kSliceF16, 5) KAMI_SPLIT_CASE(kSliceF16, 6) KAMI_SPLIT_CASE(kSliceF16, 7)
+        default: break;
+        }
+    else if (sk == kSliceBF16)
+        switch (s)
+        {
+            KAMI_SPLIT_CASE(kSliceBF16, 2) KAMI_SPLIT_CASE(kSliceBF16, 3) KAMI_SPLIT_CASE(kSliceBF16, 4)
+            KAMI_SPLIT_CASE(kSliceBF16, 5) KAMI_SPLIT_CASE(kSliceBF16, 6) KAMI_SPLIT_CASE(kSliceBF16, 7)
+            KAMI_SPLIT_CASE(kSliceBF16, 8)
         default: break;
         }
     else
         switch (s)
         {
-        case 2: return split_fns<false, 2>();
-        case 3: return split_fns<false, 3>();
-        case 4: return split_fns<false, 4>();
-        case 5: return split_fns<false, 5>();
-        case 6: return split_fns<false, 6>();
-        case 7: return split_fns<false, 7>();
+            KAMI_SPLIT_CASE(kSliceI8, 2) KAMI_SPLIT_CASE(kSliceI8, 3) KAMI_SPLIT_CASE(kSliceI8, 4)
+            KAMI_SPLIT_CASE(kSliceI8, 5) KAMI_SPLIT_CASE(kSliceI8, 6) KAMI_SPLIT_CASE(kSliceI8, 7)
+            KAMI_SPLIT_CASE(kSliceI8, 8)
         default: break;
         }
+#undef KAMI_SPLIT_CASE
     return {nullptr, nullptr};
 }
 
 // raise the dynamic shared memory limit of one kernel, once per process
-cudaError_t allow_smem(const void *fn, bool bf, int s, int which)
+cudaError_t allow_smem(const void *fn, int sk, int s, int which)
 {
-    static std::once_flag once[2][9][2];
-    static cudaError_t err[2][9][2];
-    std::call_once(once[bf][s][which], [&] {
-        err[bf][s][which] = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    static std::once_flag once[3][9][2];
+    static cudaError_t err[3][9][2];
+    std::call_once(once[sk][s][which], [&] {
+        err[sk][s][which] = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
     });
-    return err[bf][s][which];
+    return err[sk][s][which];
 }
 
 size_t split_smem(int s) { return (size_t)((s + 1) / 2) * 2 * kStackBytes + 1024 + 1024; }
@@ -870,10 +981,10 @@ extern "C" int kami_split_f64_gemm_batched(int nslices, kami_dtype_t slice_type,
                                            int64_t ldc, int64_t strideC, double alpha, double beta, int num_iter,
                                            void *stream)
 {
-    const bool bf = slice_type == KAMI_BF16;
-    if (slice_type != KAMI_F16 && slice_type != KAMI_BF16)
-        return fail(KAMI_ERR_INVALID_VALUE, "split-FP64: slice_type must be KAMI_F16 or KAMI_BF16");
-    const int smax = bf ? 8 : 7;
+    if (slice_type != KAMI_F16 && slice_type != KAMI_BF16 && slice_type != KAMI_S8)
+        return fail(KAMI_ERR_INVALID_VALUE, "split-FP64: slice_type must be KAMI_F16, KAMI_BF16 or KAMI_S8");
+    const int sk = slice_type == KAMI_F16 ? kSliceF16 : (slice_type == KAMI_BF16 ? kSliceBF16 : kSliceI8);
+    const int smax = sk == kSliceF16 ? 7 : 8;
     if (nslices < 2 || nslices > smax)
         return fail(KAMI_ERR_UNSUPPORTED, "split-FP64: %d slices; supported 2..%d for this slice type", nslices,
                     smax);
@@ -912,21 +1023,28 @@ extern "C" int kami_split_f64_gemm_batched(int nslices, kami_dtype_t slice_type,
     p.b_layout = b_layout;
     p.c_vec = !(reinterpret_cast<uintptr_t>(C) & 15) && !(ldc & 1) && !(strideC & 1);
     p.s = nslices;
-    p.beta = bf ? 7 : 9;
+    p.beta = sk == kSliceF16 ? 9 : (sk == kSliceBF16 ? 7 : 8);
     p.alpha = alpha;
     p.beta_c = beta;
     p.num_iter = num_iter;
-    p.idesc = tc::idesc_f16(bf, 128, 128);
+    p.idesc = sk == kSliceI8 ? tc::idesc_i8(128, 128) : tc::idesc_f16(sk == kSliceBF16, 128, 128);
     uint32_t cols = 32;
     while ((int)cols < ((nslices - 1) / 2 + 1) * 128)
         cols <<= 1;
     p.tmem_cols = cols;
     p.timeout_ns = (uint64_t)(5e8 + (double)num_iter * nslices * nslices * 4 * 2000.0);
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    const SplitFns fns = split_lookup(bf, nslices);
+    const SplitFns fns = split_lookup(sk, nslices);
     if (!fns.per_problem)
         return fail(KAMI_ERR_UNSUPPORTED, "split-FP64: no kernel for %d slices", nslices);
-    if (num_iter <= 4)
+    // persistent form: streamed products, and repeated products whenever the
+    // per-problem form would hold one CTA per SM (four digit stacks: 7-8
+    // digits) or the digits are int8 -- its warp groups then overlap the
+    // splitting and recombination of neighbouring problems with the MMAs
+    // (repeated 20x at 64^3: 8 int8 digits 1.20 ms vs 1.47 ms per problem CTA;
+    // 6 FP16 digits stay per problem: 1.36 ms vs 1.44 ms)
+    const int nstack_sel = (nslices + 1) / 2;
+    if (num_iter <= 4 || nstack_sel >= 4 || sk == kSliceI8)
     {
         // streamed regime: the persistent, phase-overlapped form
         SplitStreamParams sp{};
@@ -947,7 +1065,7 @@ extern "C" int kami_split_f64_gemm_batched(int nslices, kami_dtype_t slice_type,
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         const void *fn = fns.persistent;
-        cudaError_t e2 = allow_smem(fn, bf, nslices, 1);
+        cudaError_t e2 = allow_smem(fn, sk, nslices, 1);
         if (e2 != cudaSuccess)
             return cuda_fail(e2, "cudaFuncSetAttribute(split_f64_persistent)");
         const int64_t grid = batch < sms ? batch : sms;
@@ -959,7 +1077,7 @@ extern "C" int kami_split_f64_gemm_batched(int nslices, kami_dtype_t slice_type,
     }
     const size_t smem = split_smem(nslices);
     const void *fn = fns.per_problem;
-    cudaError_t e = allow_smem(fn, bf, nslices, 0);
+    cudaError_t e = allow_smem(fn, sk, nslices, 0);
     if (e != cudaSuccess)
         return cuda_fail(e, "cudaFuncSetAttribute(split_f64_kernel)");
     void *args[] = {&p};

@@ -130,6 +130,18 @@ __device__ __forceinline__ void mma_f16_ss(uint32_t d_tmem, uint64_t a_desc, uin
                  : "memory");
 }
 
+// D[tmem] (+)= A[smem desc] * B[smem desc]^T, kind::i8 (signed 8-bit in,
+// INT32 accumulator)
+__device__ __forceinline__ void mma_i8_ss(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                          uint32_t accumulate)
+{
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "setp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+                 "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+                 : "memory");
+}
+
 // Arrive on `bar` once all previously issued tcgen05.mma of this thread
 // have completed.
 __device__ __forceinline__ void mma_commit(uint64_t *bar)
@@ -231,6 +243,18 @@ __host__ __device__ constexpr uint32_t idesc_f16(bool bf16, int M, int N, int a_
            | ((bf16 ? 1u : 0u) << 10)        // B format
            | ((uint32_t)(a_mn & 1) << 15)    // A major
            | ((uint32_t)(b_mn & 1) << 16)    // B major
+           | ((uint32_t)(N >> 3) << 17)      // N / 8
+           | ((uint32_t)(M >> 4) << 24);     // M / 16
+}
+
+// Instruction descriptor of tcgen05.mma kind::i8 with both operands signed
+// 8-bit, K-major, and an INT32 accumulator (D format 2, A/B format 1 =
+// signed), given M and N.
+__host__ __device__ constexpr uint32_t idesc_i8(int M, int N)
+{
+    return (2u << 4)                         // D format S32
+           | (1u << 7)                       // A signed 8-bit
+           | (1u << 10)                      // B signed 8-bit
            | ((uint32_t)(N >> 3) << 17)      // N / 8
            | ((uint32_t)(M >> 4) << 24);     // M / 16
 }

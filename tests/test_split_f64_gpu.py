@@ -102,3 +102,47 @@ def test_streamed_many_problems_exact(cuda, slice_dtype, s, b_layout, N):
     C = api.split_f64_gemm(torch.tensor(A, device="cuda"), torch.tensor(B, device="cuda"), nslices=s,
                            slice_dtype=slice_dtype, b_layout=b_layout)
     assert np.array_equal(C.cpu().numpy(), np.matmul(A, Bt))
+
+
+@pytest.mark.parametrize("s", [2, 4, 7, 8])
+def test_int8_digits_exact_on_integer_inputs(cuda, s):
+    """int8 digits (kind::i8 MMAs, INT32 accumulation) on integer inputs:
+    exact, per-problem (num_iter > 4) and streamed forms."""
+    rng = np.random.default_rng(20 + s)
+    A = rng.integers(-1000, 1001, (300, 64, 64)).astype(np.float64)
+    B = rng.integers(-1000, 1001, (300, 64, 64)).astype(np.float64)
+    ref = oracle.gemm(A, B)
+    dA, dB = torch.tensor(A, device="cuda"), torch.tensor(B, device="cuda")
+    C = api.split_f64_gemm(dA, dB, nslices=s, slice_dtype=torch.int8)
+    assert np.array_equal(C.cpu().numpy(), ref)
+    C5 = api.split_f64_gemm(dA[:8], dB[:8], nslices=s, slice_dtype=torch.int8, num_iter=5)
+    assert np.array_equal(C5.cpu().numpy(), 5 * ref[:8])
+
+
+def test_int8_eight_digits_error_vs_native(cuda):
+    """8 int8 digits (62 bits): no worse than 2x the native FP64 kernel's
+    normwise error against the double-double oracle, on the wide-exponent
+    workload."""
+    rng = np.random.default_rng(21)
+    A = wide_range((64, 64, 64), rng)
+    B = wide_range((64, 64, 64), rng)
+    hi, lo = oracle.gemm_dd(A, B)
+    dA, dB = torch.tensor(A, device="cuda"), torch.tensor(B, device="cuda")
+    e_native = oracle.normwise_error_dd(api.gemm_batched(dA, dB).cpu().numpy(), hi, lo)
+    for it in (1, 6):  # streamed and per-problem forms
+        C = api.split_f64_gemm(dA, dB, nslices=8, slice_dtype=torch.int8, num_iter=it).cpu().numpy() / it
+        e = oracle.normwise_error_dd(C, hi, lo)
+        assert e <= 2.0 * e_native, (it, e, e_native)
+
+
+@pytest.mark.parametrize("M,N,K,b_layout", [(17, 40, 34, "row_kn"), (64, 1, 64, "row_kn"), (33, 64, 2, "ref_nk")])
+def test_int8_shapes_layouts(cuda, M, N, K, b_layout):
+    rng = np.random.default_rng(M + N + K)
+    A = rng.uniform(-1, 1, (5, M, K))
+    Bt = rng.uniform(-1, 1, (5, K, N))
+    B = np.ascontiguousarray(Bt.transpose(0, 2, 1)) if b_layout == "ref_nk" else Bt
+    hi, lo = oracle.gemm_dd(A, np.ascontiguousarray(Bt.transpose(0, 2, 1)))
+    C = api.split_f64_gemm(torch.tensor(A, device="cuda"), torch.tensor(B, device="cuda"), nslices=8,
+                           slice_dtype=torch.int8, b_layout=b_layout).cpu().numpy()
+    bound = 8 * K * 2.0 ** -53 * (np.abs(A).max(axis=2)[:, :, None] * np.abs(Bt).max(axis=1)[:, None, :]) * 2
+    assert np.all(np.abs(C - (hi + lo)) <= bound)
