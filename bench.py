@@ -207,8 +207,7 @@ def run_reference(args, rank, world):
 # ---------------------------------------------------------------------------
 def run_ours(args, rank, world):
     import torch
-    import torch.distributed as dist
-    from kami_b200 import api
+    from kami_b200 import api, replicas
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
@@ -237,8 +236,7 @@ def run_ours(args, rank, world):
     got = C[0].double().cpu()
     rel = float((got - ref).norm() / ref.norm())
 
-    if world > 1:
-        dist.barrier()
+    replicas.barrier()
     sampler = ClockSampler(dev.index) if rank == 0 else None
     if sampler:
         sampler.start()
@@ -254,8 +252,7 @@ def run_ours(args, rank, world):
         times.append((e0, e1))
     torch.cuda.synchronize()
     ms = [a.elapsed_time(b) for a, b in times]
-    if world > 1:
-        dist.barrier()
+    replicas.barrier()
     # ---- end-to-end through the C ABI with host buffers ----
     A_pin = A_h.pin_memory()
     B_pin = B_h.pin_memory()
@@ -292,13 +289,10 @@ def run_ours(args, rank, world):
 
     step_ms = sum(ms) / len(ms)
     e2e_step = sum(e2e_ms) / len(e2e_ms)
-    if world > 1:
-        t = torch.tensor([step_ms, e2e_step], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        step_ms, e2e_step = float(t[0]), float(t[1])
+    step_ms, e2e_step = replicas.max_over_ranks([step_ms, e2e_step], dev)
     flops_rank = 2.0 * M * N * K * batch * num_iter
-    value = flops_rank * world / (step_ms * 1e-3) / 1e12
-    e2e_value = flops_rank * world / (e2e_step * 1e-3) / 1e12
+    value = replicas.aggregate_rate(flops_rank, step_ms, world) / 1e12
+    e2e_value = replicas.aggregate_rate(flops_rank, e2e_step, world) / 1e12
     if rank != 0:
         return
     peak_tf, peak_bw, src = measured_peaks()
