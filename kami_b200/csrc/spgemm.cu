@@ -207,6 +207,58 @@ struct SpNumArgs
     int num_iter;
 };
 
+// Store one C tile with alpha / beta: lane holds rows g, g+8 and columns
+// 2t, 2t+1 (acc0) and 2t+8, 2t+9 (acc1).
+__device__ __forceinline__ void store_c_tile(const SpNumArgs &p, int64_t c, int gq, int tq, const float (&acc0)[4],
+                                             const float (&acc1)[4])
+{
+    const int r0 = gq, r1 = gq + 8, c0 = 2 * tq;
+    if (p.out_type == KAMI_F32)
+    {
+        float *out = reinterpret_cast<float *>(p.vc) + c * 256;
+        float2 v00 = make_float2(acc0[0], acc0[1]), v01 = make_float2(acc1[0], acc1[1]);
+        float2 v10 = make_float2(acc0[2], acc0[3]), v11 = make_float2(acc1[2], acc1[3]);
+        if (p.alpha != 1.f || p.beta != 0.f)
+        {
+            const float2 o00 = *reinterpret_cast<float2 *>(out + r0 * 16 + c0);
+            const float2 o01 = *reinterpret_cast<float2 *>(out + r0 * 16 + c0 + 8);
+            const float2 o10 = *reinterpret_cast<float2 *>(out + r1 * 16 + c0);
+            const float2 o11 = *reinterpret_cast<float2 *>(out + r1 * 16 + c0 + 8);
+            const float a = p.alpha, b = p.beta;
+            v00 = make_float2(a * v00.x + (b != 0.f ? b * o00.x : 0.f), a * v00.y + (b != 0.f ? b * o00.y : 0.f));
+            v01 = make_float2(a * v01.x + (b != 0.f ? b * o01.x : 0.f), a * v01.y + (b != 0.f ? b * o01.y : 0.f));
+            v10 = make_float2(a * v10.x + (b != 0.f ? b * o10.x : 0.f), a * v10.y + (b != 0.f ? b * o10.y : 0.f));
+            v11 = make_float2(a * v11.x + (b != 0.f ? b * o11.x : 0.f), a * v11.y + (b != 0.f ? b * o11.y : 0.f));
+        }
+        *reinterpret_cast<float2 *>(out + r0 * 16 + c0) = v00;
+        *reinterpret_cast<float2 *>(out + r0 * 16 + c0 + 8) = v01;
+        *reinterpret_cast<float2 *>(out + r1 * 16 + c0) = v10;
+        *reinterpret_cast<float2 *>(out + r1 * 16 + c0 + 8) = v11;
+    }
+    else
+    {
+        uint16_t *out = reinterpret_cast<uint16_t *>(p.vc) + c * 256;
+        const bool bf = p.out_type == KAMI_BF16;
+        auto cvt = [&](float x, uint16_t old) -> uint16_t {
+            float y = p.alpha * x;
+            if (p.beta != 0.f)
+                y += p.beta * to_float(old, bf);
+            return bf ? __bfloat16_as_ushort(__float2bfloat16_rn(y)) : __half_as_ushort(__float2half_rn(y));
+        };
+        const int offs[4] = {r0 * 16 + c0, r0 * 16 + c0 + 8, r1 * 16 + c0, r1 * 16 + c0 + 8};
+        const float vals[4][2] = {{acc0[0], acc0[1]}, {acc1[0], acc1[1]}, {acc0[2], acc0[3]}, {acc1[2], acc1[3]}};
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+        {
+            uint32_t *dst = reinterpret_cast<uint32_t *>(out + offs[q]);
+            const uint32_t old = p.beta != 0.f ? *dst : 0u;
+            const uint16_t lo16 = cvt(vals[q][0], (uint16_t)(old & 0xffff));
+            const uint16_t hi16 = cvt(vals[q][1], (uint16_t)(old >> 16));
+            *dst = (uint32_t)lo16 | ((uint32_t)hi16 << 16);
+        }
+    }
+}
+
 template <bool BF16>
 __global__ void __launch_bounds__(256) spgemm_numeric_kernel(const SpNumArgs p)
 {
@@ -287,51 +339,207 @@ __global__ void __launch_bounds__(256) spgemm_numeric_kernel(const SpNumArgs p)
         }
     }
 
-    // store the tile: lane holds rows g, g+8 and columns 2t, 2t+1 (+8)
-    const int r0 = gq, r1 = gq + 8, c0 = 2 * tq;
-    if (p.out_type == KAMI_F32)
+    store_c_tile(p, c, gq, tq, acc0, acc1);
+}
+
+// ---------------------------------------------------------------------------
+// numeric, one CTA per block-row of C (16-byte aligned tiles)
+//
+// The C tiles of block-row i all multiply the same A tiles A(i, k) and search
+// the same B block-rows k for their column j.  So the CTA stages, once, the
+// A tiles of row i (ldmatrix layout) and the column indices of every B row k
+// it touches in shared memory; each of its 8 warps then takes C tiles
+// (i, j) in turn: lanes binary-search j in the staged lists (shared-memory
+// latency instead of dependent global loads), and every match costs one
+// coalesced 512-byte load of the B tile into the warp's slot, one ldmatrix
+// (transposed) for its fragments, and two MMAs.  Products are accumulated in
+// ascending k, as the reference's sparse accumulator does.  Rows whose A
+// tiles or B lists exceed the staging capacity read them from global memory.
+// ---------------------------------------------------------------------------
+constexpr int kRowWarps = 8;
+constexpr int kMaxATiles = 32;   // 16 KB of A tiles (about 28 KB per CTA: 8 CTAs per SM)
+constexpr int kMaxBList = 2048;  // 8 KB of B column indices
+
+// byte offset of row r, 16-byte chunk c of a 16 x 16 16-bit tile (32-byte
+// rows): the chunk is flipped for rows 4-7 and 12-15 so that the eight rows
+// of an ldmatrix phase fall in distinct banks
+__device__ __forceinline__ int tile_swz(int r, int c) { return r * 32 + ((c ^ ((r >> 2) & 1)) << 4); }
+
+// copy one 512-byte tile (16 bytes per lane) into a swizzled shared tile
+__device__ __forceinline__ void stage_tile(uint8_t *dst, const uint16_t *src, int lane)
+{
+    const uint4 v = __ldg(reinterpret_cast<const uint4 *>(src) + lane);
+    *reinterpret_cast<uint4 *>(dst + tile_swz(lane >> 1, lane & 1)) = v;
+}
+
+// ldmatrix address of lane for the x4 load of a swizzled tile: matrices
+// (rows 0-7, chunk 0), (rows 8-15, chunk 0), (rows 0-7, chunk 1), (8-15, 1)
+__device__ __forceinline__ uint32_t tile_ldsm_addr(uint32_t base, int lane)
+{
+    const int m = lane >> 3, i = lane & 7;
+    return base + tile_swz((m & 1) * 8 + i, m >> 1);
+}
+
+__device__ __forceinline__ void ldsm4(uint32_t a, uint32_t (&r)[4])
+{
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(a));
+}
+
+__device__ __forceinline__ void ldsm4_t(uint32_t a, uint32_t (&r)[4])
+{
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(a));
+}
+
+template <bool BF16>
+__global__ void __launch_bounds__(kRowWarps * 32) spgemm_numeric_row_kernel(const SpNumArgs p)
+{
+    __shared__ __align__(16) uint8_t sA[kMaxATiles * 512];
+    __shared__ __align__(16) uint8_t sB[kRowWarps * 512]; // one B tile slot per warp
+    __shared__ int sList[kMaxBList];
+    __shared__ int sOff[kMaxATiles + 1];
+    __shared__ int sK[kMaxATiles];
+    const int i = blockIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int c0 = p.rpc[i], c1 = p.rpc[i + 1];
+    if (c0 == c1)
+        return;
+    const int a0 = p.rpa[i], na = p.rpa[i + 1] - a0;
+    const bool a_staged = na <= kMaxATiles;
+
+    // ---- staging (whole CTA): A tiles, B row lengths, their prefix, lists ----
+    bool l_staged = false;
+    if (a_staged)
     {
-        float *out = reinterpret_cast<float *>(p.vc) + c * 256;
-        float2 v00 = make_float2(acc0[0], acc0[1]), v01 = make_float2(acc1[0], acc1[1]);
-        float2 v10 = make_float2(acc0[2], acc0[3]), v11 = make_float2(acc1[2], acc1[3]);
-        if (p.alpha != 1.f || p.beta != 0.f)
+        for (int e = warp; e < na; e += kRowWarps)
+            stage_tile(sA + e * 512, p.va + (int64_t)(a0 + e) * 256, lane);
+        if (warp == 0)
         {
-            const float2 o00 = *reinterpret_cast<float2 *>(out + r0 * 16 + c0);
-            const float2 o01 = *reinterpret_cast<float2 *>(out + r0 * 16 + c0 + 8);
-            const float2 o10 = *reinterpret_cast<float2 *>(out + r1 * 16 + c0);
-            const float2 o11 = *reinterpret_cast<float2 *>(out + r1 * 16 + c0 + 8);
-            const float a = p.alpha, b = p.beta;
-            v00 = make_float2(a * v00.x + (b != 0.f ? b * o00.x : 0.f), a * v00.y + (b != 0.f ? b * o00.y : 0.f));
-            v01 = make_float2(a * v01.x + (b != 0.f ? b * o01.x : 0.f), a * v01.y + (b != 0.f ? b * o01.y : 0.f));
-            v10 = make_float2(a * v10.x + (b != 0.f ? b * o10.x : 0.f), a * v10.y + (b != 0.f ? b * o10.y : 0.f));
-            v11 = make_float2(a * v11.x + (b != 0.f ? b * o11.x : 0.f), a * v11.y + (b != 0.f ? b * o11.y : 0.f));
-        }
-        *reinterpret_cast<float2 *>(out + r0 * 16 + c0) = v00;
-        *reinterpret_cast<float2 *>(out + r0 * 16 + c0 + 8) = v01;
-        *reinterpret_cast<float2 *>(out + r1 * 16 + c0) = v10;
-        *reinterpret_cast<float2 *>(out + r1 * 16 + c0 + 8) = v11;
-    }
-    else
-    {
-        uint16_t *out = reinterpret_cast<uint16_t *>(p.vc) + c * 256;
-        const bool bf = p.out_type == KAMI_BF16;
-        auto cvt = [&](float x, uint16_t old) -> uint16_t {
-            float y = p.alpha * x;
-            if (p.beta != 0.f)
-                y += p.beta * to_float(old, bf);
-            return bf ? __bfloat16_as_ushort(__float2bfloat16_rn(y)) : __half_as_ushort(__float2half_rn(y));
-        };
-        const int offs[4] = {r0 * 16 + c0, r0 * 16 + c0 + 8, r1 * 16 + c0, r1 * 16 + c0 + 8};
-        const float vals[4][2] = {{acc0[0], acc0[1]}, {acc1[0], acc1[1]}, {acc0[2], acc0[3]}, {acc1[2], acc1[3]}};
+            // lengths of the B rows, exclusive prefix over the (<= 48) entries
+            int total = 0;
+            for (int base = 0; base < na; base += 32)
+            {
+                const int e = base + lane;
+                int len = 0;
+                if (e < na)
+                {
+                    const int k = p.cia[a0 + e];
+                    sK[e] = k;
+                    len = p.rpb[k + 1] - p.rpb[k];
+                }
+                int pre = len;
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
-        {
-            uint32_t *dst = reinterpret_cast<uint32_t *>(out + offs[q]);
-            const uint32_t old = p.beta != 0.f ? *dst : 0u;
-            const uint16_t lo16 = cvt(vals[q][0], (uint16_t)(old & 0xffff));
-            const uint16_t hi16 = cvt(vals[q][1], (uint16_t)(old >> 16));
-            *dst = (uint32_t)lo16 | ((uint32_t)hi16 << 16);
+                for (int o = 1; o < 32; o <<= 1)
+                {
+                    const int y = __shfl_up_sync(0xffffffffu, pre, o);
+                    if (lane >= o)
+                        pre += y;
+                }
+                if (e < na)
+                    sOff[e] = total + pre - len;
+                total += __shfl_sync(0xffffffffu, pre, 31);
+            }
+            if (lane == 0)
+                sOff[na] = total;
         }
+        __syncthreads();
+        l_staged = sOff[na] <= kMaxBList;
+        if (l_staged)
+            for (int e = warp; e < na; e += kRowWarps)
+            {
+                const int b0 = p.rpb[sK[e]], len = sOff[e + 1] - sOff[e];
+                for (int q = lane; q < len; q += 32)
+                    sList[sOff[e] + q] = p.cib[b0 + q];
+            }
+        __syncthreads();
+    }
+
+    const int gq = lane >> 2, tq = lane & 3;
+    const uint32_t sA_u = (uint32_t)__cvta_generic_to_shared(sA);
+    const uint32_t slot = (uint32_t)__cvta_generic_to_shared(sB + warp * 512);
+    uint8_t *slot_p = sB + warp * 512;
+    for (int c = c0 + warp; c < c1; c += kRowWarps)
+    {
+        const int j = p.cic[c];
+        float acc0[4] = {0.f, 0.f, 0.f, 0.f}; // C columns 0..7
+        float acc1[4] = {0.f, 0.f, 0.f, 0.f}; // C columns 8..15
+        for (int it = 0; it < p.num_iter; ++it)
+            for (int base = 0; base < na; base += 32)
+            {
+                // lane e: position of column j in B row k_e (global B entry), or -1
+                const int e = base + lane;
+                int match = -1;
+                if (e < na)
+                {
+                    const int k = a_staged ? sK[e] : p.cia[a0 + e];
+                    const int bstart = p.rpb[k];
+                    if (l_staged)
+                    {
+                        int l = sOff[e], h = sOff[e + 1] - 1;
+                        const int o = l;
+                        while (l <= h)
+                        {
+                            const int m = (l + h) >> 1, v = sList[m];
+                            if (v == j)
+                            {
+                                match = bstart + (m - o);
+                                break;
+                            }
+                            if (v < j)
+                                l = m + 1;
+                            else
+                                h = m - 1;
+                        }
+                    }
+                    else
+                    {
+                        int l = bstart, h = p.rpb[k + 1] - 1;
+                        while (l <= h)
+                        {
+                            const int m = (l + h) >> 1, v = p.cib[m];
+                            if (v == j)
+                            {
+                                match = m;
+                                break;
+                            }
+                            if (v < j)
+                                l = m + 1;
+                            else
+                                h = m - 1;
+                        }
+                    }
+                }
+                uint32_t hits = __ballot_sync(0xffffffffu, match >= 0);
+                while (hits)
+                {
+                    const int src = __ffs(hits) - 1;
+                    hits &= hits - 1;
+                    const int eb = __shfl_sync(0xffffffffu, match, src);
+                    const int ea = base + src;
+                    uint32_t a[4];
+                    if (a_staged)
+                        ldsm4(tile_ldsm_addr(sA_u + ea * 512, lane), a);
+                    else
+                    {
+                        const uint32_t *ta = reinterpret_cast<const uint32_t *>(p.va + (int64_t)(a0 + ea) * 256);
+                        a[0] = __ldg(ta + (gq * 16 + 2 * tq) / 2);
+                        a[1] = __ldg(ta + ((gq + 8) * 16 + 2 * tq) / 2);
+                        a[2] = __ldg(ta + (gq * 16 + 2 * tq + 8) / 2);
+                        a[3] = __ldg(ta + ((gq + 8) * 16 + 2 * tq + 8) / 2);
+                    }
+                    __syncwarp(); // the slot's previous tile has been read
+                    stage_tile(slot_p, p.vb + (int64_t)eb * 256, lane);
+                    __syncwarp();
+                    uint32_t b[4];
+                    ldsm4_t(tile_ldsm_addr(slot, lane), b); // (k lo, n 0-7), (k hi, n 0-7), (k lo, n 8-15), (k hi, n 8-15)
+                    mma16816<BF16>(acc0, a[0], a[1], a[2], a[3], b[0], b[1]);
+                    mma16816<BF16>(acc1, a[0], a[1], a[2], a[3], b[2], b[3]);
+                }
+            }
+        store_c_tile(p, c, gq, tq, acc0, acc1);
     }
 }
 
@@ -490,7 +698,15 @@ int kami_spgemm_bsr_numeric(kami_dtype_t in_type, kami_dtype_t out_type, int bsr
     if (grid > 0x7fffffff)
         return fail(KAMI_ERR_UNSUPPORTED, "spgemm numeric: too many C tiles");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    if (in_type == KAMI_BF16)
+    const bool rowwise = !(reinterpret_cast<uintptr_t>(val_a) & 15) && !(reinterpret_cast<uintptr_t>(val_b) & 15);
+    if (rowwise) // one CTA per block-row, staged operands
+    {
+        if (in_type == KAMI_BF16)
+            spgemm_numeric_row_kernel<true><<<(unsigned)mb, kRowWarps * 32, 0, s>>>(p);
+        else
+            spgemm_numeric_row_kernel<false><<<(unsigned)mb, kRowWarps * 32, 0, s>>>(p);
+    }
+    else if (in_type == KAMI_BF16)
         spgemm_numeric_kernel<true><<<(unsigned)grid, 256, 0, s>>>(p);
     else
         spgemm_numeric_kernel<false><<<(unsigned)grid, 256, 0, s>>>(p);
