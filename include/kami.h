@@ -274,12 +274,29 @@ int kami_spgemm_bsr_fill_colidx(int bsr, int mb, int kb, int nb,
                                 const int *row_ptr_b, const int *col_idx_b,
                                 const int *row_ptr_c, int *col_idx_c, void *stream);
 
+/* The symbolic pass and the column fill in one call with no copy to the
+ * host and no synchronisation (three kernels on `stream`, so the whole
+ * SpGEMM can run inside one stream or graph): row_ptr_c[0..mb] as in
+ * kami_spgemm_bsr_symbolic, nnzC = row_ptr_c[mb] left on the device, and
+ * col_idx_c filled up to `capacity` entries (the caller's upper bound for
+ * nnzC, e.g. mb * nb or the sum of B row lengths over A's entries; entries
+ * beyond it are not written -- compare row_ptr_c[mb] with capacity when it
+ * may be exceeded).  The reference's host sequence
+ * (block_spgemm_2d_half_mma.cu:805-812) synchronises here to size ColIdxC. */
+int kami_spgemm_bsr_symbolic_device(int bsr, int mb, int kb, int nb,
+                                    const int *row_ptr_a, const int *col_idx_a,
+                                    const int *row_ptr_b, const int *col_idx_b,
+                                    int *row_ptr_c, int *col_idx_c, int64_t capacity, void *stream);
+
 /* Numeric pass: val_c (nnz_c tiles in col_idx_c order) = alpha *
  * num_iter * (A * B) + beta * val_c, FP16 or BF16 tiles with FP32
  * accumulation; out_type KAMI_F32, KAMI_F16 or KAMI_BF16.  Replaces
  * block_spgemm_{1d,2d,3d}_half_mma (e.g. :171-174, argument order kept:
  * RowPtrA, ColIdxA, ValA, RowPtrB, ColIdxB, ValB, RowPtrC, ColIdxC, ValC,
- * alpha, beta); num_iter is the reference's NUM_ITER repeat. */
+ * alpha, beta); num_iter is the reference's NUM_ITER repeat.  nnz_c may be
+ * an upper bound of row_ptr_c[mb] (tiles past row_ptr_c[mb] are untouched),
+ * so a capacity from kami_spgemm_bsr_symbolic_device serves.  val_a / val_b
+ * may be NULL only for an operand without entries. */
 int kami_spgemm_bsr_numeric(kami_dtype_t in_type, kami_dtype_t out_type, int bsr,
                             int mb, int kb, int nb,
                             const int *row_ptr_a, const int *col_idx_a, const void *val_a,

@@ -234,6 +234,33 @@ def spgemm_numeric(A: BSR, B: BSR, row_ptr_c, col_idx_c, out_dtype=torch.float32
     return C_values[:nnz_c]
 
 
+def spgemm_symbolic_device(A: BSR, B: BSR, capacity: int, stream=None):
+    """RowPtrC and ColIdxC (capacity entries) without a host round trip
+    (kami_spgemm_bsr_symbolic_device); nnzC is row_ptr_c[-1] on the device."""
+    if A.block_cols != B.block_rows:
+        raise ValueError("inner block dimensions differ")
+    dev = A.row_ptr.device
+    rpc = torch.empty(A.block_rows + 1, dtype=torch.int32, device=dev)
+    cic = torch.empty(max(int(capacity), 1), dtype=torch.int32, device=dev)
+    check(load().kami_spgemm_bsr_symbolic_device(16, A.block_rows, A.block_cols, B.block_cols, A.row_ptr.data_ptr(),
+                                                 _ptr(A.col_idx), B.row_ptr.data_ptr(), _ptr(B.col_idx),
+                                                 rpc.data_ptr(), cic.data_ptr(), int(capacity), _stream_ptr(stream)))
+    return rpc, cic
+
+
+def spgemm_numeric_bound(A: BSR, B: BSR, row_ptr_c, col_idx_c, C_values, *, alpha=1.0, beta=0.0, num_iter=1,
+                         stream=None) -> torch.Tensor:
+    """Numeric pass into C_values [capacity, 16, 16] with the capacity as the
+    bound of nnzC (no host synchronisation)."""
+    cap = C_values.shape[0]
+    check(load().kami_spgemm_bsr_numeric(_DT[A.values.dtype], _DT[C_values.dtype], 16, A.block_rows, A.block_cols,
+                                         B.block_cols, A.row_ptr.data_ptr(), _ptr(A.col_idx), _ptr(A.values),
+                                         B.row_ptr.data_ptr(), _ptr(B.col_idx), _ptr(B.values),
+                                         row_ptr_c.data_ptr(), _ptr(col_idx_c), _ptr(C_values), cap,
+                                         float(alpha), float(beta), int(num_iter), _stream_ptr(stream)))
+    return C_values
+
+
 def spgemm(A: BSR, B: BSR, out_dtype=torch.float32, *, num_iter=1, stream=None) -> BSR:
     """C = A * B: symbolic, column fill, numeric (the reference's sequence)."""
     rpc, nnz = spgemm_symbolic(A, B, stream)

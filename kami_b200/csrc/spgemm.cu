@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(1024) spgemm_scan_kernel(int n, int *__restric
 
 __global__ void spgemm_colfill_kernel(int mb, int nb, const int *__restrict__ rpa, const int *__restrict__ cia,
                                       const int *__restrict__ rpb, const int *__restrict__ cib,
-                                      const int *__restrict__ rpc, int *__restrict__ cic)
+                                      const int *__restrict__ rpc, int *__restrict__ cic, int64_t cap)
 {
     extern __shared__ uint32_t bm_all[];
     const int words = (nb + 31) >> 5;
@@ -167,7 +167,9 @@ __global__ void spgemm_colfill_kernel(int mb, int nb, const int *__restrict__ rp
             while (bits)
             {
                 const int b = __ffs(bits) - 1;
-                cic[pos++] = w * 32 + b;
+                if (pos < cap) // entries beyond the caller's capacity are not written
+                    cic[pos] = w * 32 + b;
+                ++pos;
                 bits &= bits - 1;
             }
             out += __shfl_sync(0xffffffffu, pre, 31);
@@ -264,7 +266,7 @@ __global__ void __launch_bounds__(256) spgemm_numeric_kernel(const SpNumArgs p)
 {
     const int lane = threadIdx.x & 31;
     const int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (c >= p.nnzc)
+    if (c >= p.nnzc || c >= p.rpc[p.mb]) // nnz_c may be an upper bound
         return;
     // block-row of this C tile: last i with rpc[i] <= c
     int lo = 0, hi = p.mb - 1;
@@ -649,7 +651,33 @@ int kami_spgemm_bsr_fill_colidx(int bsr, int mb, int kb, int nb, const int *row_
         return st;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     spgemm_colfill_kernel<<<(mb + wpc - 1) / wpc, wpc * 32, smem, s>>>(mb, nb, row_ptr_a, col_idx_a, row_ptr_b,
-                                                                      col_idx_b, row_ptr_c, col_idx_c);
+                                                                      col_idx_b, row_ptr_c, col_idx_c, INT64_MAX);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return cuda_fail(e, "spgemm_colfill_kernel");
+    return KAMI_OK;
+}
+
+int kami_spgemm_bsr_symbolic_device(int bsr, int mb, int kb, int nb, const int *row_ptr_a, const int *col_idx_a,
+                                    const int *row_ptr_b, const int *col_idx_b, int *row_ptr_c, int *col_idx_c,
+                                    int64_t capacity, void *stream)
+{
+    if (capacity < 0 || (capacity > 0 && !col_idx_c))
+        return fail(KAMI_ERR_INVALID_VALUE, "spgemm symbolic: capacity must be >= 0 with a column array");
+    // count + scan, with no copy of nnzC to the host
+    int st = kami_spgemm_bsr_symbolic(bsr, mb, kb, nb, row_ptr_a, col_idx_a, row_ptr_b, col_idx_b, row_ptr_c,
+                                      nullptr, stream);
+    if (st || mb == 0 || nb == 0 || capacity == 0)
+        return st;
+    int wpc;
+    size_t smem;
+    if ((st = bitmap_launch(nb, &wpc, &smem)))
+        return st;
+    if ((st = prep_bitmap_fn((const void *)spgemm_colfill_kernel, smem)))
+        return st;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    spgemm_colfill_kernel<<<(mb + wpc - 1) / wpc, wpc * 32, smem, s>>>(mb, nb, row_ptr_a, col_idx_a, row_ptr_b,
+                                                                      col_idx_b, row_ptr_c, col_idx_c, capacity);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess)
         return cuda_fail(e, "spgemm_colfill_kernel");
@@ -672,7 +700,8 @@ int kami_spgemm_bsr_numeric(kami_dtype_t in_type, kami_dtype_t out_type, int bsr
         return fail(KAMI_ERR_INVALID_VALUE, "spgemm numeric: num_iter >= 1 and nnz_c >= 0 required");
     if (nnz_c == 0 || mb == 0)
         return KAMI_OK;
-    if (!row_ptr_c || !col_idx_c || !val_a || !val_b || !val_c)
+    // val_a / val_b may be NULL for an operand without entries (nothing is read)
+    if (!row_ptr_c || !col_idx_c || !val_c)
         return fail(KAMI_ERR_INVALID_VALUE, "spgemm numeric: null pointer");
     if ((reinterpret_cast<uintptr_t>(val_a) & 7) || (reinterpret_cast<uintptr_t>(val_b) & 1) ||
         (reinterpret_cast<uintptr_t>(val_c) & 7))

@@ -64,7 +64,11 @@ def test_reference_generator_num_iter(cuda, num_iter):
 
 
 @pytest.mark.parametrize("mb,kb,nb,density", [(64, 64, 64, 0.05), (200, 37, 150, 0.1), (1, 1, 1, 1.0),
-                                              (33, 64, 1000, 0.02), (512, 512, 512, 0.01), (10, 10, 40, 0.0)])
+                                              (33, 64, 1000, 0.02), (512, 512, 512, 0.01), (10, 10, 40, 0.0),
+                                              # dense rows: more products per pass than the list holds,
+                                              # B lists beyond the staging capacity, more A tiles than it
+                                              (2, 32, 40, 1.0), (2, 32, 100, 1.0), (3, 40, 8, 1.0),
+                                              (5, 20, 300, 0.9)])
 def test_structure_and_values_exact(cuda, mb, kb, nb, density):
     A = random_bsr(mb, kb, density, 1, integer=True)
     B = random_bsr(kb, nb, density, 2, integer=True)
@@ -115,3 +119,41 @@ def test_empty_operands(cuda):
     B = random_bsr(4, 6, 0.5, 7, integer=True)
     rpc, cic, vc = run(A, B, 4, 4, 6)
     assert rpc.tolist() == [0] * 5 and len(cic) == 0
+
+
+@pytest.mark.parametrize("mb,kb,nb,density", [(64, 64, 64, 0.05), (200, 37, 150, 0.1), (512, 512, 512, 0.01),
+                                              (10, 10, 40, 0.0)])
+def test_symbolic_device_matches_host_and_numeric_bound(cuda, mb, kb, nb, density):
+    """The on-device symbolic pass gives the host pass's RowPtrC / ColIdxC,
+    and the numeric pass accepts its capacity as the bound of nnzC."""
+    A = random_bsr(mb, kb, density, 1, integer=True)
+    B = random_bsr(kb, nb, density, 2, integer=True)
+    dA, dB = to_dev(A, kb), to_dev(B, nb)
+    rpc_h, nnz = api.spgemm_symbolic(dA, dB)
+    cic_h = api.spgemm_fill_colidx(dA, dB, rpc_h, nnz)
+    cap = nnz + 37
+    rpc, cic = api.spgemm_symbolic_device(dA, dB, cap)
+    assert torch.equal(rpc, rpc_h) and int(rpc[-1]) == nnz
+    assert torch.equal(cic[:nnz], cic_h)
+    vals = torch.full((cap, 16, 16), -7.0, device="cuda")
+    api.spgemm_numeric_bound(dA, dB, rpc, cic, vals)
+    r = oracle.spgemm(mb, nb, A, B, accum="double")
+    assert np.array_equal(vals[:nnz].double().cpu().numpy(), r[2])
+    assert bool((vals[nnz:] == -7.0).all())
+
+
+def test_symbolic_device_capacity_respected(cuda):
+    A = random_bsr(40, 30, 0.2, 5, integer=True)
+    B = random_bsr(30, 50, 0.2, 6, integer=True)
+    dA, dB = to_dev(A, 30), to_dev(B, 50)
+    rpc_h, nnz = api.spgemm_symbolic(dA, dB)
+    cic_h = api.spgemm_fill_colidx(dA, dB, rpc_h, nnz)
+    cap = nnz // 2
+    cic = torch.full((cap + 16,), -1, dtype=torch.int32, device="cuda")
+    rpc = torch.empty(41, dtype=torch.int32, device="cuda")
+    from kami_b200 import _lib
+    assert _lib.load().kami_spgemm_bsr_symbolic_device(16, 40, 30, 50, dA.row_ptr.data_ptr(), dA.col_idx.data_ptr(),
+                                                       dB.row_ptr.data_ptr(), dB.col_idx.data_ptr(), rpc.data_ptr(),
+                                                       cic.data_ptr(), cap, None) == 0
+    assert int(rpc[-1]) == nnz  # the true count, beyond the capacity
+    assert torch.equal(cic[:cap], cic_h[:cap]) and bool((cic[cap:] == -1).all())
