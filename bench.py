@@ -63,7 +63,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="bounded CPU-baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="block",
-                    choices=["block", "block-sweep", "fp64", "split", "uneven", "spgemm", "spmm", "bmm"],
+                    choices=["block", "block-sweep", "fp64", "split", "uneven", "spgemm", "spmm", "bmm",
+                             "comparators"],
                     help="block (default, the headline line) or one of the other configurations; "
                          "non-default workloads print one JSON line per measured case")
     return ap.parse_args()
@@ -565,6 +566,69 @@ def run_secondary(args):
             _emit({"workload": "spmm", "case": f"n=16384, 1 % tiles, dense {Nd} columns, B {lay}",
                    "nnz_blocks": int(len(ci)), "ms": t, "tflops": fl / t / 1e9, "hbm_gbs": by / t / 1e6,
                    "frac_hbm": by / t / 1e6 / peak_bw, "max_abs_err_first_64_block_rows": err})
+        return
+
+    if args.workload == "comparators":
+        # the vendor library (cuBLAS through torch) on the same workloads and
+        # data as this library's kernels, side by side (context, not a target)
+        rng = np.random.default_rng(0)
+
+        def pair(name, ours, theirs, flops, by):
+            for impl, fn in (("kami_b200", ours), ("cublas", theirs)):
+                t = min(_time_ms(fn, W, K_, flush))
+                _emit({"workload": "comparators", "case": name, "impl": impl, "ms": t, "tflops": flops / t / 1e9,
+                       "hbm_gbs": by / t / 1e6 if by else None})
+
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        # FP16 128^3 x (4 x SMs), streamed (one product per problem)
+        b, n = 4 * sms, 128
+        A = torch.tensor(rng.uniform(-1, 1, (b, n, n)), device=dev).half()
+        B = torch.tensor(rng.uniform(-1, 1, (b, n, n)), device=dev).half()
+        Bt = B.transpose(1, 2)
+        C = torch.empty((b, n, n), dtype=torch.float32, device=dev)
+        C16 = torch.empty((b, n, n), dtype=torch.float16, device=dev)
+        pair("fp16 128^3 x 592 streamed (ours FP32 out, cuBLAS FP16 out)",
+             lambda: api.gemm_batched(A, B, C), lambda: torch.bmm(A, Bt, out=C16),
+             2.0 * n ** 3 * b, b * n * n * (2 + 2 + 4))
+        # FP64 64^3 x 8192 and 32^3 x 1024 streamed
+        for b, n in ((8192, 64), (1024, 32)):
+            A = torch.tensor(rng.uniform(-1, 1, (b, n, n)), device=dev)
+            B = torch.tensor(rng.uniform(-1, 1, (b, n, n)), device=dev)
+            Bt = B.transpose(1, 2)
+            C = torch.empty((b, n, n), dtype=torch.float64, device=dev)
+            pair(f"fp64 {n}^3 x {b} streamed", lambda: api.gemm_batched(A, B, C), lambda: torch.bmm(A, Bt, out=C),
+                 2.0 * n ** 3 * b, b * n * n * 24)
+        # BF16 bmm forward + backward, 4096 x 64^3
+        b, n = 4096, 64
+        A = torch.tensor(rng.uniform(-1, 1, (b, n, n)), device=dev).bfloat16().requires_grad_()
+        B = torch.tensor(rng.uniform(-1, 1, (b, n, n)), device=dev).bfloat16().requires_grad_()
+        G = torch.tensor(rng.uniform(-1, 1, (b, n, n)), device=dev).bfloat16()
+
+        def fb(f):
+            def step():
+                A.grad = None
+                B.grad = None
+                f(A, B).backward(G)
+            return step
+
+        pair("bf16 bmm fwd+bwd 4096 x 64^3", fb(bmm), fb(torch.bmm), 6.0 * n ** 3 * b, b * n * n * 2 * 9)
+        # uneven: 20000 problems in one graph launch vs one cuBLAS call per distinct shape (problems of equal
+        # shape batched together)
+        count = 20000
+        x = np.exp(rng.uniform(np.log(8), np.log(128), (count, 3)))
+        shapes = np.clip(8 * np.round(x / 8), 8, 128).astype(np.int64)
+        plan = api.GroupedPlan(shapes, torch.float16)
+        Ag = torch.rand(plan.sizes[0], device=dev).half()
+        Bg = torch.rand(plan.sizes[1], device=dev).half()
+        Cg = torch.empty(plan.sizes[2], dtype=plan.out_dtype, device=dev)
+        groups = {}
+        for (m_, n_, k_) in map(tuple, shapes):
+            groups[(m_, n_, k_)] = groups.get((m_, n_, k_), 0) + 1
+        tens = [(torch.rand((c_, m_, k_), device=dev).half(), torch.rand((c_, k_, n_), device=dev).half())
+                for (m_, n_, k_), c_ in groups.items()]
+        fl = float(sum(2 * m_ * n_ * k_ for m_, n_, k_ in map(tuple, shapes)))
+        pair(f"fp16 uneven 20000 problems ({len(groups)} distinct shapes)", lambda: plan.run(Ag, Bg, Cg),
+             lambda: [torch.bmm(a, b_) for a, b_ in tens], fl, None)
         return
 
     if args.workload == "bmm":

@@ -12,6 +12,8 @@
 
 namespace kami {
 
+int f64_stream_launch(const GemmArgs &g, cudaStream_t s);
+int f64s_read_error(int *flag);
 int split_read_error(int *flag);
 int grouped_fallback(const GemmArgs &g, int in_type, cudaStream_t stream);
 
@@ -245,11 +247,15 @@ int kami_device_status(int *code)
     int st = tc05_read_error(code);
     if (st)
         return st;
-    int c2 = 0;
+    int c2 = 0, c3 = 0;
     if ((st = split_read_error(&c2)))
+        return st;
+    if ((st = f64s_read_error(&c3)))
         return st;
     if (!*code)
         *code = c2;
+    if (!*code)
+        *code = c3;
     if (*code)
         return fail(KAMI_ERR_TIMEOUT, "a bounded device wait gave up (code %d)", *code);
     return KAMI_OK;
@@ -368,6 +374,18 @@ int kami_gemm_batched(kami_dtype_t in_type, kami_dtype_t out_type, kami_partitio
                        (variant == KAMI_VARIANT_AUTO && tc05_prefer_ts(M, a_layout));
         st = tc05_launch(g, in_type, partition, P, workspace, ws_bytes, s, ts);
         if (st == KAMI_OK || variant != KAMI_VARIANT_AUTO)
+            return st;
+    }
+
+    // streamed FP64 problems up to 64^3 (the batched FP64 programs' regime):
+    // the persistent kernel that overlaps each problem's loads with the
+    // DMMAs of the previous ones, when the choice is left to the library and
+    // there are at least two problems per SM (148 SMs)
+    if (in_type == KAMI_F64 && variant == KAMI_VARIANT_AUTO && partition == KAMI_PARTITION_AUTO && P == 0 &&
+        alloc_warps == 0 && num_iter <= 4 && batch >= 296)
+    {
+        st = f64_stream_launch(g, s);
+        if (st != KAMI_ERR_UNSUPPORTED)
             return st;
     }
 
