@@ -35,6 +35,7 @@
 #include <tuple>
 #include <vector>
 
+#include "grouped.cuh"
 #include "kami_common.cuh"
 #include "mma_engine.cuh"
 
@@ -42,26 +43,6 @@ namespace kami {
 
 int fail(int code, const char *fmt, ...);
 int cuda_fail(cudaError_t e, const char *what);
-
-struct GroupedDesc
-{
-    int M, N, K, cfg;
-    int64_t a_off, b_off, c_off;
-    int lda, ldb, ldc, pad_;
-};
-
-struct GroupedParams
-{
-    const GroupedDesc *desc; // problems in schedule order
-    const int *cta_begin;    // ctas + 1 offsets into desc
-    const void *A;
-    const void *B;
-    void *C;
-    int out_type;
-    double alpha, beta;
-    int num_iter;
-    int small_begin, small_end; // desc range of problems run by single warps
-};
 
 namespace {
 
@@ -83,11 +64,16 @@ struct GGeom
     static constexpr int KCH = ES == 2 ? 64 : 32; // K elements per chunk
     static constexpr int PAD = ES == 2 ? 16 : 8;  // row padding (elements) for conflict-free fragment loads
     static constexpr int LD = KCH + PAD;          // smem row stride (elements)
-    static constexpr int STAGES = ES == 2 ? 3 : 2;
-    static constexpr int OPER = 128 * LD * ES;    // bytes of one operand in a stage
-    static constexpr int STAGE = 2 * OPER;
+    static constexpr int ROW = LD * ES;           // bytes of one staged row
     static constexpr int RED = kWarps * 8 * 128 * (int)sizeof(typename Tr::Acc); // depth partials
-    static constexpr int SMEM = STAGES * STAGE + RED;
+    // byte ring of staged K chunks, each sized by its problem (the largest,
+    // 128 + 128 rows, is 40 KB for FP16 and 80 KB for FP64)
+    static constexpr int RING = ES == 2 ? 192 * 1024 : 160 * 1024;
+    static constexpr int SMEM = RING + RED;
+    static constexpr int MAXF = 8; // K chunks in flight at most (cp.async groups)
+    // ring bytes of one K chunk of a problem: A rows to a multiple of 16 and B
+    // rows to a multiple of 8, the rows the fragment loads touch
+    static __host__ __device__ int chunk_bytes(int M, int N) { return (((M + 15) & ~15) + ((N + 7) & ~7)) * ROW; }
 };
 
 __device__ __forceinline__ void cp_async16(void *dst, const void *src, bool valid)
@@ -100,6 +86,22 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
+// wait until at most n (< 8) cp.async groups of this thread are pending
+__device__ __forceinline__ void cp_async_wait_dyn(int n)
+{
+    switch (n)
+    {
+    case 0: cp_async_wait<0>(); break;
+    case 1: cp_async_wait<1>(); break;
+    case 2: cp_async_wait<2>(); break;
+    case 3: cp_async_wait<3>(); break;
+    case 4: cp_async_wait<4>(); break;
+    case 5: cp_async_wait<5>(); break;
+    case 6: cp_async_wait<6>(); break;
+    default: cp_async_wait<7>(); break;
+    }
+}
+
 template <class Tr>
 __device__ __forceinline__ void load_chunk(const GroupedParams &p, const GroupedDesc &d, int k0, uint8_t *stage)
 {
@@ -109,7 +111,7 @@ __device__ __forceinline__ void load_chunk(const GroupedParams &p, const Grouped
     const Elem *A = reinterpret_cast<const Elem *>(p.A) + d.a_off;
     const Elem *B = reinterpret_cast<const Elem *>(p.B) + d.b_off;
     Elem *sA = reinterpret_cast<Elem *>(stage);
-    Elem *sB = reinterpret_cast<Elem *>(stage + G::OPER);
+    Elem *sB = reinterpret_cast<Elem *>(stage + ((d.M + 15) & ~15) * G::ROW);
     const int epc = 16 / G::ES; // elements per 16-byte chunk
     for (int c = threadIdx.x; c < d.M * CPR; c += kThreads)
     {
@@ -157,7 +159,7 @@ __device__ __forceinline__ void compute_chunk(const GroupedDesc &d, const Tile &
     using Unit = typename Tr::Unit;
     using Elem = typename Tr::Elem;
     const Elem *sA = reinterpret_cast<const Elem *>(stage);
-    const Elem *sB = reinterpret_cast<const Elem *>(stage + G::OPER);
+    const Elem *sB = reinterpret_cast<const Elem *>(stage + ((d.M + 15) & ~15) * G::ROW);
     const int lane = threadIdx.x & 31, gq = lane >> 2, tq = lane & 3;
     const int kin = min(G::KCH, d.K - k0);
     const int ksteps = (kin + Tr::KSTEP - 1) / Tr::KSTEP;
@@ -349,44 +351,61 @@ __device__ __forceinline__ void warp_problem(const GroupedParams &p, const Group
             }
 }
 
-// The CTA-wide pipeline over this CTA's larger problems.
+// The CTA-wide pipeline over this CTA's larger problems.  K chunks are staged
+// in a byte ring, each at the size its problem needs, so that many small
+// chunks are in flight at once (up to MAXF cp.async groups): the loads are
+// latency-bound, not bandwidth-bound, per SM.  Every thread runs the same
+// allocator over the same chunk sequence, so producer and consumer agree on
+// where chunk u lives without any shared state: the producer side places
+// chunk after chunk at `head` (wrapping to 0 when the rest of the ring is too
+// short, the skipped bytes counted as part of that chunk), the consumer side
+// replays the same placement to find chunk u and frees it after its MMAs.
 template <class Tr>
 __device__ __forceinline__ void cta_problems(const GroupedParams &p, int begin, int end, uint8_t *smem)
 {
     using G = GGeom<Tr>;
-    using Acc = typename Tr::Acc;
-    uint8_t *red = smem + G::STAGES * G::STAGE;
-    // unit cursor for the loads (problem index, chunk start)
-    int lp = begin, lk = 0;
-    auto issue = [&](int slot) {
-        if (lp < end)
-        {
-            const GroupedDesc d = p.desc[lp];
-            load_chunk<Tr>(p, d, lk, smem + slot * G::STAGE);
-            lk += G::KCH;
-            if (lk >= d.K)
-            {
-                lk = 0;
-                ++lp;
-            }
-        }
-        cp_async_commit();
-    };
-#pragma unroll
-    for (int s = 0; s < G::STAGES - 1; ++s)
-        issue(s);
-
+    uint8_t *red = smem + G::RING;
+    // producer cursor: problem, chunk start, ring head, chunks issued
+    int lp = begin, lk = 0, head = 0, issued = 0;
+    int used = 0; // ring bytes held by chunks issued and not yet freed
+    // consumer cursor: problem, chunk start, ring position, chunks consumed
+    int cp = begin, ck = 0, chead = 0, u = 0;
+    GroupedDesc ld_desc = p.desc[begin];
     // accumulators (up to 16 fragments per warp), live across K chunks; each
     // register-tile shape indexes them as [ii * MJ + jj]
-    Acc acc[16][4];
-    int cp = begin, ck = 0, u = 0;
+    typename Tr::Acc acc[16][4];
     while (cp < end)
     {
-        issue((u + G::STAGES - 1) % G::STAGES);
-        cp_async_wait<G::STAGES - 1>();
+        // issue every chunk that fits, up to MAXF in flight
+        while (lp < end && issued - u < G::MAXF)
+        {
+            const int sz = G::chunk_bytes(ld_desc.M, ld_desc.N);
+            const bool wrap = head + sz > G::RING; // (head may equal RING: wrap with nothing skipped)
+            const int skip = wrap ? G::RING - head : 0;
+            if (used + skip + sz > G::RING)
+                break;
+            const int at = wrap ? 0 : head;
+            load_chunk<Tr>(p, ld_desc, lk, smem + at);
+            cp_async_commit();
+            head = at + sz;
+            used += skip + sz;
+            ++issued;
+            lk += GGeom<Tr>::KCH;
+            if (lk >= ld_desc.K)
+            {
+                lk = 0;
+                if (++lp < end)
+                    ld_desc = p.desc[lp];
+            }
+        }
+        cp_async_wait_dyn(issued - u - 1);
         __syncthreads();
         const GroupedDesc d = p.desc[cp];
-        const uint8_t *stage = smem + (u % G::STAGES) * G::STAGE;
+        const int sz = G::chunk_bytes(d.M, d.N);
+        const bool wrap = chead + sz > G::RING;
+        const int skip = wrap ? G::RING - chead : 0;
+        const int at = wrap ? 0 : chead;
+        const uint8_t *stage = smem + at;
         const bool first = ck == 0, last = ck + G::KCH >= d.K;
         switch (d.cfg)
         {
@@ -403,7 +422,9 @@ __device__ __forceinline__ void cta_problems(const GroupedParams &p, int begin, 
             run_chunk<Tr, 2, 4>(p, d, ck, first, last, stage, red, acc);
             break;
         }
-        __syncthreads();
+        __syncthreads(); // every warp is done with chunk u: its bytes are free
+        chead = at + sz;
+        used -= skip + sz;
         ck += G::KCH;
         if (last)
         {
@@ -441,6 +462,8 @@ using namespace kami;
 struct kami_grouped_plan
 {
     int in_type, out_type, count, ctas, smem;
+    int kernel = 0; // 0: mma.sync warp grids (grouped_kernel), 1: tcgen05 (grouped_tc05_kernel)
+    int tc_m64 = 0, tc_m128 = 0; // tcgen05 plans: problems on M = 64 / M = 128 MMAs
     int small_begin = 0, small_end = 0; // desc range of single-warp problems
     GroupedDesc *d_desc = nullptr;
     int *d_begin = nullptr;
@@ -526,6 +549,8 @@ static int launch_grouped(const kami_grouped_plan *plan, const void *A, const vo
     p.num_iter = num_iter;
     p.small_begin = plan->small_begin;
     p.small_end = plan->small_end;
+    if (plan->kernel == 1)
+        return grouped_tc05_launch(p, plan->in_type == KAMI_BF16, plan->ctas, s);
     void *args[] = {&p};
     cudaError_t e = cudaLaunchKernel(grouped_fn(plan->in_type), dim3(plan->ctas), dim3(kThreads), args,
                                      (size_t)plan->smem, s);
@@ -547,11 +572,14 @@ static int free_plan(kami_grouped_plan *pl)
 }
 
 // Build descriptors + LPT schedule for `count` problems (host arrays) with
-// the given partitions and upload them.
+// the given partitions and upload them.  kernel 1 (FP16 / BF16 only) is the
+// tcgen05 kernel: every problem goes through its CTA pipeline (no
+// single-warp problems) and the cost model is its bytes plus a fixed
+// per-problem latency.
 static int build_plan(int in_type, int out_type, int count, const int *M, const int *N, const int *K,
                       const int64_t *ao, const int64_t *bo, const int64_t *co, const int *cfg,
                       kami_grouped_plan **out, const int *lda = nullptr, const int *ldb = nullptr,
-                      const int *ldc = nullptr)
+                      const int *ldc = nullptr, int kernel = 0)
 {
     int dev = 0, sms = 0, occ = 0;
     cudaError_t e;
@@ -559,17 +587,21 @@ static int build_plan(int in_type, int out_type, int count, const int *M, const 
         return cuda_fail(e, "cudaGetDevice");
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
         return cuda_fail(e, "cudaDeviceGetAttribute");
-    const void *fn = grouped_fn(in_type);
-    const int smem = grouped_smem(in_type);
+    const bool tc = kernel == 1;
+    const void *fn = tc ? grouped_tc05_fn(in_type == KAMI_BF16) : grouped_fn(in_type);
+    const int smem = tc ? grouped_tc05_smem() : grouped_smem(in_type);
+    const int threads = tc ? grouped_tc05_threads() : kThreads;
     if ((e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
-        return cuda_fail(e, "cudaFuncSetAttribute(grouped_kernel)");
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kThreads, smem)) != cudaSuccess)
+        return cuda_fail(e, "cudaFuncSetAttribute(grouped kernel)");
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, smem)) != cudaSuccess)
         return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     occ = std::max(occ, 1);
     const int ctas = std::max(1, std::min(count, sms * occ));
     const int esz = in_type == KAMI_F64 ? 8 : 2;
     const int osz = out_type == KAMI_F64 ? 8 : out_type == KAMI_F32 ? 4 : 2;
-    const double balance = in_type == KAMI_F64 ? 6.0 : 150.0; // FLOP per byte where compute and HBM meet
+    // FLOP per byte where compute and HBM meet (the tcgen05 kernel's MMAs
+    // are never the bound at these sizes)
+    const double balance = in_type == KAMI_F64 ? 6.0 : tc ? 1e9 : 150.0;
 
     auto *pl = new kami_grouped_plan();
     pl->in_type = in_type;
@@ -577,6 +609,7 @@ static int build_plan(int in_type, int out_type, int count, const int *M, const 
     pl->count = count;
     pl->ctas = ctas;
     pl->smem = smem;
+    pl->kernel = kernel;
     std::vector<double> cost(count);
     std::vector<int> order(count);
     for (int i = 0; i < count; ++i)
@@ -587,7 +620,10 @@ static int build_plan(int in_type, int out_type, int count, const int *M, const 
         order[i] = i;
         pl->flops += (int64_t)fl;
         pl->bytes += (int64_t)by;
-        pl->cfg_hist[cfg[i]]++;
+        if (tc)
+            (M[i] <= 64 ? pl->tc_m64 : pl->tc_m128)++;
+        else
+            pl->cfg_hist[cfg[i]]++;
     }
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
     typedef std::pair<double, int> Load;
@@ -598,7 +634,7 @@ static int build_plan(int in_type, int out_type, int count, const int *M, const 
     std::vector<int> smalls;
     for (int i : order)
     {
-        if (cfg[i] == 7)
+        if (cfg[i] == 7 && !tc)
         {
             smalls.push_back(i); // longest first, spread over all warps round-robin
             continue;
@@ -740,7 +776,7 @@ int grouped_fallback(const GemmArgs &g, int in_type, cudaStream_t stream)
             co[i] = (int64_t)i * g.sC;
         }
         int st = build_plan(in_type, g.out_type, n, vm.data(), vn.data(), vk.data(), ao.data(), bo.data(), co.data(),
-                            vc.data(), &pl, la.data(), lb.data(), lc.data());
+                            vc.data(), &pl, la.data(), lb.data(), lc.data(), in_type == KAMI_F64 ? 0 : 1);
         if (st)
             return st;
         std::lock_guard<std::mutex> lk(mu);
@@ -768,6 +804,11 @@ int kami_gemm_grouped_plan_create(kami_dtype_t in_type, kami_dtype_t out_type, i
         return fail(KAMI_ERR_UNSUPPORTED, "grouped: output type does not match the input type");
     if (count < 0 || (count > 0 && (!M || !N || !K || !a_offsets || !b_offsets || !c_offsets)))
         return fail(KAMI_ERR_INVALID_VALUE, "grouped: bad count or null shape/offset arrays");
+    const bool force_mma = (flags & KAMI_PLAN_MMA_SYNC) != 0, force_tc = (flags & KAMI_PLAN_TCGEN05) != 0;
+    if (force_mma && force_tc)
+        return fail(KAMI_ERR_INVALID_VALUE, "grouped: KAMI_PLAN_MMA_SYNC and KAMI_PLAN_TCGEN05 are exclusive");
+    if (force_tc && in_type == KAMI_F64)
+        return fail(KAMI_ERR_UNSUPPORTED, "grouped: the tcgen05 kernel takes FP16 / BF16 inputs");
     const int kq = in_type == KAMI_F64 ? 2 : 8;
     for (int i = 0; i < count; ++i)
     {
@@ -855,7 +896,77 @@ int kami_gemm_grouped_plan_create(kami_dtype_t in_type, kami_dtype_t out_type, i
             cfg[i] = cfg_valid(c, M[i], N[i]) ? c : cfg_heuristic(in_type, M[i], N[i], K[i]);
         }
     }
-    return build_plan(in_type, out_type, count, M, N, K, a_offsets, b_offsets, c_offsets, cfg.data(), plan);
+    if (in_type == KAMI_F64 || force_mma)
+        return build_plan(in_type, out_type, count, M, N, K, a_offsets, b_offsets, c_offsets, cfg.data(), plan);
+    if (force_tc || !tune || count == 0)
+        return build_plan(in_type, out_type, count, M, N, K, a_offsets, b_offsets, c_offsets, cfg.data(), plan,
+                          nullptr, nullptr, nullptr, 1);
+    // autotuned, kernel not forced: build both kernels' plans, time each on
+    // scratch buffers of the plan's extent, keep the faster
+    kami_grouped_plan *pl[2] = {nullptr, nullptr};
+    for (int k = 0; k < 2; ++k)
+    {
+        int st = build_plan(in_type, out_type, count, M, N, K, a_offsets, b_offsets, c_offsets, cfg.data(), &pl[k],
+                            nullptr, nullptr, nullptr, k);
+        if (st)
+        {
+            free_plan(pl[0]);
+            return st;
+        }
+    }
+    int64_t na = 0, nb = 0, nc = 0;
+    for (int i = 0; i < count; ++i)
+    {
+        na = std::max(na, a_offsets[i] + (int64_t)M[i] * K[i]);
+        nb = std::max(nb, b_offsets[i] + (int64_t)N[i] * K[i]);
+        nc = std::max(nc, c_offsets[i] + (int64_t)M[i] * N[i]);
+    }
+    const int osz = out_type == KAMI_F32 ? 4 : 2;
+    void *tA = nullptr, *tB = nullptr, *tC = nullptr;
+    cudaError_t e;
+    if ((e = cudaMalloc(&tA, (size_t)na * 2)) != cudaSuccess || (e = cudaMalloc(&tB, (size_t)nb * 2)) != cudaSuccess ||
+        (e = cudaMalloc(&tC, (size_t)nc * osz)) != cudaSuccess)
+    {
+        cudaFree(tA);
+        cudaFree(tB);
+        free_plan(pl[0]);
+        free_plan(pl[1]);
+        return cuda_fail(e, "cudaMalloc(grouped kernel choice scratch)");
+    }
+    cudaMemset(tA, 0, (size_t)na * 2);
+    cudaMemset(tB, 0, (size_t)nb * 2);
+    float ms[2] = {0.f, 0.f};
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int st = KAMI_OK;
+    for (int k = 0; k < 2 && st == KAMI_OK; ++k)
+    {
+        st = launch_grouped(pl[k], tA, tB, tC, 1.0, 0.0, 1, 0);
+        cudaEventRecord(e0, 0);
+        for (int r = 0; r < 3 && st == KAMI_OK; ++r)
+            st = launch_grouped(pl[k], tA, tB, tC, 1.0, 0.0, 1, 0);
+        cudaEventRecord(e1, 0);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(&ms[k], e0, e1);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st == KAMI_OK && (e = cudaGetLastError()) != cudaSuccess)
+        st = cuda_fail(e, "grouped kernel choice");
+    cudaFree(tA);
+    cudaFree(tB);
+    cudaFree(tC);
+    if (st)
+    {
+        free_plan(pl[0]);
+        free_plan(pl[1]);
+        return st;
+    }
+    const int keep = ms[1] <= ms[0] ? 1 : 0;
+    free_plan(pl[1 - keep]);
+    *plan = pl[keep];
+    return KAMI_OK;
 }
 
 int kami_gemm_grouped_run(const kami_grouped_plan *plan, const void *A, const void *B, void *C, double alpha,
@@ -886,8 +997,9 @@ int kami_gemm_grouped_plan_info(const kami_grouped_plan *plan, int64_t out[16])
     out[4] = plan->bytes;
     for (int c = 0; c < kCfgs; ++c)
         out[5 + c] = plan->cfg_hist[c];
-    for (int c = 5 + kCfgs; c < 16; ++c)
-        out[c] = 0;
+    out[13] = plan->kernel;
+    out[14] = plan->tc_m64;
+    out[15] = plan->tc_m128;
     return KAMI_OK;
 }
 

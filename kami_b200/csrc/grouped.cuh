@@ -1,0 +1,39 @@
+// grouped.cuh -- device descriptors of the uneven (grouped) batched GEMM,
+// shared by its two kernels: the mma.sync warp-grid kernel (grouped.cu) and
+// the tcgen05 kernel (grouped_tc05.cu).
+#pragma once
+#include "kami_common.cuh"
+
+namespace kami {
+
+// One problem: shape, warp partition (mma.sync kernel), element offsets of
+// A (M x K), B (N x K) and C (M x N) and their leading dimensions.
+struct GroupedDesc
+{
+    int M, N, K, cfg;
+    int64_t a_off, b_off, c_off;
+    int lda, ldb, ldc, pad_;
+};
+
+struct GroupedParams
+{
+    const GroupedDesc *desc; // problems in schedule order
+    const int *cta_begin;    // ctas + 1 offsets into desc
+    const void *A;
+    const void *B;
+    void *C;
+    int out_type;
+    double alpha, beta;
+    int num_iter;
+    int small_begin, small_end; // desc range of problems run by single warps
+};
+
+// tcgen05 grouped kernel (grouped_tc05.cu): entry point, launch geometry and
+// the device status of its bounded waits.
+const void *grouped_tc05_fn(bool bf16);
+int grouped_tc05_threads();
+int grouped_tc05_smem();
+int grouped_tc05_launch(const GroupedParams &p, bool bf16, int ctas, cudaStream_t s);
+int grouped_tc05_read_error(int *flag);
+
+} // namespace kami

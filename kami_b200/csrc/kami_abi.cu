@@ -14,6 +14,7 @@ namespace kami {
 
 int f64_stream_launch(const GemmArgs &g, cudaStream_t s);
 int f64s_read_error(int *flag);
+int grouped_tc05_read_error(int *flag);
 int split_read_error(int *flag);
 int grouped_fallback(const GemmArgs &g, int in_type, cudaStream_t stream);
 
@@ -247,15 +248,19 @@ int kami_device_status(int *code)
     int st = tc05_read_error(code);
     if (st)
         return st;
-    int c2 = 0, c3 = 0;
+    int c2 = 0, c3 = 0, c4 = 0;
     if ((st = split_read_error(&c2)))
         return st;
     if ((st = f64s_read_error(&c3)))
+        return st;
+    if ((st = grouped_tc05_read_error(&c4)))
         return st;
     if (!*code)
         *code = c2;
     if (!*code)
         *code = c3;
+    if (!*code)
+        *code = c4;
     if (*code)
         return fail(KAMI_ERR_TIMEOUT, "a bounded device wait gave up (code %d)", *code);
     return KAMI_OK;

@@ -1,6 +1,7 @@
 """Uneven grouped GEMM (one persistent launch) against the CPU oracle, with
-the static and the autotuned partition choice, FP16/BF16->FP32 and FP64, and
-inside a captured CUDA graph."""
+the static and the autotuned partition choice, both kernels (mma.sync warp
+grids and tcgen05), FP16/BF16->FP32 and FP64, and inside a captured CUDA
+graph."""
 import numpy as np
 import pytest
 import torch
@@ -52,7 +53,9 @@ def test_grouped_exact(cuda, dtype, autotune):
     As, Bs, A, B = make_inputs(shapes, dtype, 1)
     plan = api.GroupedPlan(shapes, dtype, autotune=autotune)
     info = plan.info()
-    assert info["problems"] == 600 and sum(info["partitions"]) == 600
+    assert info["problems"] == 600
+    assert sum(info["partitions"]) + info["tcgen05_m64"] + info["tcgen05_m128"] == 600
+    assert info["kernel"] == ("mma_sync" if dtype == torch.float64 else "tcgen05" if not autotune else info["kernel"])
     C = torch.empty(plan.sizes[2], dtype=plan.out_dtype, device="cuda")
     plan.run(A, B, C)
     torch.cuda.synchronize()
@@ -72,7 +75,8 @@ def test_grouped_every_partition(cuda):
     # the same problems under every partition must give identical results
     shapes = np.array([[32, 32, 64], [64, 24, 128], [16, 64, 8], [8, 8, 8], [64, 64, 40]] * 20)
     As, Bs, A, B = make_inputs(shapes, torch.float16, 2)
-    plan = api.GroupedPlan(shapes, torch.float16, autotune=True)
+    plan = api.GroupedPlan(shapes, torch.float16, autotune=True, kernel="mma_sync")
+    assert plan.info()["kernel"] == "mma_sync"
     C = torch.empty(plan.sizes[2], dtype=torch.float32, device="cuda")
     plan.run(A, B, C, num_iter=3)
     Ch = C.double().cpu().numpy() / 3
@@ -104,17 +108,111 @@ def test_grouped_cuda_graph(cuda):
     check(plan, As2, Bs2, C)
 
 
-def test_grouped_alpha_beta_out_types(cuda):
+@pytest.mark.parametrize("kernel", ["mma_sync", "tcgen05"])
+@pytest.mark.parametrize("out_dtype", [torch.float16, torch.bfloat16, torch.float32])
+def test_grouped_alpha_beta_out_types(cuda, kernel, out_dtype):
     shapes = uneven_shapes(100, 7)
     As, Bs, A, B = make_inputs(shapes, torch.float16, 8)
-    plan = api.GroupedPlan(shapes, torch.float16, out_dtype=torch.float16)
-    C = torch.full((plan.sizes[2],), 1.0, dtype=torch.float16, device="cuda")
+    plan = api.GroupedPlan(shapes, torch.float16, out_dtype=out_dtype, kernel=kernel)
+    assert plan.info()["kernel"] == kernel
+    C = torch.full((plan.sizes[2],), 1.0, dtype=out_dtype, device="cuda")
     plan.run(A, B, C, alpha=2.0, beta=-1.0)
     Ch = C.double().cpu().numpy()
     for i, (m, n, k) in enumerate(plan.shapes):
         ref = 2 * oracle.gemm(As[i][None], Bs[i][None])[0] - 1
-        ref16 = ref.astype(np.float16).astype(np.float64)
-        assert np.array_equal(Ch[plan.offsets[2][i]:plan.offsets[2][i] + m * n].reshape(m, n), ref16)
+        # exact integers in FP32; one rounding to the output type
+        ref = torch.tensor(ref, dtype=torch.float32).to(out_dtype).double().numpy()
+        assert np.array_equal(Ch[plan.offsets[2][i]:plan.offsets[2][i] + m * n].reshape(m, n), ref)
+
+
+@pytest.mark.parametrize("dtype", [torch.float16, torch.bfloat16])
+@pytest.mark.parametrize("num_iter", [1, 3])
+def test_grouped_tcgen05_edge_shapes(cuda, dtype, num_iter):
+    """The tcgen05 kernel at the edges of its tiling: K of one partial k-step
+    (8), K across two chunks with a partial last step (72, 120), M at the
+    64 / 128 MMA boundary (64, 65), N not a multiple of 16, single rows."""
+    shapes = np.array([[8, 8, 8], [64, 16, 72], [65, 24, 120], [128, 128, 128], [1, 8, 8], [17, 40, 64],
+                       [64, 64, 64], [100, 8, 16], [8, 128, 24], [127, 121, 112]] * 7)
+    As, Bs, A, B = make_inputs(shapes, dtype, 11)
+    plan = api.GroupedPlan(shapes, dtype, kernel="tcgen05")
+    info = plan.info()
+    assert info["kernel"] == "tcgen05" and info["tcgen05_m64"] + info["tcgen05_m128"] == len(shapes)
+    C = torch.full((plan.sizes[2],), -5.0, dtype=torch.float32, device="cuda")
+    plan.run(A, B, C, num_iter=num_iter)
+    torch.cuda.synchronize()
+    Ch = C.double().cpu().numpy() / num_iter
+    for i, (m, n, k) in enumerate(plan.shapes):
+        ref = oracle.gemm(As[i][None], Bs[i][None])[0]
+        assert np.array_equal(Ch[plan.offsets[2][i]:plan.offsets[2][i] + m * n].reshape(m, n), ref), (i, m, n, k)
+
+
+def test_grouped_tcgen05_few_problems_and_offsets(cuda):
+    """Fewer problems than SMs, and problems at caller offsets with gaps
+    between them (the gaps must stay untouched)."""
+    shapes = np.array([[40, 56, 32], [128, 8, 64], [8, 96, 104]])
+    As, Bs, _, _ = make_inputs(shapes, torch.float16, 12)
+    ao = np.array([0, 40 * 32 + 64, 40 * 32 + 64 + 128 * 64 + 8], dtype=np.int64)
+    bo = np.array([16, 16 + 56 * 32 + 8, 16 + 56 * 32 + 8 + 8 * 64 + 32], dtype=np.int64)
+    co = np.array([4, 4 + 40 * 56 + 13, 4 + 40 * 56 + 13 + 128 * 8 + 100], dtype=np.int64)
+    A = torch.zeros(int(ao[-1]) + 8 * 104, dtype=torch.float16, device="cuda")
+    B = torch.zeros(int(bo[-1]) + 96 * 104, dtype=torch.float16, device="cuda")
+    for i, (m, n, k) in enumerate(shapes):
+        A[ao[i]:ao[i] + m * k] = torch.tensor(As[i].ravel(), dtype=torch.float16)
+        B[bo[i]:bo[i] + n * k] = torch.tensor(Bs[i].ravel(), dtype=torch.float16)
+    C = torch.full((int(co[-1]) + 8 * 96 + 16,), 7.0, dtype=torch.float32, device="cuda")
+    plan = api.GroupedPlan(shapes, torch.float16, offsets=(ao, bo, co), kernel="tcgen05")
+    plan.run(A, B, C)
+    Ch = C.double().cpu().numpy()
+    mask = np.ones(Ch.size, bool)
+    for i, (m, n, k) in enumerate(shapes):
+        ref = oracle.gemm(As[i][None], Bs[i][None])[0]
+        assert np.array_equal(Ch[co[i]:co[i] + m * n].reshape(m, n), ref)
+        mask[co[i]:co[i] + m * n] = False
+    assert np.all(Ch[mask] == 7.0)
+
+
+def test_grouped_tcgen05_more_problems_than_cached(cuda):
+    """More problems per CTA than the kernel's shared-memory descriptor cache
+    holds (the rest are read from global memory)."""
+    rng = np.random.default_rng(15)
+    shapes = np.stack([rng.choice([8, 16, 24], 60000), rng.choice([8, 16], 60000), rng.choice([8, 16], 60000)], 1)
+    As, Bs, A, B = make_inputs(shapes, torch.float16, 16)
+    plan = api.GroupedPlan(shapes, torch.float16, kernel="tcgen05")
+    assert plan.info()["problems"] // plan.info()["ctas"] > 256
+    C = torch.empty(plan.sizes[2], dtype=torch.float32, device="cuda")
+    plan.run(A, B, C)
+    Ch = C.double().cpu().numpy()
+    co = plan.offsets[2]
+    for i in list(range(0, 60000, 997)) + [59999]:
+        m, n, k = plan.shapes[i]
+        ref = oracle.gemm(As[i][None], Bs[i][None])[0]
+        assert np.array_equal(Ch[co[i]:co[i] + m * n].reshape(m, n), ref), i
+
+
+def test_grouped_kernels_agree_on_reals(cuda):
+    """mma.sync and tcgen05 plans of the same uniform[-1, 1] problems agree
+    within the FP32-accumulation bound of each against the oracle."""
+    shapes = uneven_shapes(400, 13)
+    As, Bs, A, B = make_inputs(shapes, torch.float16, 14, integer=False)
+    A64 = [torch.tensor(a, dtype=torch.float16).double().numpy() for a in As]
+    B64 = [torch.tensor(b, dtype=torch.float16).double().numpy() for b in Bs]
+    for kernel in ("mma_sync", "tcgen05"):
+        plan = api.GroupedPlan(shapes, torch.float16, kernel=kernel)
+        C = torch.empty(plan.sizes[2], dtype=torch.float32, device="cuda")
+        plan.run(A, B, C)
+        Ch = C.double().cpu().numpy()
+        for i, (m, n, k) in enumerate(plan.shapes):
+            ref = A64[i] @ B64[i].T
+            bound = (k + 2) * 2.0 ** -23 * (np.abs(A64[i]) @ np.abs(B64[i]).T) + 1e-30
+            got = Ch[plan.offsets[2][i]:plan.offsets[2][i] + m * n].reshape(m, n)
+            assert np.all(np.abs(got - ref) <= bound), (kernel, i)
+
+
+def test_grouped_status_clean(cuda):
+    import ctypes
+    from kami_b200 import _lib
+    code = ctypes.c_int(0)
+    assert _lib.load().kami_device_status(ctypes.byref(code)) == 0 and code.value == 0
 
 
 def test_grouped_rejects_bad_shapes(cuda):
@@ -122,3 +220,5 @@ def test_grouped_rejects_bad_shapes(cuda):
         api.GroupedPlan([[200, 8, 8]], torch.float16)
     with pytest.raises(Exception):
         api.GroupedPlan([[8, 8, 12]], torch.float16)
+    with pytest.raises(Exception):
+        api.GroupedPlan([[8, 8, 8]], torch.float64, kernel="tcgen05")
