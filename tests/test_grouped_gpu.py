@@ -175,15 +175,16 @@ def test_grouped_tcgen05_more_problems_than_cached(cuda):
     """More problems per CTA than the kernel's shared-memory descriptor cache
     holds (the rest are read from global memory)."""
     rng = np.random.default_rng(15)
-    shapes = np.stack([rng.choice([8, 16, 24], 60000), rng.choice([8, 16], 60000), rng.choice([8, 16], 60000)], 1)
+    count = 90000
+    shapes = np.stack([rng.choice([8, 16, 24], count), rng.choice([8, 16], count), rng.choice([8, 16], count)], 1)
     As, Bs, A, B = make_inputs(shapes, torch.float16, 16)
     plan = api.GroupedPlan(shapes, torch.float16, kernel="tcgen05")
-    assert plan.info()["problems"] // plan.info()["ctas"] > 256
+    assert plan.info()["problems"] // plan.info()["ctas"] > 512
     C = torch.empty(plan.sizes[2], dtype=torch.float32, device="cuda")
     plan.run(A, B, C)
     Ch = C.double().cpu().numpy()
     co = plan.offsets[2]
-    for i in list(range(0, 60000, 997)) + [59999]:
+    for i in list(range(0, count, 997)) + [count - 1]:
         m, n, k = plan.shapes[i]
         ref = oracle.gemm(As[i][None], Bs[i][None])[0]
         assert np.array_equal(Ch[co[i]:co[i] + m * n].reshape(m, n), ref), i
