@@ -285,8 +285,11 @@ int kami_spgemm_bsr_fill_colidx(int bsr, int mb, int kb, int nb,
                                 const int *row_ptr_c, int *col_idx_c, void *stream);
 
 /* The symbolic pass and the column fill in one call with no copy to the
- * host and no synchronisation (three kernels on `stream`, so the whole
- * SpGEMM can run inside one stream or graph): row_ptr_c[0..mb] as in
+ * host and no synchronisation: one cooperative kernel on `stream` whose
+ * count, scan and fill phases meet at bounded grid barriers (preceded by an
+ * 8-byte memset of its barrier word; devices without cooperative launch get
+ * the three separate kernels), so the whole SpGEMM can run inside one stream
+ * or graph.  row_ptr_c[0..mb] as in
  * kami_spgemm_bsr_symbolic, nnzC = row_ptr_c[mb] left on the device, and
  * col_idx_c filled up to `capacity` entries (the caller's upper bound for
  * nnzC, e.g. mb * nb or the sum of B row lengths over A's entries; entries

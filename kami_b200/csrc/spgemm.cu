@@ -26,7 +26,9 @@
 //     m16n8k16 MMAs (FP32 accumulation) in ascending k -- the order of the
 //     reference's sparse accumulator.  No C tile is touched twice, so the
 //     kernel writes C once (the HBM floor of the product).
+#include <atomic>
 #include <cstdint>
+#include <mutex>
 
 #include "kami_common.cuh"
 
@@ -34,6 +36,15 @@ namespace kami {
 
 int fail(int code, const char *fmt, ...);
 int cuda_fail(cudaError_t e, const char *what);
+
+// Grid barriers of the fused symbolic pass: [slot][0] arrivals, [slot][1]
+// generation.  Each launch takes the next slot (zeroed on its stream just
+// before it), so launches in flight on different streams do not share one.
+constexpr int kFuseSlots = 64;
+__device__ unsigned int g_spg_bar[kFuseSlots][2];
+// device status of the fused pass's bounded barrier waits (read and cleared
+// by kami_device_status)
+__device__ int g_spg_error = 0;
 
 namespace {
 
@@ -168,6 +179,191 @@ __global__ void spgemm_colfill_kernel(int mb, int nb, const int *__restrict__ rp
             {
                 const int b = __ffs(bits) - 1;
                 if (pos < cap) // entries beyond the caller's capacity are not written
+                    cic[pos] = w * 32 + b;
+                ++pos;
+                bits &= bits - 1;
+            }
+            out += __shfl_sync(0xffffffffu, pre, 31);
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The symbolic pass in ONE launch: count, scan and column fill as phases of a
+// cooperative persistent kernel, separated by grid barriers (the reference
+// runs three launches with a device-to-host copy of nnzC between them,
+// block_spgemm_2d_half_mma.cu:805-812).  A cooperative launch keeps every CTA
+// resident, so the barrier cannot wait for a CTA that never runs; its waits
+// are bounded all the same, and a timeout sets g_spg_error and ends the CTA.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t spg_globaltimer()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Every CTA of the grid arrives; returns false (block-uniform) on a timeout.
+__device__ __forceinline__ bool spg_grid_barrier(unsigned int *bar, uint64_t limit_ns)
+{
+    __syncthreads();
+    int ok = 1;
+    if (threadIdx.x == 0)
+    {
+        volatile unsigned int *gen = bar + 1;
+        const unsigned int g0 = *gen;
+        __threadfence(); // the generation read and this CTA's writes precede its arrival
+        if (atomicAdd(bar, 1u) == gridDim.x - 1)
+        {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        }
+        else
+        {
+            const uint64_t t0 = spg_globaltimer();
+            while (*gen == g0)
+            {
+                if (spg_globaltimer() - t0 > limit_ns)
+                {
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    return __syncthreads_and(ok) != 0;
+}
+
+// In-place exclusive scan of rpc[0..n-1] by the calling CTA; total in rpc[n].
+__device__ __forceinline__ void spg_block_scan(int n, int *__restrict__ rpc)
+{
+    __shared__ int warp_sums[32];
+    __shared__ int carry_s;
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5, nw = blockDim.x >> 5;
+    if (t == 0)
+        carry_s = 0;
+    __syncthreads();
+    for (int base = 0; base < n; base += blockDim.x)
+    {
+        const int i = base + t;
+        const int v = i < n ? rpc[i] : 0;
+        int x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o)
+                x += y;
+        }
+        if (lane == 31)
+            warp_sums[wid] = x;
+        __syncthreads();
+        if (wid == 0)
+        {
+            int sum = lane < nw ? warp_sums[lane] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1)
+            {
+                const int y = __shfl_up_sync(0xffffffffu, sum, o);
+                if (lane >= o)
+                    sum += y;
+            }
+            if (lane < nw)
+                warp_sums[lane] = sum; // inclusive over warps
+        }
+        __syncthreads();
+        const int carry = carry_s;
+        const int incl = x + (wid > 0 ? warp_sums[wid - 1] : 0);
+        if (i < n)
+            rpc[i] = carry + incl - v;
+        __syncthreads();
+        if (t == (int)blockDim.x - 1)
+            carry_s = carry + incl;
+        __syncthreads();
+    }
+    if (t == 0)
+        rpc[n] = carry_s;
+}
+
+// keep_rows > 0: every warp holds at most keep_rows block-rows and keeps
+// each row's bitmap in shared memory from phase 1 to phase 3 (the column fill
+// then re-reads neither A's row nor B's rows); 0: one bitmap per warp,
+// rebuilt in phase 3.
+__global__ void spgemm_symbolic_fused_kernel(int mb, int nb, const int *__restrict__ rpa,
+                                             const int *__restrict__ cia, const int *__restrict__ rpb,
+                                             const int *__restrict__ cib, int *__restrict__ rpc,
+                                             int *__restrict__ cic, int64_t cap, unsigned int *bar,
+                                             uint64_t limit_ns, int keep_rows)
+{
+    extern __shared__ uint32_t bm_all[];
+    const int words = (nb + 31) >> 5;
+    const int wpc = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int keep = keep_rows > 0;
+    uint32_t *bm_warp = bm_all + (size_t)(threadIdx.x >> 5) * (keep ? keep_rows : 1) * words;
+    // phase 1: nnz of every C block-row
+    int r = 0;
+    for (int row = blockIdx.x * wpc + (threadIdx.x >> 5); row < mb; row += gridDim.x * wpc, ++r)
+    {
+        uint32_t *bm = bm_warp + (keep ? r * words : 0);
+        build_row_bitmap(bm, words, row, rpa, cia, rpb, cib, lane);
+        int cnt = 0;
+        for (int w = lane; w < words; w += 32)
+            cnt += __popc(bm[w]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+            cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+        if (lane == 0)
+            rpc[row] = cnt;
+        __syncwarp();
+    }
+    if (!spg_grid_barrier(bar, limit_ns))
+    {
+        if (threadIdx.x == 0)
+            atomicExch(&g_spg_error, 1);
+        return;
+    }
+    // phase 2: exclusive scan into RowPtrC (one CTA; the others wait)
+    if (blockIdx.x == 0)
+        spg_block_scan(mb, rpc);
+    if (!spg_grid_barrier(bar, limit_ns))
+    {
+        if (threadIdx.x == 0)
+            atomicExch(&g_spg_error, 2);
+        return;
+    }
+    if (cap == 0)
+        return;
+    // phase 3: ColIdxC, ascending per block-row, up to the capacity
+    r = 0;
+    for (int row = blockIdx.x * wpc + (threadIdx.x >> 5); row < mb; row += gridDim.x * wpc, ++r)
+    {
+        uint32_t *bm = bm_warp + (keep ? r * words : 0);
+        if (!keep)
+            build_row_bitmap(bm, words, row, rpa, cia, rpb, cib, lane);
+        int out = rpc[row];
+        for (int w0 = 0; w0 < words; w0 += 32)
+        {
+            const int w = w0 + lane;
+            uint32_t bits = w < words ? bm[w] : 0u;
+            const int c = __popc(bits);
+            int pre = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1)
+            {
+                const int y = __shfl_up_sync(0xffffffffu, pre, o);
+                if (lane >= o)
+                    pre += y;
+            }
+            int pos = out + pre - c;
+            while (bits)
+            {
+                const int b = __ffs(bits) - 1;
+                if (pos < cap)
                     cic[pos] = w * 32 + b;
                 ++pos;
                 bits &= bits - 1;
@@ -582,7 +778,89 @@ int check_bsr_args(int bsr, int mb, int kb, int nb, const void *a, const void *,
     return KAMI_OK;
 }
 
+// The fused one-launch symbolic pass; KAMI_ERR_UNSUPPORTED (nothing
+// launched) when the device has no cooperative launch.
+int symbolic_fused(int mb, int nb, const int *rpa, const int *cia, const int *rpb, const int *cib, int *rpc, int *cic,
+                   int64_t cap, cudaStream_t s)
+{
+    int dev = 0, sms = 0, coop = 0, occ = 0;
+    cudaError_t e;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess)
+        return cuda_fail(e, "cudaGetDevice");
+    if (dev < 0 || dev >= 64)
+        return KAMI_ERR_UNSUPPORTED;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    if (!coop)
+        return KAMI_ERR_UNSUPPORTED;
+    static std::once_flag once[64];
+    static unsigned int *bar_base[64];
+    static cudaError_t bar_err[64];
+    std::call_once(once[dev], [&] {
+        void *ptr = nullptr;
+        bar_err[dev] = cudaGetSymbolAddress(&ptr, g_spg_bar);
+        bar_base[dev] = reinterpret_cast<unsigned int *>(ptr);
+    });
+    if (bar_err[dev] != cudaSuccess)
+        return cuda_fail(bar_err[dev], "cudaGetSymbolAddress(spgemm barrier)");
+    int wpc;
+    size_t smem;
+    int st = bitmap_launch(nb, &wpc, &smem);
+    if (st)
+        return st;
+    const void *fn = (const void *)spgemm_symbolic_fused_kernel;
+    if ((st = prep_bitmap_fn(fn, smem)))
+        return st;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, wpc * 32, smem)) != cudaSuccess)
+        return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor(spgemm fused)");
+    if (occ < 1)
+        return KAMI_ERR_UNSUPPORTED;
+    const int rows_ctas = (mb + wpc - 1) / wpc;
+    int grid = rows_ctas < sms * occ ? rows_ctas : sms * occ;
+    // keep every row's bitmap from the count to the fill when the warps' rows
+    // fit in 96 KB of shared memory at a grid that stays co-resident
+    int keep_rows = 0;
+    const int words = (nb + 31) >> 5;
+    const int rpw = (mb + grid * wpc - 1) / (grid * wpc);
+    const size_t keep_smem = (size_t)wpc * rpw * words * 4;
+    if (cap > 0 && rpw > 0 && keep_smem <= 96 * 1024)
+    {
+        int occ_k = 0;
+        if (keep_smem > smem && (st = prep_bitmap_fn(fn, keep_smem)))
+            return st;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_k, fn, wpc * 32, keep_smem) == cudaSuccess &&
+            grid <= sms * occ_k)
+        {
+            keep_rows = rpw;
+            smem = keep_smem > smem ? keep_smem : smem;
+        }
+    }
+    static std::atomic<unsigned int> next_slot{0};
+    unsigned int *bar = bar_base[dev] + 2 * (next_slot.fetch_add(1) % kFuseSlots);
+    if ((e = cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned int), s)) != cudaSuccess)
+        return cuda_fail(e, "cudaMemsetAsync(spgemm barrier)");
+    // generous: a barrier waits for the slowest CTA's share of the rows
+    uint64_t limit = (uint64_t)2e9 + (uint64_t)mb * 20000ull;
+    void *args[] = {&mb, &nb, &rpa, &cia, &rpb, &cib, &rpc, &cic, &cap, &bar, &limit, &keep_rows};
+    if ((e = cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(wpc * 32), args, smem, s)) != cudaSuccess)
+        return cuda_fail(e, "cudaLaunchCooperativeKernel(spgemm_symbolic_fused_kernel)");
+    return KAMI_OK;
+}
+
 } // namespace
+
+int spgemm_read_error(int *flag)
+{
+    int v = 0, z = 0;
+    cudaError_t e = cudaMemcpyFromSymbol(&v, g_spg_error, sizeof(int));
+    if (e == cudaSuccess)
+        e = cudaMemcpyToSymbol(g_spg_error, &z, sizeof(int));
+    if (e != cudaSuccess)
+        return cuda_fail(e, "reading the spgemm status");
+    *flag = v;
+    return KAMI_OK;
+}
+
 } // namespace kami
 
 using namespace kami;
@@ -664,6 +942,18 @@ int kami_spgemm_bsr_symbolic_device(int bsr, int mb, int kb, int nb, const int *
 {
     if (capacity < 0 || (capacity > 0 && !col_idx_c))
         return fail(KAMI_ERR_INVALID_VALUE, "spgemm symbolic: capacity must be >= 0 with a column array");
+    if (mb > 0 && nb > 0)
+    {
+        const int st0 = check_bsr_args(bsr, mb, kb, nb, row_ptr_a, col_idx_a, row_ptr_b, col_idx_b);
+        if (st0)
+            return st0;
+        if (!row_ptr_c)
+            return fail(KAMI_ERR_INVALID_VALUE, "spgemm: row_ptr_c is NULL");
+        const int st1 = symbolic_fused(mb, nb, row_ptr_a, col_idx_a, row_ptr_b, col_idx_b, row_ptr_c, col_idx_c,
+                                       capacity, reinterpret_cast<cudaStream_t>(stream));
+        if (st1 != KAMI_ERR_UNSUPPORTED)
+            return st1;
+    }
     // count + scan, with no copy of nnzC to the host
     int st = kami_spgemm_bsr_symbolic(bsr, mb, kb, nb, row_ptr_a, col_idx_a, row_ptr_b, col_idx_b, row_ptr_c,
                                       nullptr, stream);

@@ -283,6 +283,15 @@ def spgemm(mA, nB, A, B, accum: str = "double"):
     return rpc, cic[:nnzc].copy(), vals.copy()
 
 
+def spgemm_row_ptr(mA, nB, row_ptr_a, col_idx_a, row_ptr_b, col_idx_b):
+    """RowPtrC of the SPA symbolic pass alone (block_spgemm_2d_half_mma.cu:557-600)."""
+    rpa, cia, rpb, cib = (np.ascontiguousarray(x, dtype=np.int32) for x in (row_ptr_a, col_idx_a, row_ptr_b,
+                                                                            col_idx_b))
+    rpc = np.zeros(mA + 1, dtype=np.int32)
+    lib().kami_oracle_spgemm_symbolic(mA, nB, _p(rpa, _ip), _p(cia, _ip), _p(rpb, _ip), _p(cib, _ip), _p(rpc, _ip))
+    return rpc
+
+
 def spgemm_nnzcub(col_idx_a: np.ndarray, row_ptr_b: np.ndarray) -> int:
     """nnzCub (block_spgemm_2d_half_mma.cu:763-768)."""
     cia = np.ascontiguousarray(col_idx_a, dtype=np.int32)

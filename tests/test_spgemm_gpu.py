@@ -142,6 +142,29 @@ def test_symbolic_device_matches_host_and_numeric_bound(cuda, mb, kb, nb, densit
     assert bool((vals[nnz:] == -7.0).all())
 
 
+@pytest.mark.parametrize("mb,kb,nb,density", [(20000, 64, 3000, 0.01), (1, 5, 7, 1.0), (3000, 3000, 40, 0.002),
+                                              (50000, 16, 100, 0.05)])
+def test_symbolic_device_one_launch_large(cuda, mb, kb, nb, density):
+    """The one-launch symbolic pass (count, scan, column fill as phases of a
+    cooperative kernel) with many block-rows per CTA, a single row, and rows
+    without entries, against the oracle's structure and the separate
+    count / fill kernels."""
+    A = random_bsr(mb, kb, density, 21, integer=True)
+    B = random_bsr(kb, nb, min(1.0, density * 10), 22, integer=True)
+    dA, dB = to_dev(A, kb), to_dev(B, nb)
+    rpc_h, nnz = api.spgemm_symbolic(dA, dB)
+    cic_h = api.spgemm_fill_colidx(dA, dB, rpc_h, nnz)
+    rpc, cic = api.spgemm_symbolic_device(dA, dB, nnz)
+    assert torch.equal(rpc, rpc_h) and torch.equal(cic[:nnz], cic_h)
+    # RowPtrC of the oracle's SPA symbolic pass
+    rpc_o = oracle.spgemm_row_ptr(mb, nb, A[0], A[1], B[0], B[1])
+    assert np.array_equal(rpc.cpu().numpy(), rpc_o)
+    from kami_b200 import _lib
+    import ctypes
+    code = ctypes.c_int(0)
+    assert _lib.load().kami_device_status(ctypes.byref(code)) == 0 and code.value == 0
+
+
 def test_symbolic_device_capacity_respected(cuda):
     A = random_bsr(40, 30, 0.2, 5, integer=True)
     B = random_bsr(30, 50, 0.2, 6, integer=True)
