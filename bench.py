@@ -64,7 +64,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="block",
                     choices=["block", "block-sweep", "fp64", "split", "uneven", "spgemm", "spmm", "bmm",
-                             "comparators"],
+                             "comparators", "ksplit"],
                     help="block (default, the headline line) or one of the other configurations; "
                          "non-default workloads print one JSON line per measured case")
     return ap.parse_args()
@@ -566,6 +566,35 @@ def run_secondary(args):
             _emit({"workload": "spmm", "case": f"n=16384, 1 % tiles, dense {Nd} columns, B {lay}",
                    "nnz_blocks": int(len(ci)), "ms": t, "tflops": fl / t / 1e9, "hbm_gbs": by / t / 1e6,
                    "frac_hbm": by / t / 1e6 / peak_bw, "max_abs_err_first_64_block_rows": err})
+        return
+
+    if args.workload == "ksplit":
+        # the register / shared-memory K split of the 1D mma.sync block GEMM at
+        # 128^3 (the reference's reg_smem program: 1D FP16 128^3 with
+        # REG_K_SPLIT_BLOCK of 8 k-steps in registers), in the reference's
+        # repeat method, and the per-warp communication / computation cycles
+        # of the traced instances (its usage_cycle programs)
+        rng = np.random.default_rng(0)
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        b, n, it = 4 * sms, 128, 1000
+        A = torch.tensor(rng.uniform(-1, 1, (b, n, n)), device=dev).half()
+        B = torch.tensor(rng.uniform(-1, 1, (b, n, n)), device=dev).half()
+        C = torch.empty((b, n, n), dtype=torch.float32, device=dev)
+        fl = 2.0 * n ** 3 * b * it
+        for P, rk in ((4, 0), (4, 2), (4, 4), (8, 0), (8, 4), (8, 8), (0, -1)):
+            used = [None]
+
+            def run():
+                used[0] = api.gemm_batched_ksplit(A, B, C, P=P, reg_k_steps=rk, num_iter=it)[1]
+
+            t = min(_time_ms(run, W, K_, flush))
+            _emit({"workload": "ksplit", "tile": n, "P": P, "reg_k_steps": rk, "reg_k_used": used[0],
+                   "num_iter": it, "ms": t, "tflops": fl / t / 1e9, "frac_tensor_peak": fl / t / 1e9 / peak_tf})
+        for part, P, rk in (("1d", 8, -1), ("1d", 4, 4), ("1d", 4, 0), ("2d", 4, -1), ("3d", 2, -1)):
+            _, cyc = api.gemm_trace(A[0], B[0], partition=part, P=P, reg_k_steps=rk, num_iter=10)
+            _emit({"workload": "ksplit-trace", "tile": n, "partition": part, "P": P, "reg_k_steps": rk,
+                   "num_iter": 10, "comm_cycles_per_iter": [int(x) // 10 for x in cyc[:, 0]],
+                   "comp_cycles_per_iter": [int(x) // 10 for x in cyc[:, 1]]})
         return
 
     if args.workload == "comparators":

@@ -143,6 +143,45 @@ int kami_gemm_workspace_size(kami_dtype_t in_type, kami_partition_t partition,
                              int64_t batch, size_t *bytes);
 
 /*
+ * 1D mma.sync block GEMM with the K dimension split between registers and
+ * shared memory: each rank keeps reg_k_steps k-steps (16 elements each) of
+ * its A and B slices in registers and the rest in a shared-memory cache read
+ * at every stage -- the residency trade-off the reference explores with one
+ * compile-time split (src/reg_smem/block_gemm_1d_half_mma.cu:30-46,
+ * REG_K_SPLIT_BLOCK).  It lets 1D 128^3 run with P = 4, whose all-register
+ * form does not fit the register file.  FP16 / BF16 in, FP32 / FP16 / BF16
+ * out; A M x K row-major, B the reference's N x K row-major; M, N, K up to
+ * 128 (the smallest compiled square tile covering them: 64 or 128).
+ * P = 0 lets the library pick P; reg_k_steps = -1 measures every compiled
+ * split (and all-register form) of the tile on the caller's A and B with a
+ * scratch C, once per request shape, and keeps the fastest -- the split as
+ * an autotuner dimension.  *reg_k_used (if not NULL) receives the split run.
+ */
+int kami_gemm_batched_ksplit(kami_dtype_t in_type, kami_dtype_t out_type,
+                             int M, int N, int K, int P, int64_t batch,
+                             const void *A, int64_t lda, int64_t strideA,
+                             const void *B, int64_t ldb, int64_t strideB,
+                             void *C, int64_t ldc, int64_t strideC,
+                             double alpha, double beta, int num_iter,
+                             int reg_k_steps, int *reg_k_used, void *stream);
+
+/*
+ * Communication / computation cycle trace of one FP16 block GEMM (the
+ * reference's src/usage_cycle/block_gemm_{1d,2d,3d}_half_mma_usage_cycle.cu,
+ * which print clock() sums per warp): C (M x N, FP32) = A (M x K) B^T (B
+ * N x K), one problem, num_iter repeats, on a traced instance of the given
+ * partition and P (reg_k_steps as in kami_gemm_batched_ksplit for 1D; -1
+ * otherwise).  cycles (device, 2 x 32 entries) receives per warp w
+ * cycles[2w] = clock64 cycles spent publishing fragments and waiting at the
+ * stage barriers, cycles[2w+1] = cycles spent reading fragments and issuing
+ * MMAs, summed over every stage and repeat; *nwarps the warp count.
+ * Compiled for 64^3 and 128^3 tiles (1D P = 2, 4, 8; 2D P = 2, 4; 3D P = 2).
+ */
+int kami_gemm_trace(kami_partition_t partition, int M, int N, int K, int P, int reg_k_steps,
+                    const void *A, const void *B, void *C, int num_iter,
+                    unsigned long long *cycles, int *nwarps, void *stream);
+
+/*
  * Describe the kernel kami_gemm_batched would launch (after AUTO resolution):
  * out[0] = variant, out[1] = partition, out[2] = P, out[3] = threads per
  * CTA, out[4] = dynamic shared memory bytes, out[5] = problems per CTA,

@@ -91,6 +91,53 @@ def gemm_batched(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = None
     return C3[0] if squeeze else C3
 
 
+def gemm_batched_ksplit(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = None, *, P: int = 0,
+                        reg_k_steps: int = -1, num_iter: int = 1, alpha: float = 1.0, beta: float = 0.0,
+                        out_dtype: torch.dtype | None = None, stream=None):
+    """1D block GEMM with K split between registers and shared memory
+    (kami_gemm_batched_ksplit).  A: [batch, M, K], B: [batch, N, K] (the
+    reference's layout), FP16 or BF16.  reg_k_steps -1 measures the compiled
+    splits and keeps the fastest.  Returns (C, reg_k_steps used)."""
+    A3, B3 = _as3(A), _as3(B)
+    if A3.dtype != B3.dtype or A3.dtype not in (torch.float16, torch.bfloat16):
+        raise TypeError("A and B must both be float16 or both bfloat16")
+    _check_inner(A3, "A")
+    _check_inner(B3, "B")
+    batch, M, K = A3.shape
+    N = B3.shape[1]
+    if C is None:
+        C3 = torch.empty((batch, M, N), dtype=out_dtype or torch.float32, device=A3.device)
+    else:
+        C3 = _as3(C)
+        _check_inner(C3, "C")
+    used = ctypes.c_int(-2)
+    check(load().kami_gemm_batched_ksplit(_DT[A3.dtype], _DT[C3.dtype], M, N, K, P, batch,
+                                          A3.data_ptr(), _ld(A3), _bs(A3), B3.data_ptr(), _ld(B3), _bs(B3),
+                                          C3.data_ptr(), _ld(C3), _bs(C3), float(alpha), float(beta), int(num_iter),
+                                          int(reg_k_steps), ctypes.byref(used), _stream_ptr(stream)))
+    out = C if C is not None else (C3[0] if A.dim() == 2 else C3)
+    return out, used.value
+
+
+def gemm_trace(A: torch.Tensor, B: torch.Tensor, *, partition: str = "1d", P: int, reg_k_steps: int = -1,
+               num_iter: int = 10, stream=None):
+    """Per-warp communication / computation clock64 cycles of one FP16 block
+    GEMM (kami_gemm_trace).  A: [M, K], B: [N, K] float16 on the device.
+    Returns (C [M, N] float32, cycles [nwarps, 2] int64 numpy array)."""
+    import numpy as np
+    if A.dtype != torch.float16 or B.dtype != torch.float16:
+        raise TypeError("the traced instances take float16 A and B")
+    A, B = A.contiguous(), B.contiguous()
+    M, K = A.shape
+    N = B.shape[0]
+    C = torch.empty((M, N), dtype=torch.float32, device=A.device)
+    cyc = torch.zeros(64, dtype=torch.int64, device=A.device)
+    nw = ctypes.c_int(0)
+    check(load().kami_gemm_trace(_PART[partition], M, N, K, P, reg_k_steps, A.data_ptr(), B.data_ptr(),
+                                 C.data_ptr(), int(num_iter), cyc.data_ptr(), ctypes.byref(nw), _stream_ptr(stream)))
+    return C, cyc.cpu().numpy()[: 2 * nw.value].reshape(nw.value, 2)
+
+
 def describe(M: int, N: int, K: int, batch: int, dtype=torch.float16, out_dtype=None, *, partition="auto",
              variant="auto", P=0, alloc_warps=0, a_layout="row_mk", b_layout="ref_nk") -> dict:
     """The kernel kami_gemm_batched would launch for this request."""

@@ -28,6 +28,7 @@ struct GemmArgs {
     double alpha, beta;
     int num_iter;
     int problems_per_cta;
+    unsigned long long *trace; // traced instances: per-warp {communication, computation} cycles of problem 0
 };
 
 // Host-side description of a resolved launch (kami_gemm_describe).

@@ -34,6 +34,22 @@
 //     k0 + 2t units), which leaves each dot product unchanged and turns the
 //     reference's 32-bit loads into 64-bit (FP16) / 128-bit (FP64) loads.
 //   * P == 1 keeps everything in registers (no shared-memory round trip).
+//
+// Two optional forms, compiled only where an instance asks for them:
+//   * K split (RK >= 0, 1D): only the first RK k-steps of each rank's A and B
+//     slices stay in registers; the remaining k-steps are written once to a
+//     shared-memory cache (A per rank, B readable by every rank) and read
+//     from there at every stage -- the register / shared-memory residency
+//     trade-off of the reference's src/reg_smem/block_gemm_1d_half_mma.cu
+//     (REG_K_SPLIT_BLOCK, :30-46).  It lets 1D 128^3 run with P = 4, whose
+//     all-register form does not fit the register file.  RK = 0 caches
+//     everything and needs no barrier after the first.
+//   * TRACE: clock64 counts per warp of the cycles spent communicating
+//     (publishing fragments and waiting at the stage barrier) and computing
+//     (fragment reads and MMAs), written for problem 0 to GemmArgs::trace --
+//     the measurement of the reference's src/usage_cycle/ kernels
+//     (block_gemm_1d_half_mma_usage_cycle.cu:127-197), kept out of the
+//     untraced instances.
 #pragma once
 
 #include "kami_common.cuh"
@@ -147,7 +163,7 @@ struct TrF64
 // ---------------------------------------------------------------------------
 // Compile-time geometry of one (traits, BM, BN, BK, P, partition) instance.
 // ---------------------------------------------------------------------------
-template <class Tr, int BM, int BN, int BK, int P, int PART>
+template <class Tr, int BM, int BN, int BK, int P, int PART, int RK = -1>
 struct BlockGeom
 {
     static constexpr int NW = PART == 1 ? P : PART == 2 ? P * P : P * P * P;
@@ -163,20 +179,32 @@ struct BlockGeom
     static_assert(TK >= 1 && TK * Tr::KSTEP == SUB_K, "per-rank K slice must be a multiple of the MMA k-step");
     static_assert(NW <= 32, "at most 32 warps per problem");
 
-    static constexpr bool EXCHANGE = P > 1;
+    // K split: k-steps of a rank's slices held in registers (RKE) and in the
+    // shared-memory cache (SKE)
+    static constexpr int RKE = RK < 0 ? TK : RK;
+    static constexpr int SKE = TK - RKE;
+    static_assert(RK < 0 || (PART == 1 && P > 1 && RK <= TK), "the K split is a 1D form with P > 1");
+
+    static constexpr bool EXCHANGE = P > 1 && RKE > 0;
     static constexpr int A_FRAG_U = 4 * 32; // units per published A fragment
     static constexpr int B_FRAG_U = 2 * 32;
     static constexpr int XA_SLOTS = PART == 1 ? 0 : PART == 2 ? P : P * P;
     static constexpr int XB_SLOTS = PART == 1 ? 1 : PART == 2 ? P : P * P;
     static constexpr int XA_SLOT_U = TM * TK * A_FRAG_U;
-    static constexpr int XB_SLOT_U = TN * TK * B_FRAG_U;
+    static constexpr int XB_SLOT_U = TN * RKE * B_FRAG_U;
     static constexpr int XBUF_U = XA_SLOTS * XA_SLOT_U + XB_SLOTS * XB_SLOT_U;
     static constexpr size_t XBYTES = EXCHANGE ? 2ull * XBUF_U * sizeof(typename Tr::Unit) : 0;
     static constexpr int F = TM * TN;
     static constexpr int FO = (F + P - 1) / P;
     static constexpr size_t RBYTES =
         (PART == 3 && P > 1) ? (size_t)P * P * P * (P - 1) * FO * 32 * 4 * sizeof(typename Tr::Acc) : 0;
-    static constexpr size_t SMEM = XBYTES > RBYTES ? XBYTES : RBYTES; // per problem group
+    // K-split caches, per rank: A fragments (read by the rank itself) then B
+    // fragments (read by every rank at the rank's stage)
+    static constexpr int AC_U = TM * SKE * A_FRAG_U;
+    static constexpr int BC_U = TN * SKE * B_FRAG_U;
+    static constexpr size_t XR = XBYTES > RBYTES ? XBYTES : RBYTES;
+    static constexpr size_t CBYTES = (size_t)NW * (AC_U + BC_U) * sizeof(typename Tr::Unit);
+    static constexpr size_t SMEM = XR + CBYTES; // per problem group
 };
 
 template <class Tr>
@@ -223,10 +251,10 @@ __device__ __forceinline__ void load_b_frag(const GemmArgs &g, const typename Tr
     b[1] = hi;
 }
 
-template <class Tr, int BM, int BN, int BK, int P, int PART>
+template <class Tr, int BM, int BN, int BK, int P, int PART, int RK = -1, bool TRACE = false>
 __global__ void block_mma_kernel(const GemmArgs g)
 {
-    using G = BlockGeom<Tr, BM, BN, BK, P, PART>;
+    using G = BlockGeom<Tr, BM, BN, BK, P, PART, RK>;
     using Unit = typename Tr::Unit;
     using Acc = typename Tr::Acc;
     using Elem = typename Tr::Elem;
@@ -280,18 +308,46 @@ __global__ void block_mma_kernel(const GemmArgs g)
     const int b_k0 = PART == 1 ? 0 : PART == 2 ? wr * G::SUB_K : (wr * P + wd) * G::SUB_K;
     const int lane_k = tq * 2 * Tr::EPU; // permuted k offset of this lane inside a k-step
 
-    Unit a[TM][TK][4];
-    Unit b[TN][TK][2];
+    constexpr int RKE = G::RKE, SKE = G::SKE, RKA = RKE > 0 ? RKE : 1;
+    Unit a[TM][RKA][4];
+    Unit b[TN][RKA][2];
 #pragma unroll
     for (int i = 0; i < TM; ++i)
 #pragma unroll
-        for (int k = 0; k < TK; ++k)
+        for (int k = 0; k < RKE; ++k)
             load_a_frag<Tr>(g, A, a_row0 + 16 * i + gq, a_k0 + k * KU + lane_k, a[i][k]);
 #pragma unroll
     for (int j = 0; j < TN; ++j)
 #pragma unroll
-        for (int k = 0; k < TK; ++k)
+        for (int k = 0; k < RKE; ++k)
             load_b_frag<Tr>(g, B, b_n0 + 8 * j + gq, b_k0 + k * KU + lane_k, b[j][k]);
+    // K split: the k-steps past RKE go to this rank's shared-memory cache
+    Unit *cache = reinterpret_cast<Unit *>(smem_raw + (size_t)group * G::SMEM + G::XR);
+    if constexpr (SKE > 0)
+    {
+        Unit *ac = cache + w * (G::AC_U + G::BC_U), *bc = ac + G::AC_U;
+#pragma unroll
+        for (int i = 0; i < TM; ++i)
+#pragma unroll
+            for (int k = 0; k < SKE; ++k)
+            {
+                Unit f[4];
+                load_a_frag<Tr>(g, A, a_row0 + 16 * i + gq, a_k0 + (RKE + k) * KU + lane_k, f);
+                Unit *d = ac + (i * SKE + k) * G::A_FRAG_U;
+                Tr::st2(d + lane * 2, f[0], f[1]);
+                Tr::st2(d + 64 + lane * 2, f[2], f[3]);
+            }
+#pragma unroll
+        for (int j = 0; j < TN; ++j)
+#pragma unroll
+            for (int k = 0; k < SKE; ++k)
+            {
+                Unit f[2];
+                load_b_frag<Tr>(g, B, b_n0 + 8 * j + gq, b_k0 + (RKE + k) * KU + lane_k, f);
+                Tr::st2(bc + (j * SKE + k) * G::B_FRAG_U + lane * 2, f[0], f[1]);
+            }
+    }
+    long long t_comm = 0, t_comp = 0; // TRACE instances only
 
     Acc acc[TM][CN][4];
 #pragma unroll
@@ -302,9 +358,10 @@ __global__ void block_mma_kernel(const GemmArgs g)
             for (int e = 0; e < 4; ++e)
                 acc[i][j][e] = Acc(0);
 
-    if constexpr (!G::EXCHANGE)
+    if constexpr (P == 1)
     {
         // P == 1: one rank holds everything; no exchange.
+        const long long t0 = TRACE ? clock64() : 0;
         for (int it = 0; it < g.num_iter; ++it)
         {
 #pragma unroll
@@ -315,6 +372,8 @@ __global__ void block_mma_kernel(const GemmArgs g)
                     for (int i = 0; i < TM; ++i)
                         Tr::mma(acc[i][j], a[i][k], b[j][k][0], b[j][k][1]);
         }
+        if constexpr (TRACE)
+            t_comp += clock64() - t0;
     }
     else
     {
@@ -326,16 +385,17 @@ __global__ void block_mma_kernel(const GemmArgs g)
                 const int parity = (it * P + s) & 1;
                 Unit *xa = xbuf + parity * G::XBUF_U;
                 Unit *xb = xa + G::XA_SLOTS * G::XA_SLOT_U;
+                const long long t0 = TRACE ? clock64() : 0;
                 // ---- publish ----
                 if constexpr (PART == 1)
                 {
-                    if (wr == s)
+                    if (RKE > 0 && wr == s)
                     {
 #pragma unroll
                         for (int j = 0; j < TN; ++j)
 #pragma unroll
-                            for (int k = 0; k < TK; ++k)
-                                Tr::st2(xb + (j * TK + k) * G::B_FRAG_U + lane * 2, b[j][k][0], b[j][k][1]);
+                            for (int k = 0; k < RKE; ++k)
+                                Tr::st2(xb + (j * RKE + k) * G::B_FRAG_U + lane * 2, b[j][k][0], b[j][k][1]);
                     }
                 }
                 else
@@ -365,21 +425,56 @@ __global__ void block_mma_kernel(const GemmArgs g)
                                 Tr::st2(dst + (j * TK + k) * G::B_FRAG_U + lane * 2, b[j][k][0], b[j][k][1]);
                     }
                 }
-                named_barrier(bar_id, bar_n);
+                // the exchange needs a barrier per stage; an all-cached K split
+                // only one, before the caches are first read
+                if (RKE > 0 || (it == 0 && s == 0))
+                    named_barrier(bar_id, bar_n);
+                long long t1 = 0;
+                if constexpr (TRACE)
+                {
+                    t1 = clock64();
+                    t_comm += t1 - t0;
+                }
                 // ---- compute ----
                 if constexpr (PART == 1)
                 {
 #pragma unroll
                     for (int j = 0; j < TN; ++j)
 #pragma unroll
-                        for (int k = 0; k < TK; ++k)
+                        for (int k = 0; k < RKE; ++k)
                         {
                             Unit b0, b1;
-                            Tr::lds2(xb + (j * TK + k) * G::B_FRAG_U + lane * 2, b0, b1);
+                            Tr::lds2(xb + (j * RKE + k) * G::B_FRAG_U + lane * 2, b0, b1);
 #pragma unroll
                             for (int i = 0; i < TM; ++i)
                                 Tr::mma(acc[i][s * TN + j], a[i][k], b0, b1);
                         }
+                    if constexpr (SKE > 0)
+                    {
+                        const Unit *ac = cache + w * (G::AC_U + G::BC_U);
+                        const Unit *bc = cache + s * (G::AC_U + G::BC_U) + G::AC_U; // rank s's B
+#pragma unroll
+                        for (int k = 0; k < SKE; ++k)
+                        {
+                            Unit af[TM][4];
+#pragma unroll
+                            for (int i = 0; i < TM; ++i)
+                            {
+                                const Unit *f = ac + (i * SKE + k) * G::A_FRAG_U;
+                                Tr::lds2(f + lane * 2, af[i][0], af[i][1]);
+                                Tr::lds2(f + 64 + lane * 2, af[i][2], af[i][3]);
+                            }
+#pragma unroll
+                            for (int j = 0; j < TN; ++j)
+                            {
+                                Unit b0, b1;
+                                Tr::lds2(bc + (j * SKE + k) * G::B_FRAG_U + lane * 2, b0, b1);
+#pragma unroll
+                                for (int i = 0; i < TM; ++i)
+                                    Tr::mma(acc[i][s * TN + j], af[i], b0, b1);
+                            }
+                        }
+                    }
                 }
                 else
                 {
@@ -407,7 +502,17 @@ __global__ void block_mma_kernel(const GemmArgs g)
                         }
                     }
                 }
+                if constexpr (TRACE)
+                    t_comp += clock64() - t1;
             }
+        }
+    }
+    if constexpr (TRACE)
+    {
+        if (lane == 0 && prob == 0 && g.trace)
+        {
+            g.trace[2 * w] = (unsigned long long)t_comm;
+            g.trace[2 * w + 1] = (unsigned long long)t_comp;
         }
     }
 
