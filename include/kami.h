@@ -207,13 +207,16 @@ int kami_gemm_describe(kami_dtype_t in_type, kami_dtype_t out_type,
  * 2D / 3D warp grid) chosen for its shape.
  *
  * kami_gemm_grouped_plan_create builds (host, synchronous) the device
- * descriptors and a longest-first schedule over persistent CTAs.  Two
+ * descriptors and a longest-first schedule over persistent CTAs.  Three
  * kernels run a plan: the mma.sync kernel, whose eight warps split each
- * problem by its warp partition, and (FP16 / BF16 inputs) the tcgen05
- * kernel, which issues each problem's MMAs from one thread into tensor
- * memory while loader and epilogue warps stream the operands and C.  The
- * tcgen05 kernel is the default for FP16 / BF16, the mma.sync kernel for
- * FP64; KAMI_PLAN_MMA_SYNC / KAMI_PLAN_TCGEN05 force one.  With
+ * problem by its warp partition; (FP16 / BF16 inputs) the tcgen05 kernel,
+ * which issues each problem's MMAs from one thread into tensor memory while
+ * loader and epilogue warps stream the operands and C; and (FP64 inputs) the
+ * staged DMMA kernel, whose loader warps stream K chunks into shared memory
+ * while fourteen compute warps share each problem's C.  The tcgen05 kernel
+ * is the default for FP16 / BF16, the staged kernel for FP64 (the warp-grid
+ * kernel when problems of at most 32 x 32 carry most of the bytes);
+ * KAMI_PLAN_MMA_SYNC / KAMI_PLAN_TCGEN05 / KAMI_PLAN_STAGED force one.  With
  * flags & KAMI_PLAN_AUTOTUNE the plan first measures every valid partition
  * per 16-rounded shape bucket on this device (cached per process) instead of
  * using the static cost model, and, unless a kernel is forced, times both
@@ -224,6 +227,7 @@ int kami_gemm_describe(kami_dtype_t in_type, kami_dtype_t out_type,
 #define KAMI_PLAN_AUTOTUNE 1
 #define KAMI_PLAN_MMA_SYNC 2
 #define KAMI_PLAN_TCGEN05 4
+#define KAMI_PLAN_STAGED 8
 typedef struct kami_grouped_plan kami_grouped_plan;
 
 int kami_gemm_grouped_plan_create(kami_dtype_t in_type, kami_dtype_t out_type, int count,
@@ -235,7 +239,8 @@ int kami_gemm_grouped_run(const kami_grouped_plan *plan, const void *A, const vo
 /* out[0] = problems, out[1] = persistent CTAs, out[2] = shared memory bytes,
  * out[3] = FLOPs, out[4] = bytes moved, out[5..12] = problems per partition
  * of the mma.sync kernel (0-2: 1D/2D warp grids, 3-6: 3D warp grids with K
- * depth, 7: one warp per problem), out[13] = kernel (0 mma.sync, 1 tcgen05),
+ * depth, 7: one warp per problem), out[13] = kernel (0 mma.sync, 1 tcgen05,
+ * 2 staged FP64 DMMA),
  * out[14] / out[15] = problems on M = 64 / M = 128 tcgen05 MMAs. */
 int kami_gemm_grouped_plan_info(const kami_grouped_plan *plan, int64_t out[16]);
 int kami_gemm_grouped_plan_destroy(kami_grouped_plan *plan);

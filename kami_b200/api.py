@@ -158,8 +158,9 @@ class GroupedPlan:
     shapes: sequence of (M, N, K).  Problems are packed back to back in the
     A, B and C buffers (A_i M x K, B_i N x K, C_i M x N, row-major) unless
     explicit element offsets are given.  kernel: None (the library's choice:
-    tcgen05 for FP16 / BF16, measured against mma.sync when autotuned),
-    "mma_sync" or "tcgen05" (KAMI_PLAN_MMA_SYNC / KAMI_PLAN_TCGEN05)."""
+    tcgen05 for FP16 / BF16, staged DMMA for FP64, measured against mma.sync
+    when autotuned), "mma_sync", "tcgen05" or "staged" (KAMI_PLAN_MMA_SYNC /
+    KAMI_PLAN_TCGEN05 / KAMI_PLAN_STAGED)."""
 
     def __init__(self, shapes, dtype=torch.float16, out_dtype=None, *, autotune=False, offsets=None, kernel=None):
         import numpy as np
@@ -180,7 +181,7 @@ class GroupedPlan:
         check(load().kami_gemm_grouped_plan_create(_DT[dtype], _DT[self.out_dtype], self.count,
                                                    M.ctypes.data, N.ctypes.data, K.ctypes.data, ao.ctypes.data,
                                                    bo.ctypes.data, co.ctypes.data,
-                                                   (1 if autotune else 0) | {None: 0, "mma_sync": 2, "tcgen05": 4}[kernel],
+                                                   (1 if autotune else 0) | {None: 0, "mma_sync": 2, "tcgen05": 4, "staged": 8}[kernel],
                                                    ctypes.byref(h)))
         self._h = h
 
@@ -189,7 +190,7 @@ class GroupedPlan:
         check(load().kami_gemm_grouped_plan_info(self._h, out))
         v = list(out)
         return {"problems": v[0], "ctas": v[1], "smem": v[2], "flops": v[3], "bytes": v[4],
-                "partitions": v[5:13], "kernel": "tcgen05" if v[13] == 1 else "mma_sync",
+                "partitions": v[5:13], "kernel": {0: "mma_sync", 1: "tcgen05", 2: "staged"}[v[13]],
                 "tcgen05_m64": v[14], "tcgen05_m128": v[15]}
 
     def run(self, A: torch.Tensor, B: torch.Tensor, C: torch.Tensor, *, alpha=1.0, beta=0.0, num_iter=1,

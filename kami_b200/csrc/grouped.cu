@@ -462,7 +462,8 @@ using namespace kami;
 struct kami_grouped_plan
 {
     int in_type, out_type, count, ctas, smem;
-    int kernel = 0; // 0: mma.sync warp grids (grouped_kernel), 1: tcgen05 (grouped_tc05_kernel)
+    int kernel = 0; // 0: mma.sync warp grids (grouped_kernel), 1: tcgen05 (grouped_tc05_kernel),
+                    // 2: staged FP64 DMMA (grouped_f64_kernel)
     int tc_m64 = 0, tc_m128 = 0; // tcgen05 plans: problems on M = 64 / M = 128 MMAs
     int small_begin = 0, small_end = 0; // desc range of single-warp problems
     GroupedDesc *d_desc = nullptr;
@@ -551,6 +552,8 @@ static int launch_grouped(const kami_grouped_plan *plan, const void *A, const vo
     p.small_end = plan->small_end;
     if (plan->kernel == 1)
         return grouped_tc05_launch(p, plan->in_type == KAMI_BF16, plan->ctas, s);
+    if (plan->kernel == 2)
+        return grouped_f64s_launch(p, plan->ctas, s);
     void *args[] = {&p};
     cudaError_t e = cudaLaunchKernel(grouped_fn(plan->in_type), dim3(plan->ctas), dim3(kThreads), args,
                                      (size_t)plan->smem, s);
@@ -573,9 +576,9 @@ static int free_plan(kami_grouped_plan *pl)
 
 // Build descriptors + LPT schedule for `count` problems (host arrays) with
 // the given partitions and upload them.  kernel 1 (FP16 / BF16 only) is the
-// tcgen05 kernel: every problem goes through its CTA pipeline (no
-// single-warp problems) and the cost model is its bytes plus a fixed
-// per-problem latency.
+// tcgen05 kernel, kernel 2 (FP64 only) the staged DMMA kernel: every problem
+// goes through their CTA pipelines (no single-warp problems); the tcgen05
+// kernel's cost model is its bytes plus a fixed per-problem latency.
 static int build_plan(int in_type, int out_type, int count, const int *M, const int *N, const int *K,
                       const int64_t *ao, const int64_t *bo, const int64_t *co, const int *cfg,
                       kami_grouped_plan **out, const int *lda = nullptr, const int *ldb = nullptr,
@@ -587,10 +590,10 @@ static int build_plan(int in_type, int out_type, int count, const int *M, const 
         return cuda_fail(e, "cudaGetDevice");
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
         return cuda_fail(e, "cudaDeviceGetAttribute");
-    const bool tc = kernel == 1;
-    const void *fn = tc ? grouped_tc05_fn(in_type == KAMI_BF16) : grouped_fn(in_type);
-    const int smem = tc ? grouped_tc05_smem() : grouped_smem(in_type);
-    const int threads = tc ? grouped_tc05_threads() : kThreads;
+    const bool tc = kernel == 1, staged = kernel == 2;
+    const void *fn = tc ? grouped_tc05_fn(in_type == KAMI_BF16) : staged ? grouped_f64s_fn() : grouped_fn(in_type);
+    const int smem = tc ? grouped_tc05_smem() : staged ? grouped_f64s_smem() : grouped_smem(in_type);
+    const int threads = tc ? grouped_tc05_threads() : staged ? grouped_f64s_threads() : kThreads;
     if ((e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
         return cuda_fail(e, "cudaFuncSetAttribute(grouped kernel)");
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, smem)) != cudaSuccess)
@@ -622,7 +625,7 @@ static int build_plan(int in_type, int out_type, int count, const int *M, const 
         pl->bytes += (int64_t)by;
         if (tc)
             (M[i] <= 64 ? pl->tc_m64 : pl->tc_m128)++;
-        else
+        else if (!staged)
             pl->cfg_hist[cfg[i]]++;
     }
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
@@ -634,7 +637,7 @@ static int build_plan(int in_type, int out_type, int count, const int *M, const 
     std::vector<int> smalls;
     for (int i : order)
     {
-        if (cfg[i] == 7 && !tc)
+        if (cfg[i] == 7 && kernel == 0)
         {
             smalls.push_back(i); // longest first, spread over all warps round-robin
             continue;
@@ -776,7 +779,7 @@ int grouped_fallback(const GemmArgs &g, int in_type, cudaStream_t stream)
             co[i] = (int64_t)i * g.sC;
         }
         int st = build_plan(in_type, g.out_type, n, vm.data(), vn.data(), vk.data(), ao.data(), bo.data(), co.data(),
-                            vc.data(), &pl, la.data(), lb.data(), lc.data(), in_type == KAMI_F64 ? 0 : 1);
+                            vc.data(), &pl, la.data(), lb.data(), lc.data(), in_type == KAMI_F64 ? 2 : 1);
         if (st)
             return st;
         std::lock_guard<std::mutex> lk(mu);
@@ -804,11 +807,15 @@ int kami_gemm_grouped_plan_create(kami_dtype_t in_type, kami_dtype_t out_type, i
         return fail(KAMI_ERR_UNSUPPORTED, "grouped: output type does not match the input type");
     if (count < 0 || (count > 0 && (!M || !N || !K || !a_offsets || !b_offsets || !c_offsets)))
         return fail(KAMI_ERR_INVALID_VALUE, "grouped: bad count or null shape/offset arrays");
-    const bool force_mma = (flags & KAMI_PLAN_MMA_SYNC) != 0, force_tc = (flags & KAMI_PLAN_TCGEN05) != 0;
-    if (force_mma && force_tc)
-        return fail(KAMI_ERR_INVALID_VALUE, "grouped: KAMI_PLAN_MMA_SYNC and KAMI_PLAN_TCGEN05 are exclusive");
+    const bool force_mma = (flags & KAMI_PLAN_MMA_SYNC) != 0, force_tc = (flags & KAMI_PLAN_TCGEN05) != 0,
+               force_st = (flags & KAMI_PLAN_STAGED) != 0;
+    if ((int)force_mma + (int)force_tc + (int)force_st > 1)
+        return fail(KAMI_ERR_INVALID_VALUE,
+                    "grouped: KAMI_PLAN_MMA_SYNC, KAMI_PLAN_TCGEN05 and KAMI_PLAN_STAGED are exclusive");
     if (force_tc && in_type == KAMI_F64)
         return fail(KAMI_ERR_UNSUPPORTED, "grouped: the tcgen05 kernel takes FP16 / BF16 inputs");
+    if (force_st && in_type != KAMI_F64)
+        return fail(KAMI_ERR_UNSUPPORTED, "grouped: the staged DMMA kernel takes FP64 inputs");
     const int kq = in_type == KAMI_F64 ? 2 : 8;
     for (int i = 0; i < count; ++i)
     {
@@ -896,18 +903,39 @@ int kami_gemm_grouped_plan_create(kami_dtype_t in_type, kami_dtype_t out_type, i
             cfg[i] = cfg_valid(c, M[i], N[i]) ? c : cfg_heuristic(in_type, M[i], N[i], K[i]);
         }
     }
-    if (in_type == KAMI_F64 || force_mma)
+    // the kernel besides the warp-grid one: tcgen05 for 16-bit inputs, the
+    // staged DMMA kernel for FP64
+    const int alt = in_type == KAMI_F64 ? 2 : 1;
+    // FP64 without a measurement: the staged kernel, unless problems of at
+    // most 32 x 32 carry most of the bytes -- its fourteen compute warps pay
+    // a fixed cost per problem that the warp-grid kernel's one-warp path for
+    // such problems does not (20000 problems of 32^3: 0.21 ms staged, 0.15
+    // warp grids; the uneven 8..128 mix: 0.36 against 0.81)
+    bool tiny_mix = false;
+    if (in_type == KAMI_F64 && !force_st && !tune)
+    {
+        double tiny = 0.0, all = 0.0;
+        for (int i = 0; i < count; ++i)
+        {
+            const double by = (double)(M[i] + N[i]) * K[i] + (double)M[i] * N[i];
+            all += by;
+            if (M[i] <= 32 && N[i] <= 32)
+                tiny += by;
+        }
+        tiny_mix = tiny > 0.6 * all;
+    }
+    if (force_mma || tiny_mix)
         return build_plan(in_type, out_type, count, M, N, K, a_offsets, b_offsets, c_offsets, cfg.data(), plan);
-    if (force_tc || !tune || count == 0)
+    if (force_tc || force_st || !tune || count == 0)
         return build_plan(in_type, out_type, count, M, N, K, a_offsets, b_offsets, c_offsets, cfg.data(), plan,
-                          nullptr, nullptr, nullptr, 1);
+                          nullptr, nullptr, nullptr, alt);
     // autotuned, kernel not forced: build both kernels' plans, time each on
     // scratch buffers of the plan's extent, keep the faster
     kami_grouped_plan *pl[2] = {nullptr, nullptr};
     for (int k = 0; k < 2; ++k)
     {
         int st = build_plan(in_type, out_type, count, M, N, K, a_offsets, b_offsets, c_offsets, cfg.data(), &pl[k],
-                            nullptr, nullptr, nullptr, k);
+                            nullptr, nullptr, nullptr, k == 0 ? 0 : alt);
         if (st)
         {
             free_plan(pl[0]);
@@ -921,11 +949,11 @@ int kami_gemm_grouped_plan_create(kami_dtype_t in_type, kami_dtype_t out_type, i
         nb = std::max(nb, b_offsets[i] + (int64_t)N[i] * K[i]);
         nc = std::max(nc, c_offsets[i] + (int64_t)M[i] * N[i]);
     }
-    const int osz = out_type == KAMI_F32 ? 4 : 2;
+    const int isz = in_type == KAMI_F64 ? 8 : 2, osz = out_type == KAMI_F64 ? 8 : out_type == KAMI_F32 ? 4 : 2;
     void *tA = nullptr, *tB = nullptr, *tC = nullptr;
     cudaError_t e;
-    if ((e = cudaMalloc(&tA, (size_t)na * 2)) != cudaSuccess || (e = cudaMalloc(&tB, (size_t)nb * 2)) != cudaSuccess ||
-        (e = cudaMalloc(&tC, (size_t)nc * osz)) != cudaSuccess)
+    if ((e = cudaMalloc(&tA, (size_t)na * isz)) != cudaSuccess ||
+        (e = cudaMalloc(&tB, (size_t)nb * isz)) != cudaSuccess || (e = cudaMalloc(&tC, (size_t)nc * osz)) != cudaSuccess)
     {
         cudaFree(tA);
         cudaFree(tB);
@@ -933,8 +961,8 @@ int kami_gemm_grouped_plan_create(kami_dtype_t in_type, kami_dtype_t out_type, i
         free_plan(pl[1]);
         return cuda_fail(e, "cudaMalloc(grouped kernel choice scratch)");
     }
-    cudaMemset(tA, 0, (size_t)na * 2);
-    cudaMemset(tB, 0, (size_t)nb * 2);
+    cudaMemset(tA, 0, (size_t)na * isz);
+    cudaMemset(tB, 0, (size_t)nb * isz);
     float ms[2] = {0.f, 0.f};
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);

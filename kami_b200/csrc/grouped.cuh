@@ -1,6 +1,7 @@
 // grouped.cuh -- device descriptors of the uneven (grouped) batched GEMM,
-// shared by its two kernels: the mma.sync warp-grid kernel (grouped.cu) and
-// the tcgen05 kernel (grouped_tc05.cu).
+// shared by its three kernels: the mma.sync warp-grid kernel (grouped.cu),
+// the tcgen05 kernel (grouped_tc05.cu, FP16 / BF16) and the staged DMMA
+// kernel (grouped_f64.cu, FP64).
 #pragma once
 #include "kami_common.cuh"
 
@@ -35,5 +36,12 @@ int grouped_tc05_threads();
 int grouped_tc05_smem();
 int grouped_tc05_launch(const GroupedParams &p, bool bf16, int ctas, cudaStream_t s);
 int grouped_tc05_read_error(int *flag);
+
+// staged FP64 grouped kernel (grouped_f64.cu)
+const void *grouped_f64s_fn();
+int grouped_f64s_threads();
+int grouped_f64s_smem();
+int grouped_f64s_launch(const GroupedParams &p, int ctas, cudaStream_t s);
+int grouped_f64s_read_error(int *flag);
 
 } // namespace kami

@@ -1,7 +1,7 @@
 """Uneven grouped GEMM (one persistent launch) against the CPU oracle, with
-the static and the autotuned partition choice, both kernels (mma.sync warp
-grids and tcgen05), FP16/BF16->FP32 and FP64, and inside a captured CUDA
-graph."""
+the static and the autotuned partition choice, all three kernels (mma.sync
+warp grids, tcgen05 for FP16/BF16, staged DMMA for FP64), FP16/BF16->FP32
+and FP64, and inside a captured CUDA graph."""
 import numpy as np
 import pytest
 import torch
@@ -54,21 +54,72 @@ def test_grouped_exact(cuda, dtype, autotune):
     plan = api.GroupedPlan(shapes, dtype, autotune=autotune)
     info = plan.info()
     assert info["problems"] == 600
-    assert sum(info["partitions"]) + info["tcgen05_m64"] + info["tcgen05_m128"] == 600
-    assert info["kernel"] == ("mma_sync" if dtype == torch.float64 else "tcgen05" if not autotune else info["kernel"])
+    default = "staged" if dtype == torch.float64 else "tcgen05"  # the uneven 8..128 mix
+    assert info["kernel"] in ((default,) if not autotune else (default, "mma_sync"))
+    if info["kernel"] == "mma_sync":
+        assert sum(info["partitions"]) == 600
+    elif info["kernel"] == "tcgen05":
+        assert info["tcgen05_m64"] + info["tcgen05_m128"] == 600
     C = torch.empty(plan.sizes[2], dtype=plan.out_dtype, device="cuda")
     plan.run(A, B, C)
     torch.cuda.synchronize()
     check(plan, As, Bs, C)
 
 
-def test_grouped_fp64_uniform(cuda):
+@pytest.mark.parametrize("kernel", ["mma_sync", "staged"])
+def test_grouped_fp64_uniform(cuda, kernel):
     shapes = uneven_shapes(200, 5)
     As, Bs, A, B = make_inputs(shapes, torch.float64, 6, integer=False)
-    plan = api.GroupedPlan(shapes, torch.float64)
+    plan = api.GroupedPlan(shapes, torch.float64, kernel=kernel)
+    assert plan.info()["kernel"] == kernel
     C = torch.empty(plan.sizes[2], dtype=torch.float64, device="cuda")
     plan.run(A, B, C)
     check(plan, As, Bs, C, exact=False)
+
+
+def test_grouped_fp64_default_kernel_by_mix(cuda):
+    """FP64 plans default to the staged kernel, and to the warp-grid kernel
+    when problems of at most 32 x 32 carry most of the bytes."""
+    assert api.GroupedPlan(uneven_shapes(300, 1), torch.float64).info()["kernel"] == "staged"
+    assert api.GroupedPlan(np.full((300, 3), 32), torch.float64).info()["kernel"] == "mma_sync"
+    assert api.GroupedPlan(np.full((300, 3), 32), torch.float64, kernel="staged").info()["kernel"] == "staged"
+
+
+@pytest.mark.parametrize("num_iter", [1, 3])
+def test_grouped_staged_fp64_edges(cuda, num_iter):
+    """The staged DMMA kernel at the edges of its tiling: K of one partial
+    k-step (2, 6), K across chunks with a partial last step (34, 98, 128),
+    M and N not multiples of 16 (odd N too), a whole 128 x 128 C (five
+    sub-tiles on some warps), single rows and columns; alpha / beta."""
+    shapes = np.array([[8, 8, 2], [16, 16, 6], [17, 33, 34], [128, 128, 128], [1, 9, 98], [100, 1, 64],
+                       [128, 120, 40], [64, 64, 32], [3, 127, 126], [48, 80, 96]] * 9)
+    As, Bs, A, B = make_inputs(shapes, torch.float64, 17)
+    plan = api.GroupedPlan(shapes, torch.float64, kernel="staged")
+    C0 = np.random.default_rng(3).integers(-3, 4, plan.sizes[2]).astype(np.float64)
+    C = torch.tensor(C0, device="cuda")
+    plan.run(A, B, C, alpha=2.0, beta=-1.0, num_iter=num_iter)
+    Ch = C.cpu().numpy()
+    co = plan.offsets[2]
+    for i, (m, n, k) in enumerate(plan.shapes):
+        ref = 2.0 * num_iter * oracle.gemm(As[i][None], Bs[i][None])[0] - C0[co[i]:co[i] + m * n].reshape(m, n)
+        assert np.array_equal(Ch[co[i]:co[i] + m * n].reshape(m, n), ref), (i, m, n, k)
+
+
+def test_grouped_staged_fp64_many_problems(cuda):
+    """More problems per CTA than the staged kernel caches in shared memory."""
+    rng = np.random.default_rng(18)
+    count = 50000
+    shapes = np.stack([rng.choice([8, 16, 24], count), rng.choice([8, 16], count), rng.choice([2, 8, 16], count)], 1)
+    As, Bs, A, B = make_inputs(shapes, torch.float64, 19)
+    plan = api.GroupedPlan(shapes, torch.float64, kernel="staged")
+    assert plan.info()["problems"] // plan.info()["ctas"] > 256
+    C = torch.empty(plan.sizes[2], dtype=torch.float64, device="cuda")
+    plan.run(A, B, C)
+    Ch = C.cpu().numpy()
+    co = plan.offsets[2]
+    for i in list(range(0, count, 499)) + [count - 1]:
+        m, n, k = plan.shapes[i]
+        assert np.array_equal(Ch[co[i]:co[i] + m * n].reshape(m, n), oracle.gemm(As[i][None], Bs[i][None])[0]), i
 
 
 def test_grouped_every_partition(cuda):
@@ -223,3 +274,5 @@ def test_grouped_rejects_bad_shapes(cuda):
         api.GroupedPlan([[8, 8, 12]], torch.float16)
     with pytest.raises(Exception):
         api.GroupedPlan([[8, 8, 8]], torch.float64, kernel="tcgen05")
+    with pytest.raises(Exception):
+        api.GroupedPlan([[8, 8, 8]], torch.float16, kernel="staged")
