@@ -676,7 +676,9 @@ def run_secondary(args):
         ms = _time_ms(step, W, K_, flush)
         t = min(ms)
         fl = 3 * 2.0 * n ** 3 * batch
-        by = batch * n * n * 2 * 9
+        # tensor passes of the step: forward reads A, B and writes C; the fused
+        # backward reads A, B, dC and writes dA, dB
+        by = batch * n * n * 2 * 8
         _emit({"workload": "bmm", "dtype": "bf16", "batch": batch, "M": n, "N": n, "K": n, "ms_fwd_bwd": t,
                "tflops": fl / t / 1e9, "hbm_gbs": by / t / 1e6, "frac_hbm": by / t / 1e6 / peak_bw})
         return

@@ -143,6 +143,23 @@ int kami_gemm_workspace_size(kami_dtype_t in_type, kami_partition_t partition,
                              int64_t batch, size_t *bytes);
 
 /*
+ * Backward of the batched GEMM C = A B in the torch.bmm layout (A M x K,
+ * B K x N, C M x N, row-major, problems packed at strides M K, K N, M N):
+ * given dC, dA = dC B^T (M x K) and dB = A^T dC (K x N) in out_type; dA or
+ * dB may be NULL to skip that gradient.  No counterpart in the reference (it
+ * has no backward pass); this is the library's differentiation path.  FP16 /
+ * BF16 with M, N, K in {64, 128} (and 16-byte aligned buffers) run ONE
+ * tcgen05 kernel per problem that reads A, B and dC once and serves both
+ * products from the same shared-memory tiles (dC is the K-major operand of
+ * one product and the MN-major operand of the other); other requests run as
+ * two kami_gemm_batched products.
+ */
+int kami_gemm_backward_batched(kami_dtype_t in_type, kami_dtype_t out_type,
+                               int M, int N, int K, int64_t batch,
+                               const void *A, const void *B, const void *dC,
+                               void *dA, void *dB, void *stream);
+
+/*
  * 1D mma.sync block GEMM with the K dimension split between registers and
  * shared memory: each rank keeps reg_k_steps k-steps (16 elements each) of
  * its A and B slices in registers and the rest in a shared-memory cache read

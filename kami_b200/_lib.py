@@ -40,6 +40,7 @@ SIGNATURES = {
                            _vp, _i64, _i64, _i,
                            _vp, _i64, _i64,
                            _d, _d, _i, _vp, _sz, _vp], _i),
+    "kami_gemm_backward_batched": ([_i, _i, _i, _i, _i, _i64, _vp, _vp, _vp, _vp, _vp, _vp], _i),
     "kami_gemm_batched_ksplit": ([_i, _i, _i, _i, _i, _i, _i64, _vp, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _i64,
                                   _d, _d, _i, _i, ctypes.POINTER(_i), _vp], _i),
     "kami_gemm_trace": ([_i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _i, _vp, ctypes.POINTER(_i), _vp], _i),

@@ -91,6 +91,32 @@ def gemm_batched(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = None
     return C3[0] if squeeze else C3
 
 
+def gemm_backward(A: torch.Tensor, B: torch.Tensor, dC: torch.Tensor, *, need_dA: bool = True,
+                  need_dB: bool = True, out_dtype: torch.dtype | None = None, stream=None):
+    """Gradients of C = A @ B (torch.bmm layout: A [batch, M, K], B [batch,
+    K, N], dC [batch, M, N], contiguous) by kami_gemm_backward_batched: one
+    fused kernel for FP16 / BF16 64 / 128 shapes.  Returns (dA, dB), None for
+    a gradient not asked for; outputs in ``out_dtype`` (default: the input
+    dtype)."""
+    A3, B3, G3 = _as3(A).contiguous(), _as3(B).contiguous(), _as3(dC).contiguous()
+    if not (A3.dtype == B3.dtype == G3.dtype):
+        raise TypeError("A, B and dC must have the same dtype")
+    batch, M, K = A3.shape
+    N = B3.shape[2]
+    if B3.shape[1] != K or G3.shape[1:] != (M, N) or B3.shape[0] != batch or G3.shape[0] != batch:
+        raise ValueError("shapes do not match C = A @ B")
+    odt = out_dtype or A3.dtype
+    dA = torch.empty((batch, M, K), dtype=odt, device=A3.device) if need_dA else None
+    dB = torch.empty((batch, K, N), dtype=odt, device=A3.device) if need_dB else None
+    check(load().kami_gemm_backward_batched(_DT[A3.dtype], _DT[odt], M, N, K, batch, A3.data_ptr(), B3.data_ptr(),
+                                            G3.data_ptr(), dA.data_ptr() if dA is not None else None,
+                                            dB.data_ptr() if dB is not None else None, _stream_ptr(stream)))
+    if A.dim() == 2:
+        dA = dA[0] if dA is not None else None
+        dB = dB[0] if dB is not None else None
+    return dA, dB
+
+
 def gemm_batched_ksplit(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = None, *, P: int = 0,
                         reg_k_steps: int = -1, num_iter: int = 1, alpha: float = 1.0, beta: float = 0.0,
                         out_dtype: torch.dtype | None = None, stream=None):

@@ -8,6 +8,10 @@ the C ABI (no torch matmul on the path).
     dB = A^T @ dC         A read transposed (a_layout="col_mk"), dC as the
                           K x N operand (b_layout="row_kn")
 
+With the library's default kernel choice the backward is one call of
+kami_gemm_backward_batched: for FP16 / BF16 64 / 128 shapes a single fused
+kernel reads A, B and dC once and writes both gradients.
+
 All three products accumulate in FP32 (FP16/BF16 inputs) or FP64 and are
 returned in the input dtype, as torch.bmm does.
 """
@@ -39,6 +43,10 @@ class KamiBmm(torch.autograd.Function):
         A, B = ctx.saved_tensors
         dC = dC.contiguous()
         dA = dB = None
+        if ctx.partition == "auto" and ctx.variant == "auto" and A.dim() == 3:
+            # both gradients in one launch (kami_gemm_backward_batched)
+            dA, dB = api.gemm_backward(A, B, dC, need_dA=ctx.needs_input_grad[0], need_dB=ctx.needs_input_grad[1])
+            return dA, dB, None, None
         if ctx.needs_input_grad[0]:
             dA = api.gemm_batched(dC, B, b_layout="ref_nk", partition=ctx.partition, variant=ctx.variant,
                                   out_dtype=_out_dtype(A.dtype))

@@ -285,6 +285,38 @@ int kami_gemm_workspace_size(kami_dtype_t in_type, kami_partition_t partition, k
     return KAMI_OK;
 }
 
+int kami_gemm_backward_batched(kami_dtype_t in_type, kami_dtype_t out_type, int M, int N, int K, int64_t batch,
+                               const void *A, const void *B, const void *dC, void *dA, void *dB, void *stream)
+{
+    if (in_type != KAMI_F16 && in_type != KAMI_BF16 && in_type != KAMI_F64)
+        return fail(KAMI_ERR_INVALID_VALUE, "backward: in_type must be KAMI_F16, KAMI_BF16 or KAMI_F64");
+    if ((in_type == KAMI_F64) != (out_type == KAMI_F64) ||
+        (in_type != KAMI_F64 && out_type != KAMI_F32 && out_type != KAMI_F16 && out_type != KAMI_BF16))
+        return fail(KAMI_ERR_UNSUPPORTED, "backward: output type does not match the input type");
+    if (M < 1 || N < 1 || K < 1 || batch < 0)
+        return fail(KAMI_ERR_INVALID_VALUE, "backward: M, N, K must be positive and batch >= 0");
+    if (!A || !B || !dC)
+        return fail(KAMI_ERR_INVALID_VALUE, "backward: A, B and dC must be non-null device pointers");
+    if ((!dA && !dB) || batch == 0)
+        return KAMI_OK;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    int st = tc05_backward_launch(in_type, out_type, M, N, K, batch, A, B, dC, dA, dB, s);
+    if (st != KAMI_ERR_UNSUPPORTED)
+        return st;
+    // two products on the forward kernels: dA = dC (M x N) times B read as the
+    // reference's N x K operand (B is K x N row-major); dB = A read transposed
+    // (col_mk) times dC as the K x N operand
+    if (dA && (st = kami_gemm_batched(in_type, out_type, KAMI_PARTITION_AUTO, KAMI_VARIANT_AUTO, M, K, N, 0, 0, batch,
+                                      dC, N, (int64_t)M * N, KAMI_A_ROW_MK, B, N, (int64_t)K * N, KAMI_B_REF_NK, dA, K,
+                                      (int64_t)M * K, 1.0, 0.0, 1, nullptr, 0, stream)))
+        return st;
+    if (dB && (st = kami_gemm_batched(in_type, out_type, KAMI_PARTITION_AUTO, KAMI_VARIANT_AUTO, K, N, M, 0, 0, batch,
+                                      A, K, (int64_t)M * K, KAMI_A_COL_MK, dC, N, (int64_t)M * N, KAMI_B_ROW_KN, dB, N,
+                                      (int64_t)K * N, 1.0, 0.0, 1, nullptr, 0, stream)))
+        return st;
+    return KAMI_OK;
+}
+
 int kami_gemm_describe(kami_dtype_t in_type, kami_dtype_t out_type, kami_partition_t partition,
                        kami_variant_t variant, int M, int N, int K, int P, int alloc_warps, int64_t batch,
                        kami_a_layout_t a_layout, kami_b_layout_t b_layout, int out[8])

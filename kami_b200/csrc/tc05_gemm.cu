@@ -735,6 +735,221 @@ int tc05_launch(const GemmArgs &g, int in_type, int partition, int P, void *, si
     return KAMI_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Fused backward of C = A B (A: M x K, B: K x N, C: M x N, row-major -- the
+// torch.bmm layout) for M, N, K in {64, 128}: one CTA per problem loads dC,
+// A and B once by TMA (64-column boxes, 128-byte swizzle) and runs both
+// gradients from the same shared-memory tiles:
+//   dA = dC B^T   (M x K): dC as the K-major A operand (rows m, K = n) and B
+//                  as the K-major B operand (rows k, K = n);
+//   dB = A^T dC   (K x N): A as the MN-major A operand (K = m rows of 64
+//                  k-elements) and dC as the MN-major B operand (K = m rows
+//                  of 64 n-elements) -- a row-major tile with 64-column boxes
+//                  is both the K-major view of one product and the MN-major
+//                  view of the other.
+// The two accumulators sit side by side in TMEM (columns 0..K-1 and
+// K..K+N-1); the four warps drain dA, then dB.  Waits are bounded as in the
+// forward kernels.
+// ---------------------------------------------------------------------------
+struct Tc05BwdParams
+{
+    int M, N, K;
+    int64_t batch;
+    void *dA, *dB; // either may be null
+    int out_type;
+    uint32_t idesc_a, idesc_b; // dA: M x K (K-major, K-major); dB: K x N (MN-major, MN-major)
+    uint32_t tmem_cols;
+    uint64_t timeout_ns;
+};
+
+template <bool BF16>
+__global__ void __launch_bounds__(128) tc05_bwd_kernel(const __grid_constant__ CUtensorMap tmG,
+                                                       const __grid_constant__ CUtensorMap tmA,
+                                                       const __grid_constant__ CUtensorMap tmB,
+                                                       const Tc05BwdParams p)
+{
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int M = p.M, N = p.N, K = p.K;
+    uint8_t *sG = smem;                          // dC: N / 64 boxes of M rows x 128 B
+    uint8_t *sA = sG + (size_t)M * N * 2;        // A:  K / 64 boxes of M rows
+    uint8_t *sB = sA + (size_t)M * K * 2;        // B:  N / 64 boxes of K rows
+    float *epi = reinterpret_cast<float *>(sB + (size_t)K * N * 2);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(reinterpret_cast<uint8_t *>(epi) + 4 * kEpiTileBytes);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2);
+    int *ok_slot = reinterpret_cast<int *>(tmem_slot + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int prob = blockIdx.x;
+
+    if (threadIdx.x == 0)
+    {
+        tc::mbar_init(&bars[0], 1);
+        tc::mbar_init(&bars[1], 1);
+        tc::fence_mbar_init();
+        *ok_slot = 1;
+        tc::prefetch_tmap(&tmG);
+        tc::prefetch_tmap(&tmA);
+        tc::prefetch_tmap(&tmB);
+        tc::mbar_expect_tx(&bars[0], (uint32_t)((M * N + M * K + K * N) * 2));
+        for (int b = 0; b < N / 64; ++b)
+            tc::tma_load_3d(sG + (size_t)b * M * 128, &tmG, &bars[0], b * 64, 0, prob);
+        for (int b = 0; b < K / 64; ++b)
+            tc::tma_load_3d(sA + (size_t)b * M * 128, &tmA, &bars[0], b * 64, 0, prob);
+        for (int b = 0; b < N / 64; ++b)
+            tc::tma_load_3d(sB + (size_t)b * K * 128, &tmB, &bars[0], b * 64, 0, prob);
+    }
+    if (warp == 0)
+    {
+        tc::tmem_alloc(tmem_slot, p.tmem_cols);
+        tc::tmem_relinquish();
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (threadIdx.x == 0)
+    {
+        if (!tc::mbar_wait_bounded(&bars[0], 0, p.timeout_ns))
+        {
+            tc05_flag(1);
+            *ok_slot = 0;
+            tc::mbar_wait_bounded(&bars[0], 0, p.timeout_ns); // copies still in flight
+            tc::mbar_arrive(&bars[1]);
+        }
+        else
+        {
+            tc::tc_fence_after();
+            const uint32_t g0 = tc::smem_u32(sG), a0 = tc::smem_u32(sA), b0 = tc::smem_u32(sB);
+            if (p.dA)
+            {
+                // dA = dC B^T: K-major operands, k-step of 16 n = +32 B, next
+                // 64-column box after 4 steps
+                for (int ks = 0; ks < N / 16; ++ks)
+                {
+                    const uint32_t ga = g0 + (uint32_t)((ks >> 2) * M * 128 + (ks & 3) * 32);
+                    const uint32_t bb = b0 + (uint32_t)((ks >> 2) * K * 128 + (ks & 3) * 32);
+                    tc::mma_f16_ss(tmem, tc::desc_kmajor_sw128(ga), tc::desc_kmajor_sw128(bb), p.idesc_a,
+                                   ks > 0 ? 1u : 0u);
+                }
+            }
+            if (p.dB)
+            {
+                // dB = A^T dC: MN-major operands, k-step of 16 m-rows = +2 KB,
+                // the next 64-element MN chunk one box (M rows) away
+                for (int ks = 0; ks < M / 16; ++ks)
+                    tc::mma_f16_ss(tmem + (uint32_t)K, tc::desc_mnmajor_sw128(a0 + ks * 2048, (uint32_t)M * 128),
+                                   tc::desc_mnmajor_sw128(g0 + ks * 2048, (uint32_t)M * 128), p.idesc_b,
+                                   ks > 0 ? 1u : 0u);
+            }
+            tc::mma_commit(&bars[1]);
+        }
+    }
+    __syncwarp();
+
+    const bool done = __all_sync(0xffffffffu, tc::mbar_wait_bounded(&bars[1], 0, p.timeout_ns));
+    tc::tc_fence_after();
+    if (!done)
+        tc05_flag(2);
+    const bool ok = done && *reinterpret_cast<volatile int *>(ok_slot);
+    if (ok)
+    {
+        const uint32_t lane_addr = (uint32_t)(warp * 32) << 16;
+        const int osz = p.out_type == KAMI_F32 ? 4 : 2;
+        float *T = epi + warp * (kEpiTileBytes / 4);
+        for (int which = 0; which < 2; ++which)
+        {
+            void *out = which == 0 ? p.dA : p.dB;
+            if (!out)
+                continue;
+            const int rows = which == 0 ? M : K, cols = which == 0 ? K : N;
+            const uint32_t col0 = which == 0 ? 0u : (uint32_t)K;
+            GemmArgs g{};
+            g.M = rows;
+            g.N = cols;
+            g.ldc = cols;
+            g.out_type = p.out_type;
+            g.c_vec = 1;
+            g.c_vec4 = 1;
+            g.alpha = 1.0;
+            g.beta = 0.0;
+            void *Cb = reinterpret_cast<char *>(out) + (int64_t)prob * rows * cols * osz;
+            const int row_base = rows == 128 ? warp * 32 : warp * 16;
+            for (int c0 = 0; c0 < cols; c0 += 16)
+            {
+                uint32_t v[16];
+                tc::tmem_ld16(tmem + lane_addr + col0 + c0, v);
+                tc::tmem_ld_wait();
+                float f[16];
+#pragma unroll
+                for (int e = 0; e < 16; ++e)
+                    f[e] = __uint_as_float(v[e]);
+                store_chunk(g, Cb, f, row_base, rows == 128 ? 32 : 16, c0, T);
+            }
+        }
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == 0)
+    {
+        __syncwarp();
+        tc::tc_fence_after();
+        tc::tmem_dealloc(tmem, p.tmem_cols);
+    }
+}
+
+// Launch the fused backward; KAMI_ERR_UNSUPPORTED (nothing launched) outside
+// FP16 / BF16 with M, N, K in {64, 128}, packed problems and 16-byte aligned
+// buffers.
+int tc05_backward_launch(int in_type, int out_type, int M, int N, int K, int64_t batch, const void *A, const void *B,
+                         const void *dC, void *dA, void *dB, cudaStream_t stream)
+{
+    auto dim_ok = [](int x) { return x == 64 || x == 128; };
+    if ((in_type != KAMI_F16 && in_type != KAMI_BF16) || !dim_ok(M) || !dim_ok(N) || !dim_ok(K) ||
+        (out_type != KAMI_F32 && out_type != KAMI_F16 && out_type != KAMI_BF16) || batch < 1 || batch > 0x7fffffff)
+        return KAMI_ERR_UNSUPPORTED;
+    auto al = [](const void *q) { return q == nullptr || (reinterpret_cast<uintptr_t>(q) & 15) == 0; };
+    if (!al(A) || !al(B) || !al(dC) || !al(dA) || !al(dB))
+        return KAMI_ERR_UNSUPPORTED;
+    const bool bf16 = in_type == KAMI_BF16;
+    CUtensorMap mg, ma, mb;
+    int st;
+    // row-major tiles as {columns, rows, batch} maps with 64-column boxes of all rows
+    if ((st = make_map(&mg, bf16, dC, N, M, batch, N, (int64_t)M * N, M)) ||
+        (st = make_map(&ma, bf16, A, K, M, batch, K, (int64_t)M * K, M)) ||
+        (st = make_map(&mb, bf16, B, N, K, batch, N, (int64_t)K * N, K)))
+        return st;
+    Tc05BwdParams p{};
+    p.M = M;
+    p.N = N;
+    p.K = K;
+    p.batch = batch;
+    p.dA = dA;
+    p.dB = dB;
+    p.out_type = out_type;
+    p.idesc_a = tc::idesc_f16(bf16, M, K, 0, 0);
+    p.idesc_b = tc::idesc_f16(bf16, K, N, 1, 1);
+    uint32_t cols = 32;
+    while ((int)cols < K + N)
+        cols <<= 1;
+    p.tmem_cols = cols;
+    p.timeout_ns = (uint64_t)(5e8 + (double)(M + N) * 4000.0);
+    const size_t smem = (size_t)(M * N + M * K + K * N) * 2 + 4 * kEpiTileBytes + 64 + 1024;
+    const void *fn = bf16 ? (const void *)&tc05_bwd_kernel<true> : (const void *)&tc05_bwd_kernel<false>;
+    static std::once_flag once[2];
+    cudaError_t e = cudaSuccess;
+    std::call_once(once[bf16 ? 1 : 0], [&] {
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    });
+    if (e != cudaSuccess)
+        return cuda_fail(e, "cudaFuncSetAttribute(tc05_bwd_kernel)");
+    void *args[] = {&mg, &ma, &mb, &p};
+    e = cudaLaunchKernel(fn, dim3((unsigned)batch), dim3(128), args, smem, stream);
+    if (e != cudaSuccess)
+        return cuda_fail(e, "cudaLaunchKernel(tc05_bwd_kernel)");
+    return KAMI_OK;
+}
+
 // Failure-detection self test: one thread waits on an mbarrier that nothing
 // arrives at, with the same bounded wait the GEMM kernels use, and records
 // code 4 in the status word when the wait gives up.

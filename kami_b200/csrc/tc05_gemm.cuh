@@ -32,4 +32,10 @@ int tc05_read_error(int *flag);
 // Launch a one-thread kernel whose bounded wait must time out (status 4).
 int tc05_selftest_bounded_wait(uint64_t limit_ns, cudaStream_t s);
 
+// Fused backward (dA = dC B^T, dB = A^T dC) of packed row-major problems;
+// KAMI_ERR_UNSUPPORTED (nothing launched) outside FP16 / BF16 with M, N, K in
+// {64, 128}.
+int tc05_backward_launch(int in_type, int out_type, int M, int N, int K, int64_t batch, const void *A, const void *B,
+                         const void *dC, void *dA, void *dB, cudaStream_t stream);
+
 } // namespace kami
