@@ -281,13 +281,16 @@ __global__ void __launch_bounds__(128) tc05_block_kernel(const __grid_constant__
 // problems overlap:
 //   warp 0 (one lane)  TMA producer: a ring of `stages` shared-memory slots,
 //                      each holding one problem's A and B;
-//   warp 1 (one lane)  MMA issuer: one TMEM accumulator of two (double
-//                      buffered), commits free the slot and publish the
-//                      accumulator;
-//   warps 2..9         epilogue, two groups of four: group g drains the
-//                      accumulator of every problem j with j % 2 == g
-//                      (tcgen05.ld of its TMEM lane quadrant, coalesced C
-//                      stores), then releases it -- two problems drain at once.
+//   warp 1 (one lane)  MMA issuer: a ring of `naccs` TMEM accumulators (as
+//                      many as 512 columns hold, at most 8), commits free the
+//                      slot and publish the accumulator;
+//   warps 2..          epilogue, `groups` groups of four (two, or four when
+//                      shared memory leaves room for their transpose tiles):
+//                      group g drains the accumulator of every problem j with
+//                      j % groups == g (tcgen05.ld of its TMEM lane quadrant,
+//                      coalesced C stores), then releases it -- the epilogue
+//                      is the longest phase of a small problem, so several
+//                      drain at once.
 // Every wait is bounded like the per-problem kernel's.
 // ---------------------------------------------------------------------------
 struct Tc05StreamParams
@@ -295,10 +298,14 @@ struct Tc05StreamParams
     Tc05Params t;
     int stages;
     int stage_bytes; // A + B of one problem (1024-byte multiple)
+    int groups;      // epilogue groups of four warps (2 or 4)
+    int naccs;       // TMEM accumulators (2..8)
 };
 
+constexpr int kStreamMaxGroups = 4;
+
 template <bool BF16>
-__global__ void __launch_bounds__(320, 1) tc05_stream_kernel(const __grid_constant__ CUtensorMap tmA,
+__global__ void __launch_bounds__(64 + 128 * kStreamMaxGroups, 1) tc05_stream_kernel(const __grid_constant__ CUtensorMap tmA,
                                                              const __grid_constant__ CUtensorMap tmB,
                                                              const Tc05StreamParams sp)
 {
@@ -308,12 +315,13 @@ __global__ void __launch_bounds__(320, 1) tc05_stream_kernel(const __grid_consta
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int S = sp.stages;
     const int a_box = p.bm * 128, b_box = p.bn * 128;
-    float *epi = reinterpret_cast<float *>(smem + (size_t)S * sp.stage_bytes); // 8 x kEpiTileBytes
-    uint64_t *full = reinterpret_cast<uint64_t *>(smem + (size_t)S * sp.stage_bytes + 8 * kEpiTileBytes);
+    const int G = sp.groups, NA = sp.naccs;
+    float *epi = reinterpret_cast<float *>(smem + (size_t)S * sp.stage_bytes); // 4 G x kEpiTileBytes
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + (size_t)S * sp.stage_bytes + 4 * G * kEpiTileBytes);
     uint64_t *empty = full + S;
-    uint64_t *tfull = empty + S;  // [2]
-    uint64_t *tempty = tfull + 2; // [2]
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tempty + 2);
+    uint64_t *tfull = empty + S;   // [NA]
+    uint64_t *tempty = tfull + NA; // [NA]
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tempty + NA);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t nprob = g.batch;
@@ -324,7 +332,7 @@ __global__ void __launch_bounds__(320, 1) tc05_stream_kernel(const __grid_consta
             tc::mbar_init(&full[i], 1);
             tc::mbar_init(&empty[i], 1);
         }
-        for (int i = 0; i < 2; ++i)
+        for (int i = 0; i < NA; ++i)
         {
             tc::mbar_init(&tfull[i], 1);
             tc::mbar_init(&tempty[i], 4);
@@ -386,13 +394,13 @@ __global__ void __launch_bounds__(320, 1) tc05_stream_kernel(const __grid_consta
             int j = 0;
             for (int64_t prob = blockIdx.x; prob < nprob; prob += gridDim.x, ++j)
             {
-                const int st = j % S, b = j & 1;
+                const int st = j % S, b = j % NA;
                 if (!tc::mbar_wait_bounded(&full[st], (j / S) & 1, limit))
                 {
                     tc05_flag(6);
                     break;
                 }
-                if (j >= 2 && !tc::mbar_wait_bounded(&tempty[b], ((j >> 1) - 1) & 1, limit))
+                if (j >= NA && !tc::mbar_wait_bounded(&tempty[b], ((j / NA) - 1) & 1, limit))
                 {
                     tc05_flag(7);
                     break;
@@ -421,7 +429,8 @@ __global__ void __launch_bounds__(320, 1) tc05_stream_kernel(const __grid_consta
     }
     else
     {
-        // epilogue group g = warps 2+4g .. 5+4g, covering TMEM lane quadrants 2, 3, 0, 1
+        // epilogue group g = warps 2+4g .. 5+4g, covering TMEM lane quadrants
+        // 2, 3, 0, 1
         const int quad = warp & 3;
         const int grp = (warp - 2) >> 2;
         const int row_base = p.bm == 128 ? quad * 32 : quad * 16;
@@ -429,10 +438,11 @@ __global__ void __launch_bounds__(320, 1) tc05_stream_kernel(const __grid_consta
         const int osz = g.out_type == KAMI_F32 ? 4 : 2;
         float *T = epi + (warp - 2) * (kEpiTileBytes / 4);
         int j = grp;
-        for (int64_t prob = blockIdx.x + (int64_t)grp * gridDim.x; prob < nprob; prob += 2 * (int64_t)gridDim.x, j += 2)
+        for (int64_t prob = blockIdx.x + (int64_t)grp * gridDim.x; prob < nprob;
+             prob += (int64_t)G * gridDim.x, j += G)
         {
-            const int b = j & 1;
-            const bool ok = __all_sync(0xffffffffu, tc::mbar_wait_bounded(&tfull[b], (j >> 1) & 1, limit));
+            const int b = j % NA;
+            const bool ok = __all_sync(0xffffffffu, tc::mbar_wait_bounded(&tfull[b], (j / NA) & 1, limit));
             if (!ok)
             {
                 tc05_flag(8);
@@ -639,23 +649,32 @@ int tc05_plan(int in_type, int out_type, int partition, int P, int M, int N, int
 }
 
 // Launch the persistent streaming form: one CTA per SM, as many ring slots
-// as shared memory holds (2..6), two TMEM accumulators.
+// as shared memory holds (2..6), four epilogue groups when at least three
+// slots still fit beside their tiles (else two), and as many TMEM
+// accumulators as 512 columns hold (at most 8).
 static int stream_launch(CUtensorMap &ma, CUtensorMap &mb, Tc05Params &p, bool bf16, cudaStream_t stream)
 {
     Tc05StreamParams sp{};
     sp.t = p;
     sp.stage_bytes = p.nkb * (p.bm + p.bn) * 128;
-    const int budget = 227 * 1024 - 1024 - 256 - 8 * kEpiTileBytes;
+    sp.groups = kStreamMaxGroups;
+    int budget = 227 * 1024 - 1024 - 512 - 4 * sp.groups * kEpiTileBytes;
+    if (budget / sp.stage_bytes < 3)
+    {
+        sp.groups = 2;
+        budget = 227 * 1024 - 1024 - 512 - 4 * sp.groups * kEpiTileBytes;
+    }
     sp.stages = std::min(6, budget / sp.stage_bytes);
     if (sp.stages < 2)
         return fail(KAMI_ERR_UNSUPPORTED, "tcgen05 streaming form: a problem needs %d bytes of shared memory",
                     sp.stage_bytes);
+    sp.naccs = std::min(8, 512 / p.bn);
     uint32_t cols = 32;
-    while ((int)cols < 2 * p.bn)
+    while ((int)cols < sp.naccs * p.bn)
         cols <<= 1;
     sp.t.tmem_cols = cols;
     sp.t.timeout_ns = p.timeout_ns + 500000000ull;
-    const size_t smem = (size_t)sp.stages * sp.stage_bytes + 8 * kEpiTileBytes + 1024 + 256;
+    const size_t smem = (size_t)sp.stages * sp.stage_bytes + 4 * sp.groups * kEpiTileBytes + 1024 + 512;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -668,7 +687,7 @@ static int stream_launch(CUtensorMap &ma, CUtensorMap &mb, Tc05Params &p, bool b
         return cuda_fail(e, "cudaFuncSetAttribute(tc05_stream_kernel)");
     const int64_t grid = std::min<int64_t>(p.g.batch, sms);
     void *args[] = {&ma, &mb, &sp};
-    e = cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(320), args, smem, stream);
+    e = cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(64 + 128 * sp.groups), args, smem, stream);
     if (e != cudaSuccess)
         return cuda_fail(e, "cudaLaunchKernel(tc05_stream_kernel)");
     return KAMI_OK;
@@ -714,10 +733,11 @@ int tc05_launch(const GemmArgs &g, int in_type, int partition, int P, void *, si
 
     // Streamed regime: the persistent form for problems of >= 32 KB of operands
     // (measured on B200: 128^3 x 592 121 vs 105 TFLOP/s, x 8192 190 vs 150);
-    // smaller problems drain faster as one CTA each (64^3 x 8192: 84 vs 75).
+    // smaller problems drain as fast as one CTA each (64^3 x 8192: 84 vs 75
+    // with two epilogue groups; BF16 64^3 x 4096: 30.8 vs 31.7 us with four).
     const int stage_bytes = s.nkb * (s.bm + s.bn) * 128;
     if (s.part == KAMI_PARTITION_1D && !s.a_tmem && g.num_iter <= 4 && stage_bytes >= 32768 &&
-        2 * stage_bytes <= 227 * 1024 - 1024 - 256 - 8 * kEpiTileBytes)
+        2 * stage_bytes <= 227 * 1024 - 1024 - 512 - 8 * kEpiTileBytes)
         return stream_launch(ma, mb, p, bf16, stream);
 
     const void *fn = bf16 ? (const void *)&tc05_block_kernel<true> : (const void *)&tc05_block_kernel<false>;
@@ -778,7 +798,7 @@ __global__ void __launch_bounds__(128) tc05_bwd_kernel(const __grid_constant__ C
     uint64_t *bars = reinterpret_cast<uint64_t *>(reinterpret_cast<uint8_t *>(epi) + 4 * kEpiTileBytes);
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2);
     int *ok_slot = reinterpret_cast<int *>(tmem_slot + 1);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
     const int prob = blockIdx.x;
 
     if (threadIdx.x == 0)
