@@ -17,6 +17,7 @@ int f64s_read_error(int *flag);
 int grouped_tc05_read_error(int *flag);
 int spgemm_read_error(int *flag);
 int grouped_f64s_read_error(int *flag);
+int spmm_tc05_read_error(int *flag);
 int split_read_error(int *flag);
 int grouped_fallback(const GemmArgs &g, int in_type, cudaStream_t stream);
 
@@ -250,7 +251,7 @@ int kami_device_status(int *code)
     int st = tc05_read_error(code);
     if (st)
         return st;
-    int c2 = 0, c3 = 0, c4 = 0, c5 = 0, c6 = 0;
+    int c2 = 0, c3 = 0, c4 = 0, c5 = 0, c6 = 0, c7 = 0;
     if ((st = split_read_error(&c2)))
         return st;
     if ((st = f64s_read_error(&c3)))
@@ -260,6 +261,8 @@ int kami_device_status(int *code)
     if ((st = spgemm_read_error(&c5)))
         return st;
     if ((st = grouped_f64s_read_error(&c6)))
+        return st;
+    if ((st = spmm_tc05_read_error(&c7)))
         return st;
     if (!*code)
         *code = c2;
@@ -271,6 +274,8 @@ int kami_device_status(int *code)
         *code = c5;
     if (!*code)
         *code = c6;
+    if (!*code)
+        *code = c7;
     if (*code)
         return fail(KAMI_ERR_TIMEOUT, "a bounded device wait gave up (code %d)", *code);
     return KAMI_OK;

@@ -158,3 +158,57 @@ def test_shared_operands_batched_output(cuda):
     ref = 3 * oracle.spmm(rp, ci, vals.astype(np.float64), 4, B, "ref_nk")
     got = C.double().cpu().numpy()
     assert all(np.array_equal(got[b], ref) for b in (0, 1, 350, 699))
+
+
+def _int_bsr(mb, kb, density, seed):
+    rng = np.random.default_rng(seed)
+    rp, ci = oracle.bsr_pattern(mb, kb, density, seed)
+    vals = rng.integers(-2, 3, (ci.size, 16, 16)).astype(np.float64)
+    return rp, ci, vals
+
+
+@pytest.mark.parametrize("N", [1, 16, 100, 128, 129, 256, 300, 512, 600])
+@pytest.mark.parametrize("dtype", [torch.float16, torch.bfloat16])
+def test_tcgen05_form_exact(cuda, N, dtype):
+    """One problem with K beyond the staged panel and B as K x N: the tcgen05
+    kernel (C^T = B^T A^T per block-row) for N up to 512 (600 takes the
+    mma.sync streamed form), rows without entries included."""
+    mb, kb = 40, 24
+    rp, ci, vals = _int_bsr(mb, kb, 0.15, N)
+    B = np.random.default_rng(N + 1).integers(-2, 3, (kb * 16, N)).astype(np.float64)
+    A = api.BSR(torch.tensor(rp, device="cuda"), torch.tensor(ci, device="cuda"),
+                torch.tensor(vals, dtype=dtype, device="cuda"), kb)
+    C = api.spmm(A, torch.tensor(B, dtype=dtype, device="cuda"), b_layout="row_kn")
+    assert np.array_equal(C.double().cpu().numpy(), oracle.spmm(rp, ci, vals, kb, B, "row_kn"))
+
+
+@pytest.mark.parametrize("out_dtype", [torch.float32, torch.float16, torch.bfloat16])
+def test_tcgen05_form_alpha_beta_repeats(cuda, out_dtype):
+    mb, kb, N = 30, 20, 200
+    rp, ci, vals = _int_bsr(mb, kb, 0.2, 5)
+    B = np.random.default_rng(6).integers(-1, 2, (kb * 16, N)).astype(np.float64)
+    C0 = np.random.default_rng(7).integers(-3, 4, (mb * 16, N)).astype(np.float64)
+    A = api.BSR(torch.tensor(rp, device="cuda"), torch.tensor(ci, device="cuda"),
+                torch.tensor(vals, dtype=torch.float16, device="cuda"), kb)
+    dC = torch.tensor(C0, dtype=out_dtype, device="cuda")
+    api.spmm(A, torch.tensor(B, dtype=torch.float16, device="cuda"), dC, b_layout="row_kn", alpha=2.0, beta=-1.0,
+             num_iter=3)
+    ref = 2.0 * 3 * oracle.spmm(rp, ci, vals, kb, B, "row_kn") - C0
+    ref = torch.tensor(ref, dtype=torch.float32).to(out_dtype).double().numpy()
+    assert np.array_equal(dC.double().cpu().numpy(), ref)
+
+
+def test_tcgen05_form_out_of_range_columns(cuda):
+    """A block column outside [0, kb) contributes nothing (the tensor copy of
+    B rows past its end fills zeros)."""
+    mb, kb, N = 4, 20, 64
+    rp = np.array([0, 2, 2, 4, 5], dtype=np.int32)
+    ci = np.array([3, 25, 0, 19, -4], dtype=np.int32)
+    vals = np.ones((5, 16, 16))
+    B = np.random.default_rng(9).integers(-2, 3, (kb * 16, N)).astype(np.float64)
+    A = api.BSR(torch.tensor(rp, device="cuda"), torch.tensor(ci, device="cuda"),
+                torch.tensor(vals, dtype=torch.float16, device="cuda"), kb)
+    C = api.spmm(A, torch.tensor(B, dtype=torch.float16, device="cuda"), b_layout="row_kn").cpu().numpy()
+    keep = np.array([True, False, True, True, False])
+    ref = oracle.spmm(rp, np.where(keep, ci, 0).astype(np.int32), vals * keep[:, None, None], kb, B, "row_kn")
+    assert np.array_equal(C, ref)
