@@ -169,17 +169,20 @@ def _int_bsr(mb, kb, density, seed):
 
 @pytest.mark.parametrize("N", [1, 16, 100, 128, 129, 256, 300, 512, 600])
 @pytest.mark.parametrize("dtype", [torch.float16, torch.bfloat16])
-def test_tcgen05_form_exact(cuda, N, dtype):
-    """One problem with K beyond the staged panel and B as K x N: the tcgen05
-    kernel (C^T = B^T A^T per block-row) for N up to 512 (600 takes the
-    mma.sync streamed form), rows without entries included."""
+@pytest.mark.parametrize("b_layout", ["row_kn", "ref_nk"])
+def test_tcgen05_form_exact(cuda, N, dtype, b_layout):
+    """One problem with K beyond the staged panel: the tcgen05 kernel for B
+    K x N (C^T = B^T A^T per block-row) with N up to 512, the mma.sync
+    streamed form for N = 600 and for the reference's N x K; rows without
+    entries included."""
     mb, kb = 40, 24
     rp, ci, vals = _int_bsr(mb, kb, 0.15, N)
-    B = np.random.default_rng(N + 1).integers(-2, 3, (kb * 16, N)).astype(np.float64)
+    Bk = np.random.default_rng(N + 1).integers(-2, 3, (kb * 16, N)).astype(np.float64)
+    B = Bk if b_layout == "row_kn" else np.ascontiguousarray(Bk.T)
     A = api.BSR(torch.tensor(rp, device="cuda"), torch.tensor(ci, device="cuda"),
                 torch.tensor(vals, dtype=dtype, device="cuda"), kb)
-    C = api.spmm(A, torch.tensor(B, dtype=dtype, device="cuda"), b_layout="row_kn")
-    assert np.array_equal(C.double().cpu().numpy(), oracle.spmm(rp, ci, vals, kb, B, "row_kn"))
+    C = api.spmm(A, torch.tensor(B, dtype=dtype, device="cuda"), b_layout=b_layout)
+    assert np.array_equal(C.double().cpu().numpy(), oracle.spmm(rp, ci, vals, kb, B, b_layout))
 
 
 @pytest.mark.parametrize("out_dtype", [torch.float32, torch.float16, torch.bfloat16])
@@ -198,17 +201,19 @@ def test_tcgen05_form_alpha_beta_repeats(cuda, out_dtype):
     assert np.array_equal(dC.double().cpu().numpy(), ref)
 
 
-def test_tcgen05_form_out_of_range_columns(cuda):
-    """A block column outside [0, kb) contributes nothing (the tensor copy of
-    B rows past its end fills zeros)."""
+@pytest.mark.parametrize("b_layout", ["row_kn", "ref_nk"])
+def test_tcgen05_form_out_of_range_columns(cuda, b_layout):
+    """A block column outside [0, kb) contributes nothing (zero-filled B
+    slice in the tcgen05 kernel, skipped by the mma.sync kernels)."""
     mb, kb, N = 4, 20, 64
     rp = np.array([0, 2, 2, 4, 5], dtype=np.int32)
     ci = np.array([3, 25, 0, 19, -4], dtype=np.int32)
     vals = np.ones((5, 16, 16))
-    B = np.random.default_rng(9).integers(-2, 3, (kb * 16, N)).astype(np.float64)
+    Bk = np.random.default_rng(9).integers(-2, 3, (kb * 16, N)).astype(np.float64)
+    B = Bk if b_layout == "row_kn" else np.ascontiguousarray(Bk.T)
     A = api.BSR(torch.tensor(rp, device="cuda"), torch.tensor(ci, device="cuda"),
                 torch.tensor(vals, dtype=torch.float16, device="cuda"), kb)
-    C = api.spmm(A, torch.tensor(B, dtype=torch.float16, device="cuda"), b_layout="row_kn").cpu().numpy()
+    C = api.spmm(A, torch.tensor(B, dtype=torch.float16, device="cuda"), b_layout=b_layout).cpu().numpy()
     keep = np.array([True, False, True, True, False])
-    ref = oracle.spmm(rp, np.where(keep, ci, 0).astype(np.int32), vals * keep[:, None, None], kb, B, "row_kn")
+    ref = oracle.spmm(rp, np.where(keep, ci, 0).astype(np.int32), vals * keep[:, None, None], kb, B, b_layout)
     assert np.array_equal(C, ref)
