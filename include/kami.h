@@ -137,6 +137,28 @@ int kami_gemm_batched(kami_dtype_t in_type, kami_dtype_t out_type,
                       double alpha, double beta, int num_iter,
                       void *workspace, size_t ws_bytes, void *stream);
 
+/*
+ * kami_gemm_batched on HOST buffers (C = num_iter * A B^T per problem, A
+ * packed M x K row-major, B the reference's N x K row-major, C M x N; alpha 1,
+ * beta 0): the reference's host sequence -- copy in, launch, copy out
+ * (e.g. batched_gemm_2d_double_mma.cu) -- as one call, with the batch cut
+ * into chunks of whole SM waves so that the input copies of chunk c + 1 and
+ * the result copy of chunk c - 1 overlap the product of chunk c (two extra
+ * streams, double-buffered device workspace).  Host buffers should be pinned
+ * (pageable memory works, without overlap) and stay valid until the work on
+ * `stream` completes; `stream` waits for the last result copy.  workspace:
+ * device memory of kami_gemm_batched_host_workspace_size bytes, or NULL for a
+ * library-owned buffer (allocated on first use, grown as needed).  Calls are
+ * serialised by a process-wide lock.
+ */
+int kami_gemm_batched_host(kami_dtype_t in_type, kami_dtype_t out_type,
+                           kami_partition_t partition, kami_variant_t variant,
+                           int M, int N, int K, int64_t batch,
+                           const void *A, const void *B, void *C, int num_iter,
+                           void *workspace, size_t ws_bytes, void *stream);
+int kami_gemm_batched_host_workspace_size(kami_dtype_t in_type, kami_dtype_t out_type,
+                                          int M, int N, int K, int64_t batch, size_t *bytes);
+
 /* Bytes of device workspace kami_gemm_batched needs for this request. */
 int kami_gemm_workspace_size(kami_dtype_t in_type, kami_partition_t partition,
                              kami_variant_t variant, int M, int N, int K, int P,

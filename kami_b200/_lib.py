@@ -40,6 +40,8 @@ SIGNATURES = {
                            _vp, _i64, _i64, _i,
                            _vp, _i64, _i64,
                            _d, _d, _i, _vp, _sz, _vp], _i),
+    "kami_gemm_batched_host": ([_i, _i, _i, _i, _i, _i, _i, _i64, _vp, _vp, _vp, _i, _vp, _sz, _vp], _i),
+    "kami_gemm_batched_host_workspace_size": ([_i, _i, _i, _i, _i, _i64, ctypes.POINTER(_sz)], _i),
     "kami_gemm_backward_batched": ([_i, _i, _i, _i, _i, _i64, _vp, _vp, _vp, _vp, _vp, _vp], _i),
     "kami_gemm_batched_ksplit": ([_i, _i, _i, _i, _i, _i, _i64, _vp, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _i64,
                                   _d, _d, _i, _i, ctypes.POINTER(_i), _vp], _i),

@@ -91,6 +91,24 @@ def gemm_batched(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = None
     return C3[0] if squeeze else C3
 
 
+def gemm_batched_host(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor, *, partition: str = "auto",
+                      variant: str = "auto", num_iter: int = 1, stream=None) -> torch.Tensor:
+    """kami_gemm_batched_host: C = num_iter * A B^T for CPU tensors (pinned for
+    overlap; contiguous A [batch, M, K], B [batch, N, K], C [batch, M, N]), the
+    host copies pipelined with the product by chunks.  Returns C; it is
+    complete once ``stream`` (default: the current stream) is synchronised."""
+    for x, name in ((A, "A"), (B, "B"), (C, "C")):
+        if x.is_cuda or not x.is_contiguous():
+            raise ValueError(f"{name} must be a contiguous CPU tensor")
+    A3, B3, C3 = _as3(A), _as3(B), _as3(C)
+    batch, M, K = A3.shape
+    N = B3.shape[1]
+    check(load().kami_gemm_batched_host(_DT[A3.dtype], _DT[C3.dtype], _PART[partition], _VAR[variant], M, N, K,
+                                        batch, A3.data_ptr(), B3.data_ptr(), C3.data_ptr(), int(num_iter), None, 0,
+                                        _stream_ptr(stream)))
+    return C
+
+
 def gemm_backward(A: torch.Tensor, B: torch.Tensor, dC: torch.Tensor, *, need_dA: bool = True,
                   need_dB: bool = True, out_dtype: torch.dtype | None = None, stream=None):
     """Gradients of C = A @ B (torch.bmm layout: A [batch, M, K], B [batch,
