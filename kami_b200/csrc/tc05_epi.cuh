@@ -69,6 +69,11 @@ __device__ __forceinline__ void store_chunk(const GemmArgs &g, void *Cb, const f
         t4[q] = make_float4(f[4 * q], f[4 * q + 1], f[4 * q + 2], f[4 * q + 3]);
     __syncwarp();
     const int rr = lane >> 2, cq = (lane & 3) * 4;
+    // plain stores (alpha 1, beta 0, 4-element vectors allowed): the value goes
+    // out as one 16-byte (FP32) or 8-byte (16-bit) store with no per-element
+    // scaling or type dispatch
+    const bool plain = g.c_vec4 && g.alpha == 1.0 && g.beta == 0.0;
+    const int ot = g.out_type;
 #pragma unroll
     for (int i = 0; i < 4; ++i)
     {
@@ -77,8 +82,25 @@ __device__ __forceinline__ void store_chunk(const GemmArgs &g, void *Cb, const f
         {
             const int r = row_base + lr;
             const int c = c0 + cq;
-            if (r < g.M && c < g.N)
-                store4(g, Cb, r, c, *reinterpret_cast<const float4 *>(T + lr * kEpiStride + cq));
+            const float4 x = *reinterpret_cast<const float4 *>(T + lr * kEpiStride + cq);
+            if (plain && r < g.M && c + 3 < g.N)
+            {
+                const int64_t off = (int64_t)r * g.ldc + c;
+                if (ot == KAMI_F32)
+                    *reinterpret_cast<float4 *>(reinterpret_cast<float *>(Cb) + off) = x;
+                else
+                {
+                    const bool bf = ot == KAMI_BF16;
+                    const uint32_t h0 = bf ? __bfloat16_as_ushort(__float2bfloat16_rn(x.x)) : __half_as_ushort(__float2half_rn(x.x));
+                    const uint32_t h1 = bf ? __bfloat16_as_ushort(__float2bfloat16_rn(x.y)) : __half_as_ushort(__float2half_rn(x.y));
+                    const uint32_t h2 = bf ? __bfloat16_as_ushort(__float2bfloat16_rn(x.z)) : __half_as_ushort(__float2half_rn(x.z));
+                    const uint32_t h3 = bf ? __bfloat16_as_ushort(__float2bfloat16_rn(x.w)) : __half_as_ushort(__float2half_rn(x.w));
+                    *reinterpret_cast<uint2 *>(reinterpret_cast<uint16_t *>(Cb) + off) =
+                        make_uint2(h0 | (h1 << 16), h2 | (h3 << 16));
+                }
+            }
+            else if (r < g.M && c < g.N)
+                store4(g, Cb, r, c, x);
         }
     }
     __syncwarp();
