@@ -57,6 +57,14 @@ __device__ __forceinline__ void store4(const GemmArgs &g, void *Cb, int r, int c
     store_pair<float>(g, Cb, r, c + 2, x.z, x.w);
 }
 
+// two values rounded to the 16-bit output type, packed low column first
+__device__ __forceinline__ uint32_t pack2(float x, float y, bool bf)
+{
+    const uint32_t lo = bf ? __bfloat16_as_ushort(__float2bfloat16_rn(x)) : __half_as_ushort(__float2half_rn(x));
+    const uint32_t hi = bf ? __bfloat16_as_ushort(__float2bfloat16_rn(y)) : __half_as_ushort(__float2half_rn(y));
+    return lo | (hi << 16);
+}
+
 // f: the calling thread's 16 values of row (row_base + lane), columns
 // c0..c0+15; nrows: rows this warp holds (32, or 16 for M = 64 MMAs).
 __device__ __forceinline__ void store_chunk(const GemmArgs &g, void *Cb, const float (&f)[16], int row_base,
@@ -91,12 +99,8 @@ __device__ __forceinline__ void store_chunk(const GemmArgs &g, void *Cb, const f
                 else
                 {
                     const bool bf = ot == KAMI_BF16;
-                    const uint32_t h0 = bf ? __bfloat16_as_ushort(__float2bfloat16_rn(x.x)) : __half_as_ushort(__float2half_rn(x.x));
-                    const uint32_t h1 = bf ? __bfloat16_as_ushort(__float2bfloat16_rn(x.y)) : __half_as_ushort(__float2half_rn(x.y));
-                    const uint32_t h2 = bf ? __bfloat16_as_ushort(__float2bfloat16_rn(x.z)) : __half_as_ushort(__float2half_rn(x.z));
-                    const uint32_t h3 = bf ? __bfloat16_as_ushort(__float2bfloat16_rn(x.w)) : __half_as_ushort(__float2half_rn(x.w));
                     *reinterpret_cast<uint2 *>(reinterpret_cast<uint16_t *>(Cb) + off) =
-                        make_uint2(h0 | (h1 << 16), h2 | (h3 << 16));
+                        make_uint2(pack2(x.x, x.y, bf), pack2(x.z, x.w, bf));
                 }
             }
             else if (r < g.M && c < g.N)

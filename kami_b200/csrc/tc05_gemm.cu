@@ -50,6 +50,7 @@ struct Tc05Params
     uint32_t idesc;     // instruction descriptor (N = bn, or bn / P for 2D)
     uint32_t tmem_cols; // allocated TMEM columns (power of two >= 32)
     uint64_t timeout_ns;
+    int store_slots;    // per-problem kernel: staging boxes per warp for bulk C stores (0: per-thread stores)
 };
 
 __device__ __forceinline__ void tc05_flag(int code) { atomicExch(&g_tc05_error, code); }
@@ -117,9 +118,100 @@ __device__ __forceinline__ void issue_mmas(const Tc05Params &p, uint32_t tmem, u
 }
 
 
+// C through bulk tensor stores: each warp packs 128 bytes of each of its rows
+// (32 FP32 or 64 16-bit columns, the sum of the depth accumulators) into a
+// 128B-swizzled staging box and one lane stores the box.  The boxes live in
+// the operand tiles, dead once the MMAs have completed; with fewer slots than
+// boxes a slot is rewritten after the bulk stores have read it.
+struct BulkOut
+{
+    int out_type;
+    int rows, cols;   // valid extent of the output tile (M x N)
+    int bm;           // accumulator rows (MMA M: 64 -> 16 rows per warp, 128 -> 32)
+    int bn;           // accumulator columns read (a whole number of boxes)
+    int depth;        // accumulators summed, bn columns apart
+    int slots;        // staging boxes per warp
+};
+
+__device__ __forceinline__ void epilogue_bulk(const BulkOut &o, const CUtensorMap *tmC, uint32_t tcol, uint8_t *stg,
+                                              int row_base, int prob)
+{
+    const int lane = threadIdx.x & 31;
+    const bool f32 = o.out_type == KAMI_F32, bf = o.out_type == KAMI_BF16;
+    const int rows = o.bm == 128 ? 32 : 16;
+    const int bcols = f32 ? 32 : 64;
+    const int box_bytes = rows * 128;
+    int nb = 0;
+    for (int c0 = 0; c0 < o.bn; c0 += bcols, ++nb)
+    {
+        uint8_t *box = stg + (nb % o.slots) * box_bytes;
+        if (nb >= o.slots)
+        {
+            if (lane == 0)
+                tc::bulk_wait_read<0>();
+            __syncwarp();
+        }
+        uint8_t *row = box + lane * 128;
+        // 16 columns at a time: 64 bytes (FP32) or 32 bytes (16-bit) of the row
+#pragma unroll
+        for (int h = 0; h < 4; ++h)
+        {
+            if (h >= bcols / 16)
+                break;
+            uint32_t v[16];
+            tc::tmem_ld16(tcol + c0 + 16 * h, v);
+            tc::tmem_ld_wait();
+            float f[16];
+#pragma unroll
+            for (int e = 0; e < 16; ++e)
+                f[e] = __uint_as_float(v[e]);
+            for (int d = 1; d < o.depth; ++d)
+            {
+                uint32_t u[16];
+                tc::tmem_ld16(tcol + d * o.bn + c0 + 16 * h, u);
+                tc::tmem_ld_wait();
+#pragma unroll
+                for (int e = 0; e < 16; ++e)
+                    f[e] += __uint_as_float(u[e]);
+            }
+            if (lane < rows)
+            {
+                if (f32)
+                {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        *reinterpret_cast<uint4 *>(row + (((4 * h + q) ^ (lane & 7)) << 4)) =
+                            make_uint4(__float_as_uint(f[4 * q]), __float_as_uint(f[4 * q + 1]),
+                                       __float_as_uint(f[4 * q + 2]), __float_as_uint(f[4 * q + 3]));
+                }
+                else
+                {
+#pragma unroll
+                    for (int q = 0; q < 2; ++q)
+                        *reinterpret_cast<uint4 *>(row + (((2 * h + q) ^ (lane & 7)) << 4)) =
+                            make_uint4(pack2(f[8 * q], f[8 * q + 1], bf), pack2(f[8 * q + 2], f[8 * q + 3], bf),
+                                       pack2(f[8 * q + 4], f[8 * q + 5], bf), pack2(f[8 * q + 6], f[8 * q + 7], bf));
+                }
+            }
+        }
+        tc::fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0)
+        {
+            if (row_base < o.rows && c0 < o.cols)
+                tc::tma_store_3d(tmC, box, c0, row_base, prob);
+            tc::bulk_commit();
+        }
+    }
+    if (lane == 0)
+        tc::bulk_wait_read<0>();
+    __syncwarp();
+}
+
 template <bool BF16>
 __global__ void __launch_bounds__(128) tc05_block_kernel(const __grid_constant__ CUtensorMap tmA,
                                                          const __grid_constant__ CUtensorMap tmB,
+                                                         const __grid_constant__ CUtensorMap tmC,
                                                          const Tc05Params p)
 {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -242,6 +334,13 @@ __global__ void __launch_bounds__(128) tc05_block_kernel(const __grid_constant__
         void *Cb = reinterpret_cast<char *>(g.C) + (int64_t)prob * g.sC * osz;
         const int row_base = p.bm == 128 ? warp * 32 : warp * 16;
         float *T = epi + warp * (kEpiTileBytes / 4);
+        if (p.store_slots > 0)
+        {
+            const BulkOut o{g.out_type, g.M, g.N, p.bm, p.bn, depth, p.store_slots};
+            epilogue_bulk(o, &tmC, tmem + lane_addr, smem + (size_t)warp * p.store_slots * (p.bm == 128 ? 32 : 16) * 128,
+                          row_base, prob);
+        }
+        else
         for (int c0 = 0; c0 < p.bn; c0 += 16)
         {
             uint32_t v[16];
@@ -291,6 +390,12 @@ __global__ void __launch_bounds__(128) tc05_block_kernel(const __grid_constant__
 //                      coalesced C stores), then releases it -- the epilogue
 //                      is the longest phase of a small problem, so several
 //                      drain at once.
+// Plain stores (alpha 1, beta 0, 16-byte aligned C rows and problems) leave
+// through the tensor-store unit: each epilogue warp packs 128 bytes of each of
+// its rows into a 128B-swizzled staging box (32 FP32 or 64 16-bit columns)
+// and one thread issues the box as a bulk tensor store, so C goes out as
+// whole lines while the warp reads the next columns from tensor memory; the
+// accumulator is released as soon as its last columns are in registers.
 // Every wait is bounded like the per-problem kernel's.
 // ---------------------------------------------------------------------------
 struct Tc05StreamParams
@@ -300,13 +405,18 @@ struct Tc05StreamParams
     int stage_bytes; // A + B of one problem (1024-byte multiple)
     int groups;      // epilogue groups of four warps (2 or 4)
     int naccs;       // TMEM accumulators (2..8)
+    int tma_store;   // C written by bulk tensor stores (plain stores only)
+    int store_bufs;  // staging boxes per epilogue warp (1 or 2)
 };
+
+constexpr int kStoreBoxBytes = 4096; // one staging box: up to 32 rows x 128 bytes
 
 constexpr int kStreamMaxGroups = 4;
 
 template <bool BF16>
 __global__ void __launch_bounds__(64 + 128 * kStreamMaxGroups, 1) tc05_stream_kernel(const __grid_constant__ CUtensorMap tmA,
                                                              const __grid_constant__ CUtensorMap tmB,
+                                                             const __grid_constant__ CUtensorMap tmC,
                                                              const Tc05StreamParams sp)
 {
     const Tc05Params &p = sp.t;
@@ -316,8 +426,11 @@ __global__ void __launch_bounds__(64 + 128 * kStreamMaxGroups, 1) tc05_stream_ke
     const int S = sp.stages;
     const int a_box = p.bm * 128, b_box = p.bn * 128;
     const int G = sp.groups, NA = sp.naccs;
-    float *epi = reinterpret_cast<float *>(smem + (size_t)S * sp.stage_bytes); // 4 G x kEpiTileBytes
-    uint64_t *full = reinterpret_cast<uint64_t *>(smem + (size_t)S * sp.stage_bytes + 4 * G * kEpiTileBytes);
+    // per epilogue warp: a transpose tile (kEpiTileBytes) or store_bufs staging boxes
+    const int epi_warp_bytes = sp.tma_store ? sp.store_bufs * kStoreBoxBytes : kEpiTileBytes;
+    uint8_t *epi_base = smem + (size_t)S * sp.stage_bytes;
+    float *epi = reinterpret_cast<float *>(epi_base);
+    uint64_t *full = reinterpret_cast<uint64_t *>(epi_base + 4 * G * epi_warp_bytes);
     uint64_t *empty = full + S;
     uint64_t *tfull = empty + S;   // [NA]
     uint64_t *tempty = tfull + NA; // [NA]
@@ -438,6 +551,94 @@ __global__ void __launch_bounds__(64 + 128 * kStreamMaxGroups, 1) tc05_stream_ke
         const int osz = g.out_type == KAMI_F32 ? 4 : 2;
         float *T = epi + (warp - 2) * (kEpiTileBytes / 4);
         int j = grp;
+        if (sp.tma_store)
+        {
+            const int rows = p.bm == 128 ? 32 : 16;   // accumulator rows this warp holds
+            const int bcols = 128 / osz;              // columns of one staging box
+            const bool f32 = g.out_type == KAMI_F32, bf = g.out_type == KAMI_BF16;
+            uint8_t *stg = epi_base + (size_t)(warp - 2) * sp.store_bufs * kStoreBoxBytes;
+            int nb = 0;
+            for (int64_t prob = blockIdx.x + (int64_t)grp * gridDim.x; prob < nprob;
+                 prob += (int64_t)G * gridDim.x, j += G)
+            {
+                const int b = j % NA;
+                const bool ok = __all_sync(0xffffffffu, tc::mbar_wait_bounded(&tfull[b], (j / NA) & 1, limit));
+                if (!ok)
+                {
+                    tc05_flag(8);
+                    break;
+                }
+                tc::tc_fence_after();
+                for (int c0 = 0; c0 < p.bn; c0 += bcols)
+                {
+                    // this thread's 128 bytes of row (row_base + lane), columns c0..c0+bcols-1
+                    uint32_t w[32];
+#pragma unroll
+                    for (int h = 0; h < 2; ++h)
+                    {
+                        uint32_t v[16], u[16];
+                        const uint32_t col = tmem + lane_addr + (uint32_t)(b * p.bn + c0);
+                        if (f32)
+                        {
+                            tc::tmem_ld16(col + 16 * h, v);
+                            tc::tmem_ld_wait();
+#pragma unroll
+                            for (int e = 0; e < 16; ++e)
+                                w[16 * h + e] = v[e];
+                        }
+                        else
+                        {
+                            tc::tmem_ld16(col + 32 * h, v);
+                            tc::tmem_ld16(col + 32 * h + 16, u);
+                            tc::tmem_ld_wait();
+#pragma unroll
+                            for (int e = 0; e < 8; ++e)
+                            {
+                                w[16 * h + e] = pack2(__uint_as_float(v[2 * e]), __uint_as_float(v[2 * e + 1]), bf);
+                                w[16 * h + 8 + e] = pack2(__uint_as_float(u[2 * e]), __uint_as_float(u[2 * e + 1]), bf);
+                            }
+                        }
+                    }
+                    if (c0 + bcols >= p.bn)
+                    {
+                        // the accumulator's last columns are in registers: free it
+                        tc::tc_fence_before();
+                        __syncwarp();
+                        if (lane == 0)
+                            tc::mbar_arrive(&tempty[b]);
+                    }
+                    uint8_t *box = stg + (nb % sp.store_bufs) * kStoreBoxBytes;
+                    // the box's previous bulk store has finished reading it
+                    if (lane == 0)
+                    {
+                        if (sp.store_bufs == 2)
+                            tc::bulk_wait_read<1>();
+                        else
+                            tc::bulk_wait_read<0>();
+                    }
+                    __syncwarp();
+                    if (lane < rows)
+                    {
+#pragma unroll
+                        for (int q = 0; q < 8; ++q)
+                            *reinterpret_cast<uint4 *>(box + lane * 128 + ((q ^ (lane & 7)) << 4)) =
+                                make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+                    }
+                    tc::fence_proxy_async_smem();
+                    __syncwarp();
+                    if (lane == 0)
+                    {
+                        if (row_base < g.M && c0 < g.N)
+                            tc::tma_store_3d(&tmC, box, c0, row_base, (int)prob);
+                        tc::bulk_commit();
+                    }
+                    ++nb;
+                }
+            }
+            if (lane == 0)
+                tc::bulk_wait_all();
+        }
+        else
         for (int64_t prob = blockIdx.x + (int64_t)grp * gridDim.x; prob < nprob;
              prob += (int64_t)G * gridDim.x, j += G)
         {
@@ -648,21 +849,76 @@ int tc05_plan(int in_type, int out_type, int partition, int P, int M, int N, int
     return KAMI_OK;
 }
 
+// Tensor map of an output for the bulk-store epilogue: boxes of 128 bytes x
+// box_rows rows of one problem, 128B-swizzled.  False when the output does not
+// qualify (plain stores of FP32 / FP16 / BF16 with 16-byte aligned rows and
+// problems, the accumulator width bn a whole number of boxes) or the encoding
+// fails.
+static bool make_store_map(CUtensorMap *map, int out_type, void *C, int N, int M, int64_t batch, int64_t ldc,
+                           int64_t sC, int bn, int box_rows)
+{
+    if (out_type != KAMI_F32 && out_type != KAMI_F16 && out_type != KAMI_BF16)
+        return false;
+    const int osz = out_type == KAMI_F32 ? 4 : 2;
+    const int64_t s2 = batch > 1 ? sC : (int64_t)M * ldc;
+    if ((reinterpret_cast<uintptr_t>(C) & 15) || (ldc * osz) % 16 || s2 <= 0 || (s2 * osz) % 16 || bn % (128 / osz))
+        return false;
+    EncodeTiledFn fn = encode_fn();
+    if (!fn)
+        return false;
+    cuuint64_t dims[3] = {(cuuint64_t)N, (cuuint64_t)M, (cuuint64_t)batch};
+    cuuint64_t strides[2] = {(cuuint64_t)(ldc * osz), (cuuint64_t)(s2 * osz)};
+    cuuint32_t box[3] = {(cuuint32_t)(128 / osz), (cuuint32_t)box_rows, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    const CUtensorMapDataType dt = out_type == KAMI_F32    ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                   : out_type == KAMI_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                                           : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+    return fn(map, dt, 3, C, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+              CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// C of a batched GEMM: bulk stores only for alpha 1, beta 0
+static bool make_c_map(CUtensorMap *map, const GemmArgs &g, int bn, int box_rows)
+{
+    if (g.alpha != 1.0 || g.beta != 0.0)
+        return false;
+    return make_store_map(map, g.out_type, g.C, g.N, g.M, g.batch, g.ldc, g.sC, bn, box_rows);
+}
+
 // Launch the persistent streaming form: one CTA per SM, as many ring slots
-// as shared memory holds (2..6), four epilogue groups when at least three
-// slots still fit beside their tiles (else two), and as many TMEM
-// accumulators as 512 columns hold (at most 8).
+// as shared memory holds (2..6), and as many TMEM accumulators as 512
+// columns hold (at most 8).  With bulk tensor stores: two epilogue groups,
+// two staging boxes per warp when three slots still fit beside them (else
+// one).  Otherwise four epilogue groups when at least three slots still fit
+// beside their transpose tiles (else two).
 static int stream_launch(CUtensorMap &ma, CUtensorMap &mb, Tc05Params &p, bool bf16, cudaStream_t stream)
 {
     Tc05StreamParams sp{};
     sp.t = p;
     sp.stage_bytes = p.nkb * (p.bm + p.bn) * 128;
-    sp.groups = kStreamMaxGroups;
-    int budget = 227 * 1024 - 1024 - 512 - 4 * sp.groups * kEpiTileBytes;
-    if (budget / sp.stage_bytes < 3)
+    CUtensorMap mc = ma;
+    sp.tma_store = make_c_map(&mc, p.g, p.bn, p.bm == 128 ? 32 : 16);
+    int budget;
+    if (sp.tma_store)
     {
         sp.groups = 2;
+        sp.store_bufs = 2;
+        budget = 227 * 1024 - 1024 - 512 - 4 * sp.groups * sp.store_bufs * kStoreBoxBytes;
+        if (budget / sp.stage_bytes < 3)
+        {
+            sp.store_bufs = 1;
+            budget = 227 * 1024 - 1024 - 512 - 4 * sp.groups * sp.store_bufs * kStoreBoxBytes;
+        }
+    }
+    else
+    {
+        sp.groups = kStreamMaxGroups;
         budget = 227 * 1024 - 1024 - 512 - 4 * sp.groups * kEpiTileBytes;
+        if (budget / sp.stage_bytes < 3)
+        {
+            sp.groups = 2;
+            budget = 227 * 1024 - 1024 - 512 - 4 * sp.groups * kEpiTileBytes;
+        }
     }
     sp.stages = std::min(6, budget / sp.stage_bytes);
     if (sp.stages < 2)
@@ -674,7 +930,9 @@ static int stream_launch(CUtensorMap &ma, CUtensorMap &mb, Tc05Params &p, bool b
         cols <<= 1;
     sp.t.tmem_cols = cols;
     sp.t.timeout_ns = p.timeout_ns + 500000000ull;
-    const size_t smem = (size_t)sp.stages * sp.stage_bytes + 4 * sp.groups * kEpiTileBytes + 1024 + 512;
+    const size_t epi = sp.tma_store ? (size_t)4 * sp.groups * sp.store_bufs * kStoreBoxBytes
+                                    : (size_t)4 * sp.groups * kEpiTileBytes;
+    const size_t smem = (size_t)sp.stages * sp.stage_bytes + epi + 1024 + 512;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -686,7 +944,7 @@ static int stream_launch(CUtensorMap &ma, CUtensorMap &mb, Tc05Params &p, bool b
     if (e != cudaSuccess)
         return cuda_fail(e, "cudaFuncSetAttribute(tc05_stream_kernel)");
     const int64_t grid = std::min<int64_t>(p.g.batch, sms);
-    void *args[] = {&ma, &mb, &sp};
+    void *args[] = {&ma, &mb, &mc, &sp};
     e = cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(64 + 128 * sp.groups), args, smem, stream);
     if (e != cudaSuccess)
         return cuda_fail(e, "cudaLaunchKernel(tc05_stream_kernel)");
@@ -740,6 +998,16 @@ int tc05_launch(const GemmArgs &g, int in_type, int partition, int P, void *, si
         2 * stage_bytes <= 227 * 1024 - 1024 - 512 - 8 * kEpiTileBytes)
         return stream_launch(ma, mb, p, bf16, stream);
 
+    // bulk C stores staged in the operand tiles and transpose tiles (dead
+    // after the MMAs): as many boxes per warp as they hold, up to all of them
+    CUtensorMap mc = ma;
+    const int rows = s.bm == 128 ? 32 : 16;
+    if (make_c_map(&mc, g, s.bn, rows))
+    {
+        const int boxes = s.bn / (g.out_type == KAMI_F32 ? 32 : 64);
+        const int region = s.nkb * ((s.a_tmem ? 0 : s.bm) + s.bn) * 128 + 4 * kEpiTileBytes;
+        p.store_slots = std::min(boxes, region / (4 * rows * 128));
+    }
     const void *fn = bf16 ? (const void *)&tc05_block_kernel<true> : (const void *)&tc05_block_kernel<false>;
     static std::once_flag once[2];
     cudaError_t e = cudaSuccess;
@@ -748,7 +1016,7 @@ int tc05_launch(const GemmArgs &g, int in_type, int partition, int P, void *, si
     });
     if (e != cudaSuccess)
         return cuda_fail(e, "cudaFuncSetAttribute(tc05_block_kernel)");
-    void *args[] = {&ma, &mb, &p};
+    void *args[] = {&ma, &mb, &mc, &p};
     e = cudaLaunchKernel(fn, dim3((unsigned)g.batch), dim3(128), args, s.smem, stream);
     if (e != cudaSuccess)
         return cuda_fail(e, "cudaLaunchKernel(tc05_block_kernel)");
@@ -780,12 +1048,15 @@ struct Tc05BwdParams
     uint32_t idesc_a, idesc_b; // dA: M x K (K-major, K-major); dB: K x N (MN-major, MN-major)
     uint32_t tmem_cols;
     uint64_t timeout_ns;
+    int slots_a, slots_b;      // staging boxes per warp for bulk stores of dA / dB (0: per-thread stores)
 };
 
 template <bool BF16>
 __global__ void __launch_bounds__(128) tc05_bwd_kernel(const __grid_constant__ CUtensorMap tmG,
                                                        const __grid_constant__ CUtensorMap tmA,
                                                        const __grid_constant__ CUtensorMap tmB,
+                                                       const __grid_constant__ CUtensorMap tmDA,
+                                                       const __grid_constant__ CUtensorMap tmDB,
                                                        const Tc05BwdParams p)
 {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -867,10 +1138,12 @@ __global__ void __launch_bounds__(128) tc05_bwd_kernel(const __grid_constant__ C
     }
     __syncwarp();
 
-    const bool done = __all_sync(0xffffffffu, tc::mbar_wait_bounded(&bars[1], 0, p.timeout_ns));
+    const bool done_w = __all_sync(0xffffffffu, tc::mbar_wait_bounded(&bars[1], 0, p.timeout_ns));
     tc::tc_fence_after();
-    if (!done)
+    if (!done_w)
         tc05_flag(2);
+    // block-uniform outcome: the epilogue below holds a block barrier
+    const bool done = __syncthreads_and(done_w);
     const bool ok = done && *reinterpret_cast<volatile int *>(ok_slot);
     if (ok)
     {
@@ -895,6 +1168,20 @@ __global__ void __launch_bounds__(128) tc05_bwd_kernel(const __grid_constant__ C
             g.beta = 0.0;
             void *Cb = reinterpret_cast<char *>(out) + (int64_t)prob * rows * cols * osz;
             const int row_base = rows == 128 ? warp * 32 : warp * 16;
+            const int slots = which == 0 ? p.slots_a : p.slots_b;
+            // dB's staging (or transpose tiles) may overlap boxes of another
+            // warp's dA stores: every warp's dA boxes have been read first
+            // (each warp waits for its own stores at the end of its pass)
+            if (which == 1 && p.dA && p.slots_a > 0)
+                __syncthreads();
+            if (slots > 0)
+            {
+                // staged in the dC / A / B tiles, dead after the MMAs
+                const BulkOut o{p.out_type, rows, cols, rows, cols, 1, slots};
+                epilogue_bulk(o, which == 0 ? &tmDA : &tmDB, tmem + lane_addr + col0,
+                              smem + (size_t)warp * slots * (rows == 128 ? 32 : 16) * 128, row_base, prob);
+                continue;
+            }
             for (int c0 = 0; c0 < cols; c0 += 16)
             {
                 uint32_t v[16];
@@ -955,6 +1242,14 @@ int tc05_backward_launch(int in_type, int out_type, int M, int N, int K, int64_t
     p.tmem_cols = cols;
     p.timeout_ns = (uint64_t)(5e8 + (double)(M + N) * 4000.0);
     const size_t smem = (size_t)(M * N + M * K + K * N) * 2 + 4 * kEpiTileBytes + 64 + 1024;
+    // bulk stores of each gradient, staged in the operand and transpose tiles
+    CUtensorMap mda = mg, mdb = mg;
+    const int region = (M * N + M * K + K * N) * 2 + 4 * kEpiTileBytes;
+    const int bcols = out_type == KAMI_F32 ? 32 : 64;
+    if (dA && make_store_map(&mda, out_type, dA, K, M, batch, K, (int64_t)M * K, K, M == 128 ? 32 : 16))
+        p.slots_a = std::min(K / bcols, region / (4 * (M == 128 ? 32 : 16) * 128));
+    if (dB && make_store_map(&mdb, out_type, dB, N, K, batch, N, (int64_t)K * N, N, K == 128 ? 32 : 16))
+        p.slots_b = std::min(N / bcols, region / (4 * (K == 128 ? 32 : 16) * 128));
     const void *fn = bf16 ? (const void *)&tc05_bwd_kernel<true> : (const void *)&tc05_bwd_kernel<false>;
     static std::once_flag once[2];
     cudaError_t e = cudaSuccess;
@@ -963,7 +1258,7 @@ int tc05_backward_launch(int in_type, int out_type, int M, int N, int K, int64_t
     });
     if (e != cudaSuccess)
         return cuda_fail(e, "cudaFuncSetAttribute(tc05_bwd_kernel)");
-    void *args[] = {&mg, &ma, &mb, &p};
+    void *args[] = {&mg, &ma, &mb, &mda, &mdb, &p};
     e = cudaLaunchKernel(fn, dim3((unsigned)batch), dim3(128), args, smem, stream);
     if (e != cudaSuccess)
         return cuda_fail(e, "cudaLaunchKernel(tc05_bwd_kernel)");

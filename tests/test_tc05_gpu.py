@@ -153,3 +153,60 @@ def test_tc05_a_in_tmem_num_iter(cuda):
     A, B, A64, B64 = _inputs("f16", 4, 128, 128, 128, integer=True, seed=9)
     C = api.gemm_batched(A, B, variant="tcgen05_ts", num_iter=1000)
     assert np.array_equal(C.double().cpu().numpy(), oracle.gemm(A64, B64) * 1000)
+
+
+@pytest.mark.parametrize("odt", [torch.float32, torch.float16, torch.bfloat16])
+@pytest.mark.parametrize("M,N,K,batch", [(128, 128, 128, 600), (100, 128, 128, 300), (128, 120, 128, 300),
+                                         (128, 192, 64, 200), (128, 96, 128, 300), (128, 100, 128, 150),
+                                         (128, 128, 128, 1), (64, 128, 256, 300)])
+def test_tc05_streamed_store_paths(cuda, odt, M, N, K, batch):
+    """The persistent streaming form (problems of at least 32 KB of operands)
+    over its two C paths: bulk tensor stores of 128-byte boxes when C rows
+    and problems are 16-byte aligned and the padded N is a whole number of
+    boxes, per-thread stores otherwise (here N = 100 with 16-bit C, N = 96
+    with 16-bit C).  C is a column slice of a wider buffer, so rows are
+    padded: the padding must stay untouched and row tails clipped."""
+    rng = np.random.default_rng(M * N + K + batch)
+    A64 = rng.integers(-2, 3, (batch, M, K)).astype(np.float64)
+    B64 = rng.integers(-2, 3, (batch, N, K)).astype(np.float64)
+    A = torch.tensor(A64, dtype=torch.float16).cuda()
+    B = torch.tensor(B64, dtype=torch.float16).cuda()
+    ldc = N + 8
+    big = torch.full((batch, M, ldc), 7.0, dtype=odt, device="cuda")
+    C = big[:, :, :N]
+    api.gemm_batched(A, B, C, variant="tcgen05")
+    torch.cuda.synchronize()
+    _status_clean()
+    ref = oracle.gemm(A64, B64)
+    assert np.array_equal(C.double().cpu().numpy(), torch.tensor(ref).to(odt).double().numpy())
+    assert bool((big[:, :, N:] == 7.0).all())
+    # contiguous C as well
+    C2 = api.gemm_batched(A, B, variant="tcgen05", out_dtype=odt if odt != torch.float32 else None)
+    assert np.array_equal(C2.double().cpu().numpy(), torch.tensor(ref).to(odt).double().numpy())
+
+
+@pytest.mark.parametrize("odt", [torch.float32, torch.float16, torch.bfloat16])
+@pytest.mark.parametrize("M,N,K,num_iter,part,P", [(128, 64, 64, 1, "1d", 0), (100, 64, 64, 1, "1d", 0),
+                                                   (128, 96, 64, 1, "1d", 0), (64, 128, 64, 1, "1d", 0),
+                                                   (50, 120, 32, 1, "1d", 0), (128, 128, 128, 8, "1d", 0),
+                                                   (128, 128, 128, 1, "2d", 2), (128, 128, 64, 1, "3d", 2),
+                                                   (64, 64, 64, 1, "3d", 4)])
+def test_tc05_per_problem_store_paths(cuda, odt, M, N, K, num_iter, part, P):
+    """The one-CTA-per-problem form (problems under 32 KB of operands, the
+    repeated-product mode and the 2D / 3D mappings) over its two C paths:
+    bulk tensor stores staged in the dead operand tiles, or per-thread
+    stores.  C rows are padded; the padding must stay untouched."""
+    batch = 37
+    rng = np.random.default_rng(M + 7 * N + K + num_iter)
+    A64 = rng.integers(-2, 3, (batch, M, K)).astype(np.float64)
+    B64 = rng.integers(-2, 3, (batch, N, K)).astype(np.float64)
+    A = torch.tensor(A64, dtype=torch.float16).cuda()
+    B = torch.tensor(B64, dtype=torch.float16).cuda()
+    big = torch.full((batch, M, N + 8), 7.0, dtype=odt, device="cuda")
+    C = big[:, :, :N]
+    api.gemm_batched(A, B, C, variant="tcgen05", partition=part, P=P, num_iter=num_iter)
+    torch.cuda.synchronize()
+    _status_clean()
+    ref = oracle.gemm(A64, B64) * num_iter
+    assert np.array_equal(C.double().cpu().numpy(), torch.tensor(ref).to(odt).double().numpy())
+    assert bool((big[:, :, N:] == 7.0).all())
