@@ -110,9 +110,9 @@ int kami_selftest_bounded_wait(uint64_t timeout_ns, void *stream);
  * NUM_ITER.
  *
  * Replaces the launches of
- *   block_gemm_{1d,2d,3d}_half_mma   (src/block_gemm/KAMI/{1d,2d,3d}/fp16/*.cu:61/64/61)
- *   block_gemm_{1d,2d,3d}_double_mma (src/block_gemm/KAMI/{1d,2d,3d}/fp64/*.cu:55/61/62)
- *   batched_gemm_{1d,2d,3d}_double_mma (src/batched_gemm/KAMI/{1d,2d,3d}/*.cu:59/65/64)
+ *   block_gemm_{1d,2d,3d}_half_mma   (src/block_gemm/KAMI/{1d,2d,3d}/fp16/<file>.cu:61/64/61)
+ *   block_gemm_{1d,2d,3d}_double_mma (src/block_gemm/KAMI/{1d,2d,3d}/fp64/<file>.cu:55/61/62)
+ *   batched_gemm_{1d,2d,3d}_double_mma (src/batched_gemm/KAMI/{1d,2d,3d}/<file>.cu:59/65/64)
  * whose signature is (const T *A, const T *B, T *C, T alpha, T beta).  The
  * reference ignores alpha and beta; here they are applied.  The 3D partition
  * reduces its P partial C slices on the device instead of writing a P-times

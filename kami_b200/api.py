@@ -24,7 +24,15 @@ _AL = {"row_mk": _lib.A_ROW_MK, "col_mk": _lib.A_COL_MK}
 _BL = {"ref_nk": _lib.B_REF_NK, "row_kn": _lib.B_ROW_KN}
 
 
+_raw_stream = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+_cur_device = getattr(torch._C, "_cuda_getDevice", None)
+
+
 def _stream_ptr(stream) -> int:
+    """The CUDA stream handle to launch on: ``stream``, else the current
+    stream of the current device (read without building a Stream object)."""
+    if stream is None and _raw_stream is not None and _cur_device is not None:
+        return _raw_stream(_cur_device())
     s = stream if stream is not None else torch.cuda.current_stream()
     return int(s.cuda_stream)
 
@@ -89,6 +97,24 @@ def gemm_batched(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = None
     if C is not None:
         return C
     return C3[0] if squeeze else C3
+
+
+def bmm_forward(A: torch.Tensor, B: torch.Tensor) -> torch.Tensor:
+    """C = A @ B in torch.bmm layout (A [batch, M, K], B [batch, K, N], both
+    contiguous CUDA tensors of one dtype: float16, bfloat16 or float64),
+    returned in the input dtype: kami_gemm_batched with B as the K x N
+    operand and the library's kernel choice, with the fewest host steps (the
+    forward of the autograd function)."""
+    batch, M, K = A.shape
+    N = B.shape[2]
+    if B.shape[0] != batch or B.shape[1] != K:
+        raise ValueError("shapes do not match C = A @ B")
+    dt = _DT[A.dtype]
+    C = torch.empty((batch, M, N), dtype=A.dtype, device=A.device)
+    check(load().kami_gemm_batched(dt, dt, _lib.PARTITION_AUTO, _lib.VARIANT_AUTO, M, N, K, 0, 0, batch,
+                                   A.data_ptr(), K, M * K, _lib.A_ROW_MK, B.data_ptr(), N, K * N, _lib.B_ROW_KN,
+                                   C.data_ptr(), N, M * N, 1.0, 0.0, 1, None, 0, _stream_ptr(None)))
+    return C
 
 
 def gemm_batched_host(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor, *, partition: str = "auto",

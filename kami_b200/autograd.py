@@ -35,6 +35,8 @@ class KamiBmm(torch.autograd.Function):
         B = B.contiguous()
         ctx.save_for_backward(A, B)
         ctx.partition, ctx.variant = partition, variant
+        if partition == "auto" and variant == "auto" and A.dim() == 3 and B.dim() == 3 and A.is_cuda and B.is_cuda:
+            return api.bmm_forward(A, B)
         return api.gemm_batched(A, B, b_layout="row_kn", partition=partition, variant=variant,
                                 out_dtype=_out_dtype(A.dtype))
 

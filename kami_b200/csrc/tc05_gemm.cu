@@ -25,6 +25,7 @@
 // in g_tc05_error, waits (bounded) for its copies in flight, frees TMEM and
 // returns.
 #include <algorithm>
+#include <cstring>
 #include <mutex>
 
 #include "kami_common.cuh"
@@ -699,6 +700,67 @@ static EncodeTiledFn encode_fn()
     return fn;
 }
 
+// Encoded maps of the last few requests, per host thread: a training loop
+// asks for the same maps call after call (the caching allocator hands back
+// the same buffers), and a hit skips the driver's encoding.
+struct MapKey
+{
+    const void *base;
+    cuuint64_t dims[3], strides[2];
+    cuuint32_t box[3];
+    int dt, rank, swizzle, l2, oob;
+};
+
+static CUresult encode_cached(CUtensorMap *map, CUtensorMapDataType dt, cuuint32_t rank, void *base,
+                              const cuuint64_t *dims, const cuuint64_t *strides, const cuuint32_t *box,
+                              CUtensorMapSwizzle swizzle, CUtensorMapL2promotion l2, CUtensorMapFloatOOBfill oob)
+{
+    struct Entry
+    {
+        MapKey k;
+        CUtensorMap m;
+        bool used;
+    };
+    thread_local Entry cache[8];
+    thread_local int next = 0;
+    if (rank > 3)
+        return CUDA_ERROR_INVALID_VALUE;
+    MapKey k;
+    memset(&k, 0, sizeof(k));
+    k.base = base;
+    for (cuuint32_t i = 0; i < rank; ++i)
+    {
+        k.dims[i] = dims[i];
+        k.box[i] = box[i];
+        if (i + 1 < rank)
+            k.strides[i] = strides[i];
+    }
+    k.dt = (int)dt;
+    k.rank = (int)rank;
+    k.swizzle = (int)swizzle;
+    k.l2 = (int)l2;
+    k.oob = (int)oob;
+    for (int i = 0; i < 8; ++i)
+        if (cache[i].used && memcmp(&cache[i].k, &k, sizeof(k)) == 0)
+        {
+            *map = cache[i].m;
+            return CUDA_SUCCESS;
+        }
+    EncodeTiledFn fn = encode_fn();
+    if (!fn)
+        return CUDA_ERROR_NOT_SUPPORTED;
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = fn(map, dt, rank, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle, l2, oob);
+    if (r == CUDA_SUCCESS)
+    {
+        cache[next].k = k;
+        cache[next].m = *map;
+        cache[next].used = true;
+        next = (next + 1) & 7;
+    }
+    return r;
+}
+
 // 3D map {K, rows, batch} over a K-major operand, box {64, box_rows, 1},
 // 128-byte swizzle, zero fill out of bounds.  With mn_major the operand is
 // stored K x rows (rows contiguous): map {rows, K, batch}, box {64, 64, 1}.
@@ -714,11 +776,9 @@ static int make_map(CUtensorMap *map, bool bf16, const void *base, int K, int ro
         const int64_t s2 = batch > 1 ? stride : (int64_t)K * ld;
         cuuint64_t strides[2] = {(cuuint64_t)(ld * 2), (cuuint64_t)(s2 * 2)};
         cuuint32_t box[3] = {64, 64, 1};
-        cuuint32_t estr[3] = {1, 1, 1};
-        CUresult r = fn(map, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3,
-                        const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                        CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        CUresult r = encode_cached(map, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3,
+                                   const_cast<void *>(base), dims, strides, box, CU_TENSOR_MAP_SWIZZLE_128B,
+                                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
         if (r != CUDA_SUCCESS)
             return fail(KAMI_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled failed (%d) for an MN-major operand", (int)r);
         return KAMI_OK;
@@ -730,11 +790,9 @@ static int make_map(CUtensorMap *map, bool bf16, const void *base, int K, int ro
     const int64_t s2 = batch > 1 ? stride : (int64_t)rows * ld;
     cuuint64_t strides[2] = {(cuuint64_t)(ld * 2), (cuuint64_t)(s2 * 2)};
     cuuint32_t box[3] = {64, (cuuint32_t)box_rows, 1};
-    cuuint32_t estr[3] = {1, 1, 1};
-    CUresult r = fn(map, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3,
-                    const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                    CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    CUresult r = encode_cached(map, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3,
+                               const_cast<void *>(base), dims, strides, box, CU_TENSOR_MAP_SWIZZLE_128B,
+                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS)
         return fail(KAMI_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled failed (%d) for K=%d rows=%d ld=%lld", (int)r, K,
                     rows, (long long)ld);
@@ -835,7 +893,7 @@ bool tc05_prefer_ts(int M, int a_layout) { return false && M > 64 && a_layout ==
 int tc05_plan(int in_type, int out_type, int partition, int P, int M, int N, int K, int64_t batch, int a_layout,
               int b_layout, LaunchInfo *info, int a_tmem)
 {
-    Tc05Shape s;
+    Tc05Shape s{};
     int st = tc05_shape(in_type, out_type, partition, P, M, N, K, a_layout, b_layout, &s, a_tmem);
     if (st)
         return st;
@@ -863,18 +921,14 @@ static bool make_store_map(CUtensorMap *map, int out_type, void *C, int N, int M
     const int64_t s2 = batch > 1 ? sC : (int64_t)M * ldc;
     if ((reinterpret_cast<uintptr_t>(C) & 15) || (ldc * osz) % 16 || s2 <= 0 || (s2 * osz) % 16 || bn % (128 / osz))
         return false;
-    EncodeTiledFn fn = encode_fn();
-    if (!fn)
-        return false;
     cuuint64_t dims[3] = {(cuuint64_t)N, (cuuint64_t)M, (cuuint64_t)batch};
     cuuint64_t strides[2] = {(cuuint64_t)(ldc * osz), (cuuint64_t)(s2 * osz)};
     cuuint32_t box[3] = {(cuuint32_t)(128 / osz), (cuuint32_t)box_rows, 1};
-    cuuint32_t estr[3] = {1, 1, 1};
     const CUtensorMapDataType dt = out_type == KAMI_F32    ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
                                    : out_type == KAMI_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
                                                            : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
-    return fn(map, dt, 3, C, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-              CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    return encode_cached(map, dt, 3, C, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 // C of a batched GEMM: bulk stores only for alpha 1, beta 0
@@ -954,7 +1008,7 @@ static int stream_launch(CUtensorMap &ma, CUtensorMap &mb, Tc05Params &p, bool b
 int tc05_launch(const GemmArgs &g, int in_type, int partition, int P, void *, size_t, cudaStream_t stream,
                 int a_tmem)
 {
-    Tc05Shape s;
+    Tc05Shape s{};
     int st = tc05_shape(in_type, g.out_type, partition, P, g.M, g.N, g.K, g.a_layout, g.b_layout, &s, a_tmem);
     if (st)
         return st;
