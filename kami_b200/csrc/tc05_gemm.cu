@@ -250,6 +250,8 @@ __global__ void __launch_bounds__(128) tc05_block_kernel(const __grid_constant__
 
     if (threadIdx.x == 0)
     {
+        // loaded after the TMEM allocation and the block barrier: issuing them
+        // first measured slower (BF16 64^3 x 4096: 37.8 against 31.6 us)
         const uint32_t bytes = (uint32_t)(p.nkb * (a_box + b_box)); // a_box is 0 when A lives in TMEM
         tc::mbar_expect_tx(&bars[0], bytes);
         for (int kb = 0; kb < p.nkb; ++kb)
@@ -439,6 +441,26 @@ __global__ void __launch_bounds__(64 + 128 * kStreamMaxGroups, 1) tc05_stream_ke
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t nprob = g.batch;
+    // one problem's A and B into slot st (the producer thread)
+    auto load_slot = [&](int st, int64_t prob) {
+        uint8_t *sA = smem + (size_t)st * sp.stage_bytes;
+        uint8_t *sB = sA + p.nkb * a_box;
+        tc::mbar_expect_tx(&full[st], (uint32_t)sp.stage_bytes);
+        for (int kb = 0; kb < p.nkb; ++kb)
+        {
+            if (p.a_mn)
+                for (int mc = 0; mc < p.bm / 64; ++mc)
+                    tc::tma_load_3d(sA + kb * a_box + mc * 8192, &tmA, &full[st], mc * 64, kb * 64, (int)prob);
+            else
+                tc::tma_load_3d(sA + kb * a_box, &tmA, &full[st], kb * 64, 0, (int)prob);
+            if (p.b_mn)
+                for (int nc = 0; nc < p.bn / 64; ++nc)
+                    tc::tma_load_3d(sB + kb * b_box + nc * 8192, &tmB, &full[st], nc * 64, kb * 64, (int)prob);
+            else
+                tc::tma_load_3d(sB + kb * b_box, &tmB, &full[st], kb * 64, 0, (int)prob);
+        }
+    };
+    int j0 = 0; // problems whose loads thread 0 issued during setup
     if (threadIdx.x == 0)
     {
         for (int i = 0; i < S; ++i)
@@ -452,6 +474,10 @@ __global__ void __launch_bounds__(64 + 128 * kStreamMaxGroups, 1) tc05_stream_ke
             tc::mbar_init(&tempty[i], 4);
         }
         tc::fence_mbar_init();
+        // every slot is free: the first loads start before the TMEM
+        // allocation and the block barrier
+        for (int64_t prob = blockIdx.x; prob < nprob && j0 < S; prob += gridDim.x, ++j0)
+            load_slot(j0, prob);
     }
     __syncwarp();
     if (warp == 1)
@@ -469,8 +495,8 @@ __global__ void __launch_bounds__(64 + 128 * kStreamMaxGroups, 1) tc05_stream_ke
     {
         if (lane == 0)
         {
-            int j = 0;
-            for (int64_t prob = blockIdx.x; prob < nprob; prob += gridDim.x, ++j)
+            int j = j0;
+            for (int64_t prob = blockIdx.x + (int64_t)j0 * gridDim.x; prob < nprob; prob += gridDim.x, ++j)
             {
                 const int st = j % S;
                 if (j >= S && !tc::mbar_wait_bounded(&empty[st], ((j / S) - 1) & 1, limit))
@@ -478,22 +504,7 @@ __global__ void __launch_bounds__(64 + 128 * kStreamMaxGroups, 1) tc05_stream_ke
                     tc05_flag(5);
                     break;
                 }
-                uint8_t *sA = smem + (size_t)st * sp.stage_bytes;
-                uint8_t *sB = sA + p.nkb * a_box;
-                tc::mbar_expect_tx(&full[st], (uint32_t)sp.stage_bytes);
-                for (int kb = 0; kb < p.nkb; ++kb)
-                {
-                    if (p.a_mn)
-                        for (int mc = 0; mc < p.bm / 64; ++mc)
-                            tc::tma_load_3d(sA + kb * a_box + mc * 8192, &tmA, &full[st], mc * 64, kb * 64, (int)prob);
-                    else
-                        tc::tma_load_3d(sA + kb * a_box, &tmA, &full[st], kb * 64, 0, (int)prob);
-                    if (p.b_mn)
-                        for (int nc = 0; nc < p.bn / 64; ++nc)
-                            tc::tma_load_3d(sB + kb * b_box + nc * 8192, &tmB, &full[st], nc * 64, kb * 64, (int)prob);
-                    else
-                        tc::tma_load_3d(sB + kb * b_box, &tmB, &full[st], kb * 64, 0, (int)prob);
-                }
+                load_slot(st, prob);
             }
             // copies of the last slots still in flight complete before exit
             const int jn = j;
