@@ -385,7 +385,16 @@ __global__ void __launch_bounds__(128) tc05_block_kernel(const __grid_constant__
 //                      each holding one problem's A and B;
 //   warp 1 (one lane)  MMA issuer: a ring of `naccs` TMEM accumulators (as
 //                      many as 512 columns hold, at most 8), commits free the
-//                      slot and publish the accumulator;
+//                      slot and publish the accumulator; for problems of
+//                      16-32 KB of operands a second issuer (the last warp)
+//                      takes the odd problems, because one thread's issue,
+//                      commit and barrier work (~1k cycles per 64^3 problem)
+//                      bounds the rate -- only with an even number of slots
+//                      and of accumulators, so that every slot and
+//                      accumulator belongs to one issuer, which consumes its
+//                      phases in order (shared ones let an issuer wait for a
+//                      phase two ahead of the last one completed, which
+//                      parity-based waits cannot tell apart);
 //   warps 2..          epilogue, `groups` groups of four (two, or four when
 //                      shared memory leaves room for their transpose tiles):
 //                      group g drains the accumulator of every problem j with
@@ -410,6 +419,7 @@ struct Tc05StreamParams
     int naccs;       // TMEM accumulators (2..8)
     int tma_store;   // C written by bulk tensor stores (plain stores only)
     int store_bufs;  // staging boxes per epilogue warp (1 or 2)
+    int issuers;     // MMA-issuing threads (2 only with even stages and naccs)
 };
 
 constexpr int kStoreBoxBytes = 4096; // one staging box: up to 32 rows x 128 bytes
@@ -417,7 +427,7 @@ constexpr int kStoreBoxBytes = 4096; // one staging box: up to 32 rows x 128 byt
 constexpr int kStreamMaxGroups = 4;
 
 template <bool BF16>
-__global__ void __launch_bounds__(64 + 128 * kStreamMaxGroups, 1) tc05_stream_kernel(const __grid_constant__ CUtensorMap tmA,
+__global__ void __launch_bounds__(96 + 128 * kStreamMaxGroups, 1) tc05_stream_kernel(const __grid_constant__ CUtensorMap tmA,
                                                              const __grid_constant__ CUtensorMap tmB,
                                                              const __grid_constant__ CUtensorMap tmC,
                                                              const Tc05StreamParams sp)
@@ -512,12 +522,15 @@ __global__ void __launch_bounds__(64 + 128 * kStreamMaxGroups, 1) tc05_stream_ke
                 tc::mbar_wait_bounded(&full[k % S], (k / S) & 1, limit);
         }
     }
-    else if (warp == 1)
+    else if (warp == 1 || (sp.issuers == 2 && warp == 2 + 4 * G))
     {
+        // issuer t takes the problems j with j % issuers == t
+        const int t = warp == 1 ? 0 : 1;
         if (lane == 0)
         {
-            int j = 0;
-            for (int64_t prob = blockIdx.x; prob < nprob; prob += gridDim.x, ++j)
+            int j = t;
+            for (int64_t prob = blockIdx.x + (int64_t)t * gridDim.x; prob < nprob;
+                 prob += (int64_t)sp.issuers * gridDim.x, j += sp.issuers)
             {
                 const int st = j % S, b = j % NA;
                 if (!tc::mbar_wait_bounded(&full[st], (j / S) & 1, limit))
@@ -552,7 +565,7 @@ __global__ void __launch_bounds__(64 + 128 * kStreamMaxGroups, 1) tc05_stream_ke
             }
         }
     }
-    else
+    else if (warp < 2 + 4 * G)
     {
         // epilogue group g = warps 2+4g .. 5+4g, covering TMEM lane quadrants
         // 2, 3, 0, 1
@@ -956,13 +969,20 @@ static bool make_c_map(CUtensorMap *map, const GemmArgs &g, int bn, int box_rows
 // two staging boxes per warp when three slots still fit beside them (else
 // one).  Otherwise four epilogue groups when at least three slots still fit
 // beside their transpose tiles (else two).
-static int stream_launch(CUtensorMap &ma, CUtensorMap &mb, Tc05Params &p, bool bf16, cudaStream_t stream)
+static int stream_launch(CUtensorMap &ma, CUtensorMap &mb, Tc05Params &p, bool bf16, cudaStream_t stream,
+                         bool need_two)
 {
     Tc05StreamParams sp{};
     sp.t = p;
     sp.stage_bytes = p.nkb * (p.bm + p.bn) * 128;
     CUtensorMap mc = ma;
     sp.tma_store = make_c_map(&mc, p.g, p.bn, p.bm == 128 ? 32 : 16);
+    // accumulators: at least as many as epilogue groups.  Group j % groups
+    // drains problem j from accumulator j % naccs; with fewer accumulators the
+    // next user of an accumulator belongs to a group whose previous problem
+    // is older, which can reach its wait while the accumulator's current phase
+    // is still open -- a parity wait for the phase after it passes at once.
+    sp.naccs = std::min(8, 512 / p.bn);
     int budget;
     if (sp.tma_store)
     {
@@ -979,7 +999,7 @@ static int stream_launch(CUtensorMap &ma, CUtensorMap &mb, Tc05Params &p, bool b
     {
         sp.groups = kStreamMaxGroups;
         budget = 227 * 1024 - 1024 - 512 - 4 * sp.groups * kEpiTileBytes;
-        if (budget / sp.stage_bytes < 3)
+        if (budget / sp.stage_bytes < 3 || sp.naccs < sp.groups)
         {
             sp.groups = 2;
             budget = 227 * 1024 - 1024 - 512 - 4 * sp.groups * kEpiTileBytes;
@@ -989,7 +1009,6 @@ static int stream_launch(CUtensorMap &ma, CUtensorMap &mb, Tc05Params &p, bool b
     if (sp.stages < 2)
         return fail(KAMI_ERR_UNSUPPORTED, "tcgen05 streaming form: a problem needs %d bytes of shared memory",
                     sp.stage_bytes);
-    sp.naccs = std::min(8, 512 / p.bn);
     uint32_t cols = 32;
     while ((int)cols < sp.naccs * p.bn)
         cols <<= 1;
@@ -1009,8 +1028,12 @@ static int stream_launch(CUtensorMap &ma, CUtensorMap &mb, Tc05Params &p, bool b
     if (e != cudaSuccess)
         return cuda_fail(e, "cudaFuncSetAttribute(tc05_stream_kernel)");
     const int64_t grid = std::min<int64_t>(p.g.batch, sms);
+    sp.issuers = sp.stage_bytes < 32768 && sp.stages % 2 == 0 && sp.naccs % 2 == 0 ? 2 : 1;
+    if (need_two && sp.issuers != 2)
+        return KAMI_ERR_UNSUPPORTED; // nothing launched: the caller runs one CTA per problem
     void *args[] = {&ma, &mb, &mc, &sp};
-    e = cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(64 + 128 * sp.groups), args, smem, stream);
+    e = cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(64 + 128 * sp.groups + 32 * (sp.issuers - 1)), args, smem,
+                         stream);
     if (e != cudaSuccess)
         return cuda_fail(e, "cudaLaunchKernel(tc05_stream_kernel)");
     return KAMI_OK;
@@ -1055,13 +1078,20 @@ int tc05_launch(const GemmArgs &g, int in_type, int partition, int P, void *, si
     p.timeout_ns = (uint64_t)(5e8 + mmas * 2000.0);
 
     // Streamed regime: the persistent form for problems of >= 32 KB of operands
-    // (measured on B200: 128^3 x 592 121 vs 105 TFLOP/s, x 8192 190 vs 150);
-    // smaller problems drain as fast as one CTA each (64^3 x 8192: 84 vs 75
-    // with two epilogue groups; BF16 64^3 x 4096: 30.8 vs 31.7 us with four).
+    // (measured on B200: 128^3 x 592 121 vs 105 TFLOP/s, x 8192 190 vs 150),
+    // and for 16-32 KB when it runs two MMA issuers (an even number of
+    // accumulators; the six slots it gets are even): BF16 64^3 x 4096 28.7
+    // against 31.6 us one CTA per problem, FP16 64^3 x 8192 with FP32 C 51.3
+    // against 52.2 us (with one issuer 32.6 and 55.3).
     const int stage_bytes = s.nkb * (s.bm + s.bn) * 128;
-    if (s.part == KAMI_PARTITION_1D && !s.a_tmem && g.num_iter <= 4 && stage_bytes >= 32768 &&
+    if (s.part == KAMI_PARTITION_1D && !s.a_tmem && g.num_iter <= 4 && stage_bytes >= 16384 &&
         2 * stage_bytes <= 227 * 1024 - 1024 - 512 - 8 * kEpiTileBytes)
-        return stream_launch(ma, mb, p, bf16, stream);
+    {
+        const bool small = stage_bytes < 32768;
+        st = stream_launch(ma, mb, p, bf16, stream, small);
+        if (!small || st != KAMI_ERR_UNSUPPORTED)
+            return st;
+    }
 
     // bulk C stores staged in the operand tiles and transpose tiles (dead
     // after the MMAs): as many boxes per warp as they hold, up to all of them

@@ -158,14 +158,18 @@ def test_tc05_a_in_tmem_num_iter(cuda):
 @pytest.mark.parametrize("odt", [torch.float32, torch.float16, torch.bfloat16])
 @pytest.mark.parametrize("M,N,K,batch", [(128, 128, 128, 600), (100, 128, 128, 300), (128, 120, 128, 300),
                                          (128, 192, 64, 200), (128, 96, 128, 300), (128, 100, 128, 150),
-                                         (128, 128, 128, 1), (64, 128, 256, 300)])
+                                         (128, 128, 128, 1), (64, 128, 256, 300), (64, 64, 64, 1000),
+                                         (128, 64, 64, 500), (64, 128, 64, 500), (56, 64, 64, 333),
+                                         (128, 96, 64, 300), (128, 112, 64, 300)])
 def test_tc05_streamed_store_paths(cuda, odt, M, N, K, batch):
-    """The persistent streaming form (problems of at least 32 KB of operands)
-    over its two C paths: bulk tensor stores of 128-byte boxes when C rows
-    and problems are 16-byte aligned and the padded N is a whole number of
-    boxes, per-thread stores otherwise (here N = 100 with 16-bit C, N = 96
-    with 16-bit C).  C is a column slice of a wider buffer, so rows are
-    padded: the padding must stay untouched and row tails clipped."""
+    """The persistent streaming form (problems of at least 32 KB of operands,
+    and 16-32 KB ones with two MMA issuers: 64^3, 128 x 64 x 64, 64 x 128 x
+    64; 128 x 96 and 128 x 112 fall back to one CTA per problem) over its two
+    C paths: bulk tensor stores of 128-byte boxes when C rows and problems
+    are 16-byte aligned and the padded N is a whole number of boxes,
+    per-thread stores otherwise (here N = 100 with 16-bit C, N = 96 with
+    16-bit C).  C is a column slice of a wider buffer, so rows are padded:
+    the padding must stay untouched and row tails clipped."""
     rng = np.random.default_rng(M * N + K + batch)
     A64 = rng.integers(-2, 3, (batch, M, K)).astype(np.float64)
     B64 = rng.integers(-2, 3, (batch, N, K)).astype(np.float64)
@@ -186,14 +190,16 @@ def test_tc05_streamed_store_paths(cuda, odt, M, N, K, batch):
 
 
 @pytest.mark.parametrize("odt", [torch.float32, torch.float16, torch.bfloat16])
-@pytest.mark.parametrize("M,N,K,num_iter,part,P", [(128, 64, 64, 1, "1d", 0), (100, 64, 64, 1, "1d", 0),
-                                                   (128, 96, 64, 1, "1d", 0), (64, 128, 64, 1, "1d", 0),
-                                                   (50, 120, 32, 1, "1d", 0), (128, 128, 128, 8, "1d", 0),
+@pytest.mark.parametrize("M,N,K,num_iter,part,P", [(128, 64, 64, 5, "1d", 0), (100, 64, 64, 5, "1d", 0),
+                                                   (128, 96, 64, 1, "1d", 0), (64, 128, 64, 5, "1d", 0),
+                                                   (50, 120, 32, 5, "1d", 0), (64, 48, 64, 1, "1d", 0),
+                                                   (128, 128, 128, 8, "1d", 0),
                                                    (128, 128, 128, 1, "2d", 2), (128, 128, 64, 1, "3d", 2),
                                                    (64, 64, 64, 1, "3d", 4)])
 def test_tc05_per_problem_store_paths(cuda, odt, M, N, K, num_iter, part, P):
-    """The one-CTA-per-problem form (problems under 32 KB of operands, the
-    repeated-product mode and the 2D / 3D mappings) over its two C paths:
+    """The one-CTA-per-problem form (problems under 16 KB of operands or
+    without a two-issuer streaming layout, the repeated-product mode beyond 4
+    repeats, the 2D / 3D mappings) over its two C paths:
     bulk tensor stores staged in the dead operand tiles, or per-thread
     stores.  C rows are padded; the padding must stay untouched."""
     batch = 37
@@ -210,3 +216,23 @@ def test_tc05_per_problem_store_paths(cuda, odt, M, N, K, num_iter, part, P):
     ref = oracle.gemm(A64, B64) * num_iter
     assert np.array_equal(C.double().cpu().numpy(), torch.tensor(ref).to(odt).double().numpy())
     assert bool((big[:, :, N:] == 7.0).all())
+
+
+@pytest.mark.parametrize("M,N,K", [(64, 256, 64), (128, 192, 64), (64, 64, 64), (128, 160, 64)])
+def test_tc05_streamed_alpha_beta_many_per_cta(cuda, M, N, K):
+    """alpha / beta (per-thread stores) with many problems per CTA in the
+    streaming form, where wide N leaves few TMEM accumulators (2 for N >
+    170): every epilogue group must drain an accumulator only after the
+    product it waits for is complete."""
+    batch = 900
+    rng = np.random.default_rng(N + K)
+    A64 = rng.integers(-2, 3, (batch, M, K)).astype(np.float64)
+    B64 = rng.integers(-2, 3, (batch, N, K)).astype(np.float64)
+    C64 = rng.integers(-3, 4, (batch, M, N)).astype(np.float64)
+    A = torch.tensor(A64, dtype=torch.bfloat16).cuda()
+    B = torch.tensor(B64, dtype=torch.bfloat16).cuda()
+    C = torch.tensor(C64, dtype=torch.float32).cuda()
+    api.gemm_batched(A, B, C, variant="tcgen05", alpha=2.0, beta=-1.0)
+    torch.cuda.synchronize()
+    _status_clean()
+    assert np.array_equal(C.double().cpu().numpy(), 2 * oracle.gemm(A64, B64) - C64)
