@@ -105,10 +105,18 @@ def bmm_forward(A: torch.Tensor, B: torch.Tensor) -> torch.Tensor:
     returned in the input dtype: kami_gemm_batched with B as the K x N
     operand and the library's kernel choice, with the fewest host steps (the
     forward of the autograd function)."""
+    if A.dim() != 3 or B.dim() != 3:
+        raise ValueError("A and B must be 3-D: [batch, M, K] and [batch, K, N]")
+    if A.dtype != B.dtype or A.dtype not in (torch.float16, torch.bfloat16, torch.float64):
+        raise TypeError("A and B must both be float16, bfloat16 or float64")
+    if not (A.is_contiguous() and B.is_contiguous()):
+        raise ValueError("A and B must be contiguous")
     batch, M, K = A.shape
     N = B.shape[2]
     if B.shape[0] != batch or B.shape[1] != K:
         raise ValueError("shapes do not match C = A @ B")
+    if not (A.is_cuda and B.is_cuda):
+        raise ValueError("A and B must be CUDA tensors")
     dt = _DT[A.dtype]
     C = torch.empty((batch, M, N), dtype=A.dtype, device=A.device)
     check(load().kami_gemm_batched(dt, dt, _lib.PARTITION_AUTO, _lib.VARIANT_AUTO, M, N, K, 0, 0, batch,

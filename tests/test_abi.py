@@ -120,3 +120,24 @@ def test_bsr_to_tilebsr_host_conversion():
     assert perm.tolist() == [0, 1, 2, 3, 4]
     with pytest.raises(Exception):
         api.bsr_to_tilebsr(rp, ci, 4, 3, 2)
+
+
+@pytest.mark.parametrize("case", ["dims", "dtype", "mixed", "strided", "shape", "host"])
+def test_bmm_forward_argument_checks(case):
+    """api.bmm_forward (the autograd forward's launch) rejects what it cannot
+    pass to kami_gemm_batched unchanged -- before any device work."""
+    import torch
+    A = torch.zeros((2, 8, 16), dtype=torch.float16)
+    B = torch.zeros((2, 16, 8), dtype=torch.float16)
+    if case == "dims":
+        A = A[0]
+    elif case == "dtype":
+        A, B = A.float(), B.float()
+    elif case == "mixed":
+        B = B.bfloat16()
+    elif case == "strided":
+        A = torch.zeros((2, 16, 8), dtype=torch.float16).transpose(1, 2)
+    elif case == "shape":
+        B = torch.zeros((2, 12, 8), dtype=torch.float16)
+    with pytest.raises((ValueError, TypeError)):
+        api.bmm_forward(A, B)
