@@ -141,3 +141,43 @@ def test_bmm_forward_argument_checks(case):
         B = torch.zeros((2, 12, 8), dtype=torch.float16)
     with pytest.raises((ValueError, TypeError)):
         api.bmm_forward(A, B)
+
+
+@pytest.mark.parametrize("kw,status", [
+    (dict(in_type=_lib.F32), -1),                         # FP32 inputs have no kernel
+    (dict(out_type=_lib.F64), -2),                        # FP64 out only for FP64 in
+    (dict(in_type=_lib.F64, out_type=_lib.F32), -2),
+    (dict(M=0), -1),
+    (dict(batch=-1), -1),
+    (dict(A=None), -1),
+    (dict(dC=None), -1),
+    (dict(dA=None, dB=None), 0),                          # nothing asked: no work, no device call
+    (dict(batch=0), 0),
+])
+def test_backward_host_validation(kw, status):
+    """kami_gemm_backward_batched checks its request on the host before any
+    device work (these calls need no GPU)."""
+    a = dict(in_type=_lib.BF16, out_type=_lib.BF16, M=64, N=64, K=64, batch=4, A=16, B=16, dC=16, dA=16, dB=16)
+    a.update(kw)
+    st = _lib.load().kami_gemm_backward_batched(a["in_type"], a["out_type"], a["M"], a["N"], a["K"], a["batch"],
+                                                a["A"], a["B"], a["dC"], a["dA"], a["dB"], None)
+    assert st == status
+    if status:
+        assert _lib.load().kami_last_error_string()
+
+
+@pytest.mark.parametrize("kw,status", [
+    (dict(M=0), -1),
+    (dict(batch=-1), -1),
+    (dict(it=0), -1),
+    (dict(A=None), -1),
+    (dict(batch=0), 0),
+])
+def test_host_buffer_gemm_validation(kw, status):
+    """kami_gemm_batched_host rejects bad requests before touching the device;
+    an empty batch is a no-op."""
+    a = dict(M=64, N=64, K=64, batch=4, A=16, B=16, C=16, it=1)
+    a.update(kw)
+    st = _lib.load().kami_gemm_batched_host(_lib.F16, _lib.F32, 0, 0, a["M"], a["N"], a["K"], a["batch"], a["A"],
+                                            a["B"], a["C"], a["it"], None, 0, None)
+    assert st == status
