@@ -1,4 +1,4 @@
-"""Model check of the streaming tcgen05 kernel's barrier protocol (CPU).
+"""Model check of the persistent tcgen05 kernels' barrier protocols (CPU).
 
 tc05_stream_kernel (kami_b200/csrc/tc05_gemm.cu) runs one producer thread,
 one or two MMA-issuing threads and G epilogue groups over a ring of S
@@ -15,7 +15,8 @@ advancing in random order) with that parity rule, and checks that no wait
 ever passes before the phase the waiter needs has completed -- for every
 (S, NA, G, I) the launcher chooses over the shapes it admits.  It also shows
 that the two forms the launcher avoids do violate it: two issuers sharing an
-odd number of slots, and more epilogue groups than accumulators.
+odd number of slots, and more epilogue groups than accumulators.  The same
+check covers the grouped kernel (grouped_tc05.cu), whose slots hold K chunks.
 """
 import random
 
@@ -104,7 +105,6 @@ def simulate(S, NA, G, I, nprob, rng):
     grp_j = list(range(G))
     grp_busy = [0] * G
     acc_holds = [None] * NA           # problem whose product is complete in acc b
-    acc_pending = {}                  # b -> problem issued into it, not complete
 
     def need_phase_done(bar, k, who):
         # the wait for phase k passes now; it is correct only if k < bar.phase
@@ -144,7 +144,6 @@ def simulate(S, NA, G, I, nprob, rng):
                     need_phase_done(tempty[b], j // NA - 1, ("issuer acc", j))
                 done = max(now, iss_last_done[t]) + rng.randint(1, 30)   # in order per issuer
                 iss_last_done[t] = done
-                acc_pending[b] = j
                 events.append((done, "mma", (st, b, j)))
                 iss_j[t] += I
                 progressed = True
@@ -211,3 +210,111 @@ def test_avoided_forms_do_pass_waits_early(cfg):
     rng = random.Random(7)
     found = any(simulate(S, NA, G, I, 48, rng) for _ in range(40))
     assert found, cfg
+
+
+def simulate_grouped(S, NA, G, chunks, rng, acc_wait=True):
+    """grouped_tc05_kernel (kami_b200/csrc/grouped_tc05.cu): loaders fill slot
+    c % S for chunk c (problems take 1-2 K chunks of 64), one issuer consumes
+    the chunks in order (freeing each slot with a commit) and, after a
+    problem's last chunk, publishes accumulator p % NA; epilogue group p % G
+    drains it.  `acc_wait` False drops the issuer's wait for a free
+    accumulator (shown to break).  Returns the violations."""
+    nchunk = sum(chunks)
+    owner = [p for p, n in enumerate(chunks) for _ in range(n)]
+    last = {c for c in range(nchunk) if c + 1 == nchunk or owner[c + 1] != owner[c]}
+    full = [Barrier(1) for _ in range(S)]
+    empty = [Barrier(1) for _ in range(S)]
+    accf = [Barrier(1) for _ in range(NA)]
+    acce = [Barrier(1) for _ in range(NA)]
+    bad, events = [], []
+    now, lc, ic, iss_done = 0, 0, 0, 0
+    started = set()
+    grp_p = list(range(G))
+    grp_busy = [0] * G
+    acc_holds = [None] * NA
+    nprob = len(chunks)
+    for _ in range(400000):
+        progressed = False
+        order = ["load", "iss"] + [("grp", g) for g in range(G)]
+        rng.shuffle(order)
+        for role in order:
+            if role == "load" and lc < nchunk:
+                s = lc % S
+                if lc >= S:
+                    if not empty[s].passes(((lc // S) - 1) & 1):
+                        continue
+                    if lc // S - 1 >= empty[s].phase:
+                        bad.append(("loader", lc))
+                events.append((now + rng.randint(1, 40), "load", s))
+                lc += 1
+                progressed = True
+            elif role == "iss" and ic < nchunk:
+                p, s, b = owner[ic], ic % S, owner[ic] % NA
+                if p not in started:
+                    if acc_wait and p >= NA:
+                        if not acce[b].passes(((p // NA) - 1) & 1):
+                            continue
+                        if p // NA - 1 >= acce[b].phase:
+                            bad.append(("issuer acc", p))
+                    elif not acc_wait and acc_holds[b] is not None and acc_holds[b] != "drained" and p >= NA:
+                        bad.append(("issuer overwrites an undrained accumulator", p))
+                if not full[s].passes((ic // S) & 1):
+                    continue
+                if ic // S >= full[s].phase:
+                    bad.append(("issuer full", ic))
+                started.add(p)
+                iss_done = max(now, iss_done) + rng.randint(1, 30)
+                events.append((iss_done, "mma", (s, b, p, ic in last)))
+                ic += 1
+                progressed = True
+            elif isinstance(role, tuple):
+                g = role[1]
+                p = grp_p[g]
+                if p >= nprob or grp_busy[g] > now:
+                    continue
+                b = p % NA
+                if not accf[b].passes((p // NA) & 1):
+                    continue
+                if p // NA >= accf[b].phase:
+                    bad.append(("epilogue", p))
+                if acc_holds[b] != p:
+                    bad.append(("epilogue reads a product it does not own", p, acc_holds[b]))
+                grp_busy[g] = now + rng.randint(1, 50)
+                events.append((grp_busy[g], "drain", b))
+                grp_p[g] += G
+                progressed = True
+        if not progressed:
+            if not events:
+                break
+            events.sort(key=lambda e: e[0])
+            t0, kind, x = events.pop(0)
+            now = max(now, t0)
+            if kind == "load":
+                full[x].arrive()
+            elif kind == "mma":
+                s, b, p, is_last = x
+                empty[s].arrive()
+                if is_last:
+                    acc_holds[b] = p
+                    accf[b].arrive()
+            else:
+                acc_holds[x] = "drained"
+                acce[x].arrive()
+    if not bad and (ic < nchunk or any(p < nprob for p in grp_p)):
+        bad.append(("stalled", ic, grp_p))
+    return bad
+
+
+def test_grouped_kernel_protocol():
+    """The grouped kernel's constants (6 slots, 4 accumulators, 2 epilogue
+    groups, one issuer) never pass a wait early over random chunk mixes."""
+    rng = random.Random(11)
+    for _ in range(60):
+        chunks = [rng.choice((1, 1, 1, 2)) for _ in range(rng.randint(1, 50))]
+        assert simulate_grouped(6, 4, 2, chunks, rng) == []
+
+
+def test_grouped_kernel_needs_its_accumulator_wait():
+    rng = random.Random(3)
+    chunks = [1] * 40
+    assert any(simulate_grouped(6, 4, 2, chunks, rng, acc_wait=False) for _ in range(30))
