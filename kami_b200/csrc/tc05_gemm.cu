@@ -396,7 +396,8 @@ __global__ void __launch_bounds__(128) tc05_block_kernel(const __grid_constant__
 //                      phase two ahead of the last one completed, which
 //                      parity-based waits cannot tell apart);
 //   warps 2..          epilogue, `groups` groups of four (two, or four when
-//                      shared memory leaves room for their transpose tiles):
+//                      shared memory leaves room for their transpose tiles
+//                      and naccs >= 4 -- never more groups than accumulators):
 //                      group g drains the accumulator of every problem j with
 //                      j % groups == g (tcgen05.ld of its TMEM lane quadrant,
 //                      coalesced C stores), then releases it -- the epilogue
@@ -968,7 +969,10 @@ static bool make_c_map(CUtensorMap *map, const GemmArgs &g, int bn, int box_rows
 // columns hold (at most 8).  With bulk tensor stores: two epilogue groups,
 // two staging boxes per warp when three slots still fit beside them (else
 // one).  Otherwise four epilogue groups when at least three slots still fit
-// beside their transpose tiles (else two).
+// beside their transpose tiles and there are at least four accumulators
+// (else two).  A second MMA issuer for problems under 32 KB when slots and
+// accumulators are both even; need_two: launch nothing (KAMI_ERR_UNSUPPORTED,
+// no message) when that layout is not possible.
 static int stream_launch(CUtensorMap &ma, CUtensorMap &mb, Tc05Params &p, bool bf16, cudaStream_t stream,
                          bool need_two)
 {
