@@ -296,7 +296,8 @@ def run_ours(args, rank, world):
     if rank != 0:
         return
     peak_tf, peak_bw, src = measured_peaks()
-    achieved = flops_rank / (min(ms) * 1e-3) / 1e12
+    # the same statistic as `value`: mean device time of the timed launches
+    achieved = flops_rank / (statistics.fmean(ms) * 1e-3) / 1e12
     roof = {"bound": "tensor", "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s",
             "frac": achieved / peak_tf, "peak_source": f"{src} bf16 dense (burst)",
             "traffic": ncu_traffic(f"gemm_{plan['variant']}_{M}"),

@@ -287,21 +287,22 @@ int kami_gemm_grouped_plan_destroy(kami_grouped_plan *plan);
 /*
  * Allocation-free grouped GEMM (no counterpart in the reference).  The same
  * computation as kami_gemm_grouped_plan_create + kami_gemm_grouped_run, for
- * callers that may not allocate device memory: code that runs while a CUDA
- * graph is being captured, processes whose allocator forbids cudaMalloc
- * after start-up, and embedded or real-time hosts that preallocate
- * everything.  Instead of a plan in cudaMalloc'd memory it uses one fixed
- * device array owned by the library (room for KAMI_NOALLOC_MAX_PROBLEMS
- * problem descriptors plus the CTA schedule, about 0.45 MB, resident on every
- * GPU that loads the library until the process exits).  Each call rebuilds
- * the schedule on the host, copies it into that array with cudaMemcpyAsync
- * on `stream` and launches the grouped kernel; it calls no cudaMalloc or
- * cudaFree.  The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress) and sets the kernel's attributes, so make that first
- * call before any stream capture.  Requests with more than
+ * callers that cannot allocate device memory: hosts whose own allocator
+ * carves up device memory once at start-up and treats any later cudaMalloc
+ * as a fault (serving processes, real-time and embedded controllers), and
+ * plug-ins running inside such hosts.  Instead of a plan in cudaMalloc'd
+ * memory it uses one fixed device array owned by the library (room for
+ * KAMI_NOALLOC_MAX_PROBLEMS problem descriptors plus the CTA schedule, about
+ * 0.45 MB, resident on every GPU that loads the library until the process
+ * exits).  Each call rebuilds the schedule on the host, copies it into that
+ * array with cudaMemcpyAsync on `stream` and launches the mma.sync grouped
+ * kernel; it calls no cudaMalloc or cudaFree.  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress, with that
+ * device current) and sets the kernel's attributes.  Requests with more than
  * KAMI_NOALLOC_MAX_PROBLEMS problems are rejected with KAMI_ERR_UNSUPPORTED.
- * All calls share the array, which keeps the last call's contents: calls
- * whose work overlaps on the GPU (other streams, other host threads) race.
+ * All calls share the array, which keeps the last call's contents: calls on
+ * one stream are ordered and safe, calls on different streams (or host
+ * threads using different streams) whose work overlaps on the GPU race.
  * Partitions come from the static cost model (autotuning would allocate).
  * Argument meaning as in kami_gemm_grouped_plan_create / _run.
  */

@@ -37,6 +37,53 @@ def _stream_ptr(stream) -> int:
     return int(s.cuda_stream)
 
 
+def _device_index(*tensors) -> int:
+    """The CUDA device every given tensor lives on (None entries are
+    skipped).  Raises ValueError for a tensor off the GPU or operands on
+    different devices: a kernel launched on one device with another
+    device's pointers would fault or read through peer mappings."""
+    idx = None
+    for t in tensors:
+        if t is None:
+            continue
+        if not t.is_cuda:
+            raise ValueError("operands must be CUDA tensors")
+        d = t.device.index
+        if idx is None:
+            idx = d
+        elif d != idx:
+            raise ValueError(f"operands are on different devices (cuda:{idx} and cuda:{d})")
+    return idx
+
+
+class _OnDevice:
+    """Makes `index` the current device for the duration of a call (so the
+    launch and the default stream belong to the operands' device), at the
+    cost of one device query when it already is."""
+    __slots__ = ("index", "prev")
+
+    def __init__(self, index):
+        self.index = index
+        self.prev = None
+
+    def __enter__(self):
+        if self.index is not None and _cur_device is not None:
+            cur = _cur_device()
+            if cur != self.index:
+                self.prev = cur
+                torch.cuda.set_device(self.index)
+        return self
+
+    def __exit__(self, *exc):
+        if self.prev is not None:
+            torch.cuda.set_device(self.prev)
+        return False
+
+
+def _on(*tensors) -> _OnDevice:
+    return _OnDevice(_device_index(*tensors))
+
+
 def _as3(x: torch.Tensor) -> torch.Tensor:
     return x.unsqueeze(0) if x.dim() == 2 else x
 
@@ -71,8 +118,7 @@ def gemm_batched(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = None
     A3, B3 = _as3(A), _as3(B)
     if A3.dtype != B3.dtype:
         raise TypeError("A and B must have the same dtype")
-    if not (A3.is_cuda and B3.is_cuda):
-        raise ValueError("A and B must be CUDA tensors")
+    dev = _on(A3, B3, C)
     _check_inner(A3, "A")
     _check_inner(B3, "B")
     batch = A3.shape[0]
@@ -87,12 +133,13 @@ def gemm_batched(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = None
     else:
         C3 = _as3(C)
         _check_inner(C3, "C")
-    st = load().kami_gemm_batched(
-        _DT[A3.dtype], _DT[C3.dtype], _PART[partition], _VAR[variant], M, N, K, P, alloc_warps, batch,
-        A3.data_ptr(), _ld(A3), _bs(A3), _AL[a_layout],
-        B3.data_ptr(), _ld(B3), _bs(B3), _BL[b_layout],
-        C3.data_ptr(), _ld(C3), _bs(C3),
-        float(alpha), float(beta), int(num_iter), None, 0, _stream_ptr(stream))
+    with dev:
+        st = load().kami_gemm_batched(
+            _DT[A3.dtype], _DT[C3.dtype], _PART[partition], _VAR[variant], M, N, K, P, alloc_warps, batch,
+            A3.data_ptr(), _ld(A3), _bs(A3), _AL[a_layout],
+            B3.data_ptr(), _ld(B3), _bs(B3), _BL[b_layout],
+            C3.data_ptr(), _ld(C3), _bs(C3),
+            float(alpha), float(beta), int(num_iter), None, 0, _stream_ptr(stream))
     check(st)
     if C is not None:
         return C
@@ -115,13 +162,14 @@ def bmm_forward(A: torch.Tensor, B: torch.Tensor) -> torch.Tensor:
     N = B.shape[2]
     if B.shape[0] != batch or B.shape[1] != K:
         raise ValueError("shapes do not match C = A @ B")
-    if not (A.is_cuda and B.is_cuda):
-        raise ValueError("A and B must be CUDA tensors")
+    dev = _on(A, B)
     dt = _DT[A.dtype]
     C = torch.empty((batch, M, N), dtype=A.dtype, device=A.device)
-    check(load().kami_gemm_batched(dt, dt, _lib.PARTITION_AUTO, _lib.VARIANT_AUTO, M, N, K, 0, 0, batch,
-                                   A.data_ptr(), K, M * K, _lib.A_ROW_MK, B.data_ptr(), N, K * N, _lib.B_ROW_KN,
-                                   C.data_ptr(), N, M * N, 1.0, 0.0, 1, None, 0, _stream_ptr(None)))
+    with dev:
+        st = load().kami_gemm_batched(dt, dt, _lib.PARTITION_AUTO, _lib.VARIANT_AUTO, M, N, K, 0, 0, batch,
+                                      A.data_ptr(), K, M * K, _lib.A_ROW_MK, B.data_ptr(), N, K * N, _lib.B_ROW_KN,
+                                      C.data_ptr(), N, M * N, 1.0, 0.0, 1, None, 0, _stream_ptr(None))
+    check(st)
     return C
 
 
@@ -157,12 +205,15 @@ def gemm_backward(A: torch.Tensor, B: torch.Tensor, dC: torch.Tensor, *, need_dA
     N = B3.shape[2]
     if B3.shape[1] != K or G3.shape[1:] != (M, N) or B3.shape[0] != batch or G3.shape[0] != batch:
         raise ValueError("shapes do not match C = A @ B")
+    dev = _on(A3, B3, G3)
     odt = out_dtype or A3.dtype
     dA = torch.empty((batch, M, K), dtype=odt, device=A3.device) if need_dA else None
     dB = torch.empty((batch, K, N), dtype=odt, device=A3.device) if need_dB else None
-    check(load().kami_gemm_backward_batched(_DT[A3.dtype], _DT[odt], M, N, K, batch, A3.data_ptr(), B3.data_ptr(),
-                                            G3.data_ptr(), dA.data_ptr() if dA is not None else None,
-                                            dB.data_ptr() if dB is not None else None, _stream_ptr(stream)))
+    with dev:
+        st = load().kami_gemm_backward_batched(_DT[A3.dtype], _DT[odt], M, N, K, batch, A3.data_ptr(),
+                                               B3.data_ptr(), G3.data_ptr(), dA.data_ptr() if dA is not None else None,
+                                               dB.data_ptr() if dB is not None else None, _stream_ptr(stream))
+    check(st)
     if A.dim() == 2:
         dA = dA[0] if dA is not None else None
         dB = dB[0] if dB is not None else None
@@ -189,10 +240,12 @@ def gemm_batched_ksplit(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None
         C3 = _as3(C)
         _check_inner(C3, "C")
     used = ctypes.c_int(-2)
-    check(load().kami_gemm_batched_ksplit(_DT[A3.dtype], _DT[C3.dtype], M, N, K, P, batch,
-                                          A3.data_ptr(), _ld(A3), _bs(A3), B3.data_ptr(), _ld(B3), _bs(B3),
-                                          C3.data_ptr(), _ld(C3), _bs(C3), float(alpha), float(beta), int(num_iter),
-                                          int(reg_k_steps), ctypes.byref(used), _stream_ptr(stream)))
+    with _on(A3, B3, C3):
+        st = load().kami_gemm_batched_ksplit(_DT[A3.dtype], _DT[C3.dtype], M, N, K, P, batch,
+                                             A3.data_ptr(), _ld(A3), _bs(A3), B3.data_ptr(), _ld(B3), _bs(B3),
+                                             C3.data_ptr(), _ld(C3), _bs(C3), float(alpha), float(beta),
+                                             int(num_iter), int(reg_k_steps), ctypes.byref(used), _stream_ptr(stream))
+    check(st)
     out = C if C is not None else (C3[0] if A.dim() == 2 else C3)
     return out, used.value
 
@@ -211,8 +264,10 @@ def gemm_trace(A: torch.Tensor, B: torch.Tensor, *, partition: str = "1d", P: in
     C = torch.empty((M, N), dtype=torch.float32, device=A.device)
     cyc = torch.zeros(64, dtype=torch.int64, device=A.device)
     nw = ctypes.c_int(0)
-    check(load().kami_gemm_trace(_PART[partition], M, N, K, P, reg_k_steps, A.data_ptr(), B.data_ptr(),
-                                 C.data_ptr(), int(num_iter), cyc.data_ptr(), ctypes.byref(nw), _stream_ptr(stream)))
+    with _on(A, B):
+        st = load().kami_gemm_trace(_PART[partition], M, N, K, P, reg_k_steps, A.data_ptr(), B.data_ptr(),
+                                    C.data_ptr(), int(num_iter), cyc.data_ptr(), ctypes.byref(nw), _stream_ptr(stream))
+    check(st)
     return C, cyc.cpu().numpy()[: 2 * nw.value].reshape(nw.value, 2)
 
 
@@ -255,6 +310,8 @@ class GroupedPlan:
             self.sizes = (int(a[-1]), int(b[-1]), int(c[-1]))
         ao, bo, co = (np.ascontiguousarray(o, dtype=np.int64) for o in offsets)
         self.shapes, self.offsets = sh, (ao, bo, co)
+        # the plan's descriptors live on the device current at creation
+        self.device_index = _cur_device() if _cur_device is not None and torch.cuda.is_available() else None
         h = ctypes.c_void_p()
         check(load().kami_gemm_grouped_plan_create(_DT[dtype], _DT[self.out_dtype], self.count,
                                                    M.ctypes.data, N.ctypes.data, K.ctypes.data, ao.ctypes.data,
@@ -273,8 +330,13 @@ class GroupedPlan:
 
     def run(self, A: torch.Tensor, B: torch.Tensor, C: torch.Tensor, *, alpha=1.0, beta=0.0, num_iter=1,
             stream=None) -> torch.Tensor:
-        check(load().kami_gemm_grouped_run(self._h, A.data_ptr(), B.data_ptr(), C.data_ptr(), float(alpha),
-                                           float(beta), int(num_iter), _stream_ptr(stream)))
+        idx = _device_index(A, B, C)
+        if self.device_index is not None and idx != self.device_index:
+            raise ValueError(f"the plan was built on cuda:{self.device_index}, the operands are on cuda:{idx}")
+        with _OnDevice(idx):
+            st = load().kami_gemm_grouped_run(self._h, A.data_ptr(), B.data_ptr(), C.data_ptr(), float(alpha),
+                                              float(beta), int(num_iter), _stream_ptr(stream))
+        check(st)
         return C
 
     def __del__(self):
@@ -304,11 +366,13 @@ def split_f64_gemm(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = No
     batch, M, K = A3.shape
     N = B3.shape[1] if b_layout == "ref_nk" else B3.shape[2]
     C3 = torch.empty((batch, M, N), dtype=torch.float64, device=A3.device) if C is None else _as3(C)
-    check(load().kami_split_f64_gemm_batched(
-        int(nslices), _lib.S8 if slice_dtype == torch.int8 else _DT[slice_dtype], M, N, K, batch,
-        A3.data_ptr(), _ld(A3), _bs(A3),
-        B3.data_ptr(), _ld(B3), _bs(B3), _BL[b_layout], C3.data_ptr(), _ld(C3), _bs(C3),
-        float(alpha), float(beta), int(num_iter), _stream_ptr(stream)))
+    with _on(A3, B3, C3):
+        st = load().kami_split_f64_gemm_batched(
+            int(nslices), _lib.S8 if slice_dtype == torch.int8 else _DT[slice_dtype], M, N, K, batch,
+            A3.data_ptr(), _ld(A3), _bs(A3),
+            B3.data_ptr(), _ld(B3), _bs(B3), _BL[b_layout], C3.data_ptr(), _ld(C3), _bs(C3),
+            float(alpha), float(beta), int(num_iter), _stream_ptr(stream))
+    check(st)
     if C is not None:
         return C
     return C3[0] if squeeze else C3
@@ -337,17 +401,21 @@ def spgemm_symbolic(A: BSR, B: BSR, stream=None):
         raise ValueError("inner block dimensions differ")
     rpc = torch.empty(A.block_rows + 1, dtype=torch.int32, device=A.row_ptr.device)
     nnz = ctypes.c_int(0)
-    check(load().kami_spgemm_bsr_symbolic(16, A.block_rows, A.block_cols, B.block_cols, A.row_ptr.data_ptr(),
-                                          _ptr(A.col_idx), B.row_ptr.data_ptr(), _ptr(B.col_idx),
-                                          rpc.data_ptr(), ctypes.byref(nnz), _stream_ptr(stream)))
+    with _on(*_bsr_tensors(A, B)):
+        st = load().kami_spgemm_bsr_symbolic(16, A.block_rows, A.block_cols, B.block_cols, A.row_ptr.data_ptr(),
+                                             _ptr(A.col_idx), B.row_ptr.data_ptr(), _ptr(B.col_idx),
+                                             rpc.data_ptr(), ctypes.byref(nnz), _stream_ptr(stream))
+    check(st)
     return rpc, nnz.value
 
 
 def spgemm_fill_colidx(A: BSR, B: BSR, row_ptr_c: torch.Tensor, nnz_c: int, stream=None) -> torch.Tensor:
     cic = torch.empty(max(nnz_c, 1), dtype=torch.int32, device=A.row_ptr.device)
-    check(load().kami_spgemm_bsr_fill_colidx(16, A.block_rows, A.block_cols, B.block_cols, A.row_ptr.data_ptr(),
-                                             _ptr(A.col_idx), B.row_ptr.data_ptr(), _ptr(B.col_idx),
-                                             row_ptr_c.data_ptr(), cic.data_ptr(), _stream_ptr(stream)))
+    with _on(*_bsr_tensors(A, B), row_ptr_c):
+        st = load().kami_spgemm_bsr_fill_colidx(16, A.block_rows, A.block_cols, B.block_cols, A.row_ptr.data_ptr(),
+                                                _ptr(A.col_idx), B.row_ptr.data_ptr(), _ptr(B.col_idx),
+                                                row_ptr_c.data_ptr(), cic.data_ptr(), _stream_ptr(stream))
+    check(st)
     return cic[:nnz_c]
 
 
@@ -356,11 +424,13 @@ def spgemm_numeric(A: BSR, B: BSR, row_ptr_c, col_idx_c, out_dtype=torch.float32
     nnz_c = col_idx_c.numel()
     if C_values is None:
         C_values = torch.empty((max(nnz_c, 1), 16, 16), dtype=out_dtype, device=A.row_ptr.device)
-    check(load().kami_spgemm_bsr_numeric(_DT[A.values.dtype], _DT[C_values.dtype], 16, A.block_rows, A.block_cols,
-                                         B.block_cols, A.row_ptr.data_ptr(), _ptr(A.col_idx), _ptr(A.values),
-                                         B.row_ptr.data_ptr(), _ptr(B.col_idx), _ptr(B.values),
-                                         row_ptr_c.data_ptr(), _ptr(col_idx_c), _ptr(C_values), nnz_c,
-                                         float(alpha), float(beta), int(num_iter), _stream_ptr(stream)))
+    with _on(*_bsr_tensors(A, B), row_ptr_c, col_idx_c, C_values):
+        st = load().kami_spgemm_bsr_numeric(_DT[A.values.dtype], _DT[C_values.dtype], 16, A.block_rows,
+                                            A.block_cols, B.block_cols, A.row_ptr.data_ptr(), _ptr(A.col_idx),
+                                            _ptr(A.values), B.row_ptr.data_ptr(), _ptr(B.col_idx), _ptr(B.values),
+                                            row_ptr_c.data_ptr(), _ptr(col_idx_c), _ptr(C_values), nnz_c,
+                                            float(alpha), float(beta), int(num_iter), _stream_ptr(stream))
+    check(st)
     return C_values[:nnz_c]
 
 
@@ -372,9 +442,12 @@ def spgemm_symbolic_device(A: BSR, B: BSR, capacity: int, stream=None):
     dev = A.row_ptr.device
     rpc = torch.empty(A.block_rows + 1, dtype=torch.int32, device=dev)
     cic = torch.empty(max(int(capacity), 1), dtype=torch.int32, device=dev)
-    check(load().kami_spgemm_bsr_symbolic_device(16, A.block_rows, A.block_cols, B.block_cols, A.row_ptr.data_ptr(),
-                                                 _ptr(A.col_idx), B.row_ptr.data_ptr(), _ptr(B.col_idx),
-                                                 rpc.data_ptr(), cic.data_ptr(), int(capacity), _stream_ptr(stream)))
+    with _on(*_bsr_tensors(A, B)):
+        st = load().kami_spgemm_bsr_symbolic_device(16, A.block_rows, A.block_cols, B.block_cols,
+                                                    A.row_ptr.data_ptr(), _ptr(A.col_idx), B.row_ptr.data_ptr(),
+                                                    _ptr(B.col_idx), rpc.data_ptr(), cic.data_ptr(), int(capacity),
+                                                    _stream_ptr(stream))
+    check(st)
     return rpc, cic
 
 
@@ -383,11 +456,13 @@ def spgemm_numeric_bound(A: BSR, B: BSR, row_ptr_c, col_idx_c, C_values, *, alph
     """Numeric pass into C_values [capacity, 16, 16] with the capacity as the
     bound of nnzC (no host synchronisation)."""
     cap = C_values.shape[0]
-    check(load().kami_spgemm_bsr_numeric(_DT[A.values.dtype], _DT[C_values.dtype], 16, A.block_rows, A.block_cols,
-                                         B.block_cols, A.row_ptr.data_ptr(), _ptr(A.col_idx), _ptr(A.values),
-                                         B.row_ptr.data_ptr(), _ptr(B.col_idx), _ptr(B.values),
-                                         row_ptr_c.data_ptr(), _ptr(col_idx_c), _ptr(C_values), cap,
-                                         float(alpha), float(beta), int(num_iter), _stream_ptr(stream)))
+    with _on(*_bsr_tensors(A, B), row_ptr_c, col_idx_c, C_values):
+        st = load().kami_spgemm_bsr_numeric(_DT[A.values.dtype], _DT[C_values.dtype], 16, A.block_rows,
+                                            A.block_cols, B.block_cols, A.row_ptr.data_ptr(), _ptr(A.col_idx),
+                                            _ptr(A.values), B.row_ptr.data_ptr(), _ptr(B.col_idx), _ptr(B.values),
+                                            row_ptr_c.data_ptr(), _ptr(col_idx_c), _ptr(C_values), cap,
+                                            float(alpha), float(beta), int(num_iter), _stream_ptr(stream))
+    check(st)
     return C_values
 
 
@@ -415,10 +490,12 @@ def spmm(A: BSR, B: torch.Tensor, C: torch.Tensor | None = None, *, b_layout: st
         B = B.contiguous()
     if C is None:
         C = torch.empty((A.block_rows * 16, N), dtype=out_dtype, device=B.device)
-    check(load().kami_spmm_bsr(_DT[A.values.dtype], _DT[C.dtype], 16, A.block_rows, A.block_cols, N, 1,
-                               A.row_ptr.data_ptr(), _ptr(A.col_idx), 0, 0, _ptr(A.values), 0,
-                               B.data_ptr(), _ld(B[None]), 0, _BL[b_layout], C.data_ptr(), _ld(C[None]), 0,
-                               float(alpha), float(beta), int(num_iter), _stream_ptr(stream)))
+    with _on(A.row_ptr, A.col_idx, A.values, B, C):
+        st = load().kami_spmm_bsr(_DT[A.values.dtype], _DT[C.dtype], 16, A.block_rows, A.block_cols, N, 1,
+                                  A.row_ptr.data_ptr(), _ptr(A.col_idx), 0, 0, _ptr(A.values), 0,
+                                  B.data_ptr(), _ld(B[None]), 0, _BL[b_layout], C.data_ptr(), _ld(C[None]), 0,
+                                  float(alpha), float(beta), int(num_iter), _stream_ptr(stream))
+    check(st)
     return C
 
 
@@ -455,14 +532,17 @@ def spmm_batched(row_ptr: torch.Tensor, col_idx: torch.Tensor, values: torch.Ten
     ldc = _ld(C if C.dim() == 3 else C[None])
     ldb = _ld(B if B.dim() == 3 else B[None])
     L = load()
+    dev = _on(row_ptr, col_idx, values, B, C)
     common_tail = (_ptr(values), s_v, B.data_ptr(), ldb, s_b, _BL[b_layout], C.data_ptr(), ldc, s_cc,
                    float(alpha), float(beta), int(num_iter), _stream_ptr(stream))
-    if tile_rows:
-        check(L.kami_spmm_tilebsr(_DT[values.dtype], _DT[C.dtype], 16, mb, block_cols, N, batch, tile_rows,
-                                  tile_cols, row_ptr.data_ptr(), _ptr(col_idx), s_r, s_c, *common_tail))
-    else:
-        check(L.kami_spmm_bsr(_DT[values.dtype], _DT[C.dtype], 16, mb, block_cols, N, batch,
-                              row_ptr.data_ptr(), _ptr(col_idx), s_r, s_c, *common_tail))
+    with dev:
+        if tile_rows:
+            st = L.kami_spmm_tilebsr(_DT[values.dtype], _DT[C.dtype], 16, mb, block_cols, N, batch, tile_rows,
+                                     tile_cols, row_ptr.data_ptr(), _ptr(col_idx), s_r, s_c, *common_tail)
+        else:
+            st = L.kami_spmm_bsr(_DT[values.dtype], _DT[C.dtype], 16, mb, block_cols, N, batch,
+                                 row_ptr.data_ptr(), _ptr(col_idx), s_r, s_c, *common_tail)
+    check(st)
     return C
 
 
@@ -482,6 +562,10 @@ def bsr_to_tilebsr(row_ptr, col_idx, block_cols: int, tile_rows: int, tile_cols:
                                    brp.ctypes.data, bci.ctypes.data, perm.ctypes.data)
     check(n if n < 0 else 0)
     return brp, bci[:n], perm[:n]
+
+
+def _bsr_tensors(*mats):
+    return [t for m in mats for t in (m.row_ptr, m.col_idx, m.values)]
 
 
 def _ptr(t: torch.Tensor) -> int:

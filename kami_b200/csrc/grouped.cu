@@ -1038,20 +1038,22 @@ int kami_gemm_grouped_plan_destroy(kami_grouped_plan *plan) { return free_plan(p
 // ---------------------------------------------------------------------------
 // Allocation-free variant of the grouped launch.
 //
-// Callers that cannot allocate device memory -- code running inside a CUDA
-// graph capture that must not call cudaMalloc, allocators that forbid
-// allocation after start-up, embedded and real-time hosts that preallocate
-// everything -- cannot create a plan, because a plan keeps its problem
-// descriptors and schedule in cudaMalloc'd memory.  This entry point keeps
-// them instead in one fixed array of device memory that belongs to the
-// library (a file-scope __device__ array, KAMI_NOALLOC_MAX_PROBLEMS
-// descriptors plus the CTA schedule, about 0.45 MB on every GPU that loads
-// the library, held until the process exits).  Each call rebuilds the
-// schedule on the host (static staging arrays, no heap), copies it into that
-// array with cudaMemcpyAsync on the caller's stream and launches the same
-// grouped kernel.  Every call shares the array and leaves its own contents
-// behind: calls whose work overlaps on the GPU (different streams, or a
-// second call before the first kernel has read its descriptors) race.
+// Callers that cannot allocate device memory -- hosts whose own allocator
+// carves up device memory once at start-up and treats any later cudaMalloc
+// as a fault (serving processes, real-time and embedded controllers), and
+// plug-ins running inside such hosts -- cannot create a plan, because a plan
+// keeps its problem descriptors and schedule in cudaMalloc'd memory.  This
+// entry point keeps them instead in one fixed array of device memory that
+// belongs to the library (a file-scope __device__ array,
+// KAMI_NOALLOC_MAX_PROBLEMS descriptors plus the CTA schedule, about 0.45 MB
+// on every GPU that loads the library, held until the process exits).  Each
+// call rebuilds the schedule on the host (static staging arrays, no heap),
+// copies it into that array with cudaMemcpyAsync on the caller's stream and
+// launches the mma.sync grouped kernel (warp grids chosen by the static cost
+// model).  Every call shares the array and leaves its own contents behind.
+// Calls on one stream are ordered by that stream and are safe; calls on
+// different streams (or from host threads using different streams) whose
+// work overlaps on the GPU race on the array.
 // ---------------------------------------------------------------------------
 namespace kami {
 namespace {

@@ -35,9 +35,16 @@ def build(force: bool = False) -> None:
         subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 
-def build_reference(ref_root: str = "/root/reference") -> bool:
+def reference_root() -> str:
+    """The reference checkout: $KAMI_REFERENCE_ROOT, else /root/reference."""
+    return os.environ.get("KAMI_REFERENCE_ROOT") or "/root/reference"
+
+
+def build_reference(ref_root: str | None = None) -> bool:
     """Compile the reference pieces into ``oracle/_ref`` when the reference
-    sources are present.  Returns True when the libraries exist afterwards."""
+    sources are present (``ref_root``, default :func:`reference_root`).
+    Returns True when the libraries exist afterwards."""
+    ref_root = ref_root or reference_root()
     if os.path.isdir(ref_root):
         subprocess.run(["make", "-s", "-C", HERE, "-f", "Makefile.ref", "-j8", f"REF={ref_root}"],
                        check=True)

@@ -181,3 +181,32 @@ def test_host_buffer_gemm_validation(kw, status):
     st = _lib.load().kami_gemm_batched_host(_lib.F16, _lib.F32, 0, 0, a["M"], a["N"], a["K"], a["batch"], a["A"],
                                             a["B"], a["C"], a["it"], None, 0, None)
     assert st == status
+
+
+class _FakeCuda:
+    """Stands for a CUDA tensor on a given device (no GPU needed)."""
+
+    def __init__(self, index):
+        import torch
+        self.is_cuda = True
+        self.device = torch.device("cuda", index)
+
+
+def test_operands_on_different_devices_are_rejected():
+    assert api._device_index(_FakeCuda(0), None, _FakeCuda(0)) == 0
+    assert api._device_index(_FakeCuda(3)) == 3
+    with pytest.raises(ValueError, match="different devices"):
+        api._device_index(_FakeCuda(0), _FakeCuda(1))
+    with pytest.raises(ValueError, match="different devices"):
+        api._device_index(_FakeCuda(1), None, _FakeCuda(1), _FakeCuda(0))
+
+
+def test_host_tensors_are_rejected_before_any_launch():
+    import torch
+    A = torch.zeros((2, 16, 16), dtype=torch.float16)
+    with pytest.raises(ValueError, match="CUDA tensors"):
+        api.gemm_batched(A, A)
+    with pytest.raises(ValueError, match="CUDA tensors"):
+        api.split_f64_gemm(A.double(), A.double())
+    with pytest.raises(ValueError, match="CUDA tensors"):
+        api._device_index(_FakeCuda(0), A)
