@@ -480,6 +480,28 @@ def run_secondary(args):
         return
 
     if args.workload == "spgemm":
+        # (a) the reference programs' method: one 128 x 128 BSR pair (8 x 8
+        # tiles, the reference generator at sparsity 0.5, A = B as its
+        # srand(0) reuse gives) per CTA, 16384 CTAs sharing it, NUM_ITER 1000,
+        # FLOPs 2 * 16^3 * nnzCub * grid * NUM_ITER (spgemm/2d/...:763-768, 839-840)
+        rp, ci, vals = oracle.bsr_generate(8, 8, 0.5)
+        rpc_o, cic_o, vc_o = oracle.spgemm(8, 8, (rp, ci, vals), (rp, ci, vals), accum="double")
+        nnzcub_b = oracle.spgemm_nnzcub(ci, rp)
+        Ab = api.BSR(torch.tensor(rp, device=dev), torch.tensor(ci, device=dev), torch.tensor(vals, device=dev), 8)
+        grid_b = 16384
+        for part, P in [("1d", 4), ("1d", 8), ("2d", 2), ("3d", 2)]:
+            for it in (1000,):
+                Cb = api.BSR(torch.tensor(rpc_o, device=dev), torch.tensor(cic_o, device=dev),
+                             torch.empty((grid_b, len(cic_o), 16, 16), dtype=torch.float32, device=dev), 8)
+                ms = _time_ms(lambda: api.spgemm_block(Ab, Ab, Cb, partition=part, P=P, num_iter=it), W, K_, flush)
+                t = statistics.fmean(ms)
+                fl = 2.0 * 16 ** 3 * nnzcub_b * grid_b * it
+                err = float(np.abs(Cb.values[grid_b - 1].double().cpu().numpy() / it - vc_o).max())
+                _emit({"workload": "spgemm", "case": "reference block 128x128, 50 % tiles, 16384 CTAs",
+                       "partition": part, "P": P, "nnzCub": nnzcub_b, "num_iter": it, "ms": t,
+                       "tflops": fl / t / 1e9, "frac_tensor_peak": fl / t / 1e9 / peak_tf,
+                       "max_abs_err_vs_oracle": err})
+                del Cb
         nb = 1024  # n = 16384 with 16 x 16 blocks
         res = []
         for seed_a, seed_b in [(1, 2)]:

@@ -402,6 +402,46 @@ int kami_spgemm_bsr_numeric(kami_dtype_t in_type, kami_dtype_t out_type, int bsr
                             int64_t nnz_c, double alpha, double beta, int num_iter,
                             void *stream);
 
+/* The reference's block SpGEMM method: one CTA multiplies one small BSR
+ * pair (mb, kb, nb <= 16 blocks of 16 x 16, at most 384 A + B tiles) with its
+ * warps owning C tiles by `partition` -- 1D: warp w a range of block-rows;
+ * 2D: warp (r, c) a row range x column range; 3D: warp (r, c, d) the same
+ * C tiles as (r, c) over the d-th range of k, the P partial tiles reduced on
+ * the device -- and repeats the products num_iter times on register-resident
+ * fragments (FP32 accumulation).  Replaces block_spgemm_{1d,2d,3d}_half_mma
+ * (src/sparse/spgemm/1d/block_spgemm_1d_half_mma.cu:107, 2d/...:171,
+ * 3d/...:175; argument order RowPtrA, ColIdxA, ValA, RowPtrB, ColIdxB, ValB,
+ * RowPtrC, ColIdxC, ValC, alpha, beta kept), launched there as 16384 CTAs
+ * on one matrix pair.  `batch` problems share the structure (row_ptr /
+ * col_idx of A, B and C; C's from the symbolic pass) and take tile values at
+ * the given per-problem strides in elements (0 = shared, the reference's
+ * launch).  nnz_a / nnz_b / nnz_c = row_ptr_x[rows] (the caller knows them,
+ * as the reference's host does).  P: 1D 1, 2, 4, 8; 2D 2, 4; 3D 2 (0 =
+ * 4 for 1D, 2 otherwise); partition AUTO = 1D.  Larger matrices:
+ * kami_spgemm_bsr_numeric. */
+int kami_spgemm_bsr_block(kami_dtype_t in_type, kami_dtype_t out_type, kami_partition_t partition, int P, int bsr,
+                          int mb, int kb, int nb, int64_t batch,
+                          const int *row_ptr_a, const int *col_idx_a, const void *val_a, int64_t stride_val_a,
+                          int nnz_a,
+                          const int *row_ptr_b, const int *col_idx_b, const void *val_b, int64_t stride_val_b,
+                          int nnz_b,
+                          const int *row_ptr_c, const int *col_idx_c, void *val_c, int64_t stride_val_c, int nnz_c,
+                          double alpha, double beta, int num_iter, void *stream);
+
+/* kami_spgemm_bsr_numeric with the kernel chosen: KAMI_VARIANT_MMA_SYNC
+ * (one CTA per block-row: A tiles staged, each C tile's products found by
+ * searching its column in the B rows, two m16n8k16 MMAs per product),
+ * KAMI_VARIANT_TCGEN05 (one CTA per SM: the row's products enumerated once
+ * and streamed through a shared-memory ring, one tcgen05.mma of M = 64,
+ * N = 16 per product into the tile's own tensor-memory accumulator; tile
+ * arrays 16-byte aligned) or KAMI_VARIANT_AUTO (the measured faster one). */
+int kami_spgemm_bsr_numeric_variant(kami_variant_t variant, kami_dtype_t in_type, kami_dtype_t out_type, int bsr,
+                                    int mb, int kb, int nb,
+                                    const int *row_ptr_a, const int *col_idx_a, const void *val_a,
+                                    const int *row_ptr_b, const int *col_idx_b, const void *val_b,
+                                    const int *row_ptr_c, const int *col_idx_c, void *val_c,
+                                    int64_t nnz_c, double alpha, double beta, int num_iter, void *stream);
+
 /* ------------------------------------------------------------------------ */
 /* Block SpMM: BSR (16 x 16 tiles) times dense                              */
 /* ------------------------------------------------------------------------ */

@@ -57,6 +57,10 @@ SIGNATURES = {
                                      _vp, _i64, _i64, _d, _d, _i, _vp], _i),
     "kami_spgemm_bsr_symbolic": ([_i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(_i), _vp], _i),
     "kami_spgemm_bsr_fill_colidx": ([_i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp], _i),
+    "kami_spgemm_bsr_numeric_variant": ([_i, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                         _i64, _d, _d, _i, _vp], _i),
+    "kami_spgemm_bsr_block": ([_i, _i, _i, _i, _i, _i, _i, _i, _i64, _vp, _vp, _vp, _i64, _i, _vp, _vp, _vp, _i64, _i,
+                               _vp, _vp, _vp, _i64, _i, _d, _d, _i, _vp], _i),
     "kami_spgemm_bsr_symbolic_device": ([_i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _vp], _i),
     "kami_spgemm_bsr_numeric": ([_i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64,
                                  _d, _d, _i, _vp], _i),

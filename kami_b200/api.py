@@ -420,12 +420,15 @@ def spgemm_fill_colidx(A: BSR, B: BSR, row_ptr_c: torch.Tensor, nnz_c: int, stre
 
 
 def spgemm_numeric(A: BSR, B: BSR, row_ptr_c, col_idx_c, out_dtype=torch.float32, C_values=None, *,
-                   alpha=1.0, beta=0.0, num_iter=1, stream=None) -> torch.Tensor:
+                   alpha=1.0, beta=0.0, num_iter=1, variant: str = "auto", stream=None) -> torch.Tensor:
+    """Numeric pass (kami_spgemm_bsr_numeric_variant): variant "auto",
+    "mma_sync" or "tcgen05"."""
     nnz_c = col_idx_c.numel()
     if C_values is None:
         C_values = torch.empty((max(nnz_c, 1), 16, 16), dtype=out_dtype, device=A.row_ptr.device)
     with _on(*_bsr_tensors(A, B), row_ptr_c, col_idx_c, C_values):
-        st = load().kami_spgemm_bsr_numeric(_DT[A.values.dtype], _DT[C_values.dtype], 16, A.block_rows,
+        st = load().kami_spgemm_bsr_numeric_variant(_VAR[variant], _DT[A.values.dtype], _DT[C_values.dtype], 16,
+                                            A.block_rows,
                                             A.block_cols, B.block_cols, A.row_ptr.data_ptr(), _ptr(A.col_idx),
                                             _ptr(A.values), B.row_ptr.data_ptr(), _ptr(B.col_idx), _ptr(B.values),
                                             row_ptr_c.data_ptr(), _ptr(col_idx_c), _ptr(C_values), nnz_c,
@@ -452,12 +455,13 @@ def spgemm_symbolic_device(A: BSR, B: BSR, capacity: int, stream=None):
 
 
 def spgemm_numeric_bound(A: BSR, B: BSR, row_ptr_c, col_idx_c, C_values, *, alpha=1.0, beta=0.0, num_iter=1,
-                         stream=None) -> torch.Tensor:
+                         variant: str = "auto", stream=None) -> torch.Tensor:
     """Numeric pass into C_values [capacity, 16, 16] with the capacity as the
     bound of nnzC (no host synchronisation)."""
     cap = C_values.shape[0]
     with _on(*_bsr_tensors(A, B), row_ptr_c, col_idx_c, C_values):
-        st = load().kami_spgemm_bsr_numeric(_DT[A.values.dtype], _DT[C_values.dtype], 16, A.block_rows,
+        st = load().kami_spgemm_bsr_numeric_variant(_VAR[variant], _DT[A.values.dtype], _DT[C_values.dtype], 16,
+                                            A.block_rows,
                                             A.block_cols, B.block_cols, A.row_ptr.data_ptr(), _ptr(A.col_idx),
                                             _ptr(A.values), B.row_ptr.data_ptr(), _ptr(B.col_idx), _ptr(B.values),
                                             row_ptr_c.data_ptr(), _ptr(col_idx_c), _ptr(C_values), cap,
@@ -466,12 +470,39 @@ def spgemm_numeric_bound(A: BSR, B: BSR, row_ptr_c, col_idx_c, C_values, *, alph
     return C_values
 
 
-def spgemm(A: BSR, B: BSR, out_dtype=torch.float32, *, num_iter=1, stream=None) -> BSR:
+def spgemm(A: BSR, B: BSR, out_dtype=torch.float32, *, num_iter=1, variant: str = "auto", stream=None) -> BSR:
     """C = A * B: symbolic, column fill, numeric (the reference's sequence)."""
     rpc, nnz = spgemm_symbolic(A, B, stream)
     cic = spgemm_fill_colidx(A, B, rpc, nnz, stream)
-    vals = spgemm_numeric(A, B, rpc, cic, out_dtype, num_iter=num_iter, stream=stream)
+    vals = spgemm_numeric(A, B, rpc, cic, out_dtype, num_iter=num_iter, variant=variant, stream=stream)
     return BSR(rpc, cic, vals, B.block_cols)
+
+
+def spgemm_block(A: BSR, B: BSR, C: BSR, *, partition: str = "1d", P: int = 0, alpha: float = 1.0,
+                 beta: float = 0.0, num_iter: int = 1, stream=None) -> torch.Tensor:
+    """The reference's one-CTA block SpGEMM (kami_spgemm_bsr_block): C.values
+    = alpha * num_iter * A * B + beta * C.values for small BSR matrices (at
+    most 16 x 16 blocks) whose structure is shared by a batch: A.values
+    [batch, nnzA, 16, 16] or [nnzA, 16, 16] (shared), B likewise, C.values
+    [batch, nnzC, 16, 16] or [nnzC, 16, 16]; C.row_ptr / C.col_idx from the
+    symbolic pass.  The batch is the largest leading dimension."""
+    def _split(v):
+        return (v.shape[0], v.stride(0)) if v.dim() == 4 else (1, 0)
+    ba, sa = _split(A.values)
+    bb, sb = _split(B.values)
+    bc, sc = _split(C.values)
+    batch = max(ba, bb, bc)
+    if bc != batch:
+        raise ValueError("C.values must hold one tile set per problem")
+    with _on(*_bsr_tensors(A, B, C)):
+        st = load().kami_spgemm_bsr_block(
+            _DT[A.values.dtype], _DT[C.values.dtype], _PART[partition], int(P), 16, A.block_rows, A.block_cols,
+            B.block_cols, batch, A.row_ptr.data_ptr(), _ptr(A.col_idx), _ptr(A.values), sa, A.nnz_blocks,
+            B.row_ptr.data_ptr(), _ptr(B.col_idx), _ptr(B.values), sb, B.nnz_blocks,
+            C.row_ptr.data_ptr(), _ptr(C.col_idx), _ptr(C.values), sc, C.nnz_blocks,
+            float(alpha), float(beta), int(num_iter), _stream_ptr(stream))
+    check(st)
+    return C.values
 
 
 def spmm(A: BSR, B: torch.Tensor, C: torch.Tensor | None = None, *, b_layout: str = "row_kn",

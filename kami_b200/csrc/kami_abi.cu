@@ -18,6 +18,7 @@ int grouped_tc05_read_error(int *flag);
 int spgemm_read_error(int *flag);
 int grouped_f64s_read_error(int *flag);
 int spmm_tc05_read_error(int *flag);
+int spgemm_tc05_read_error(int *flag);
 int split_read_error(int *flag);
 int grouped_fallback(const GemmArgs &g, int in_type, cudaStream_t stream);
 
@@ -264,6 +265,9 @@ int kami_device_status(int *code)
         return st;
     if ((st = spmm_tc05_read_error(&c7)))
         return st;
+    int c8 = 0;
+    if ((st = spgemm_tc05_read_error(&c8)))
+        return st;
     if (!*code)
         *code = c2;
     if (!*code)
@@ -276,6 +280,8 @@ int kami_device_status(int *code)
         *code = c6;
     if (!*code)
         *code = c7;
+    if (!*code)
+        *code = c8;
     if (*code)
         return fail(KAMI_ERR_TIMEOUT, "a bounded device wait gave up (code %d)", *code);
     return KAMI_OK;

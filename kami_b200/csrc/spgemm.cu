@@ -31,6 +31,7 @@
 #include <mutex>
 
 #include "kami_common.cuh"
+#include "spgemm_tiles.cuh"
 
 namespace kami {
 
@@ -47,6 +48,8 @@ __device__ unsigned int g_spg_bar[kFuseSlots][2];
 __device__ int g_spg_error = 0;
 
 namespace {
+
+using namespace sptile;
 
 constexpr int kBsr = 16;
 
@@ -377,22 +380,6 @@ __global__ void spgemm_symbolic_fused_kernel(int mb, int nb, const int *__restri
 // ---------------------------------------------------------------------------
 // numeric
 // ---------------------------------------------------------------------------
-template <bool BF16>
-__device__ __forceinline__ void mma16816(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
-                                         uint32_t b0, uint32_t b1)
-{
-    if constexpr (BF16)
-        asm("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-            "{%0,%1,%2,%3};"
-            : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-            : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
-    else
-        asm("mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-            "{%0,%1,%2,%3};"
-            : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-            : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
-}
-
 struct SpNumArgs
 {
     int mb, nb;
@@ -405,56 +392,11 @@ struct SpNumArgs
     int num_iter;
 };
 
-// Store one C tile with alpha / beta: lane holds rows g, g+8 and columns
-// 2t, 2t+1 (acc0) and 2t+8, 2t+9 (acc1).
+// Store one C tile with alpha / beta (lane layout of store_tile_frag).
 __device__ __forceinline__ void store_c_tile(const SpNumArgs &p, int64_t c, int gq, int tq, const float (&acc0)[4],
                                              const float (&acc1)[4])
 {
-    const int r0 = gq, r1 = gq + 8, c0 = 2 * tq;
-    if (p.out_type == KAMI_F32)
-    {
-        float *out = reinterpret_cast<float *>(p.vc) + c * 256;
-        float2 v00 = make_float2(acc0[0], acc0[1]), v01 = make_float2(acc1[0], acc1[1]);
-        float2 v10 = make_float2(acc0[2], acc0[3]), v11 = make_float2(acc1[2], acc1[3]);
-        if (p.alpha != 1.f || p.beta != 0.f)
-        {
-            const float2 o00 = *reinterpret_cast<float2 *>(out + r0 * 16 + c0);
-            const float2 o01 = *reinterpret_cast<float2 *>(out + r0 * 16 + c0 + 8);
-            const float2 o10 = *reinterpret_cast<float2 *>(out + r1 * 16 + c0);
-            const float2 o11 = *reinterpret_cast<float2 *>(out + r1 * 16 + c0 + 8);
-            const float a = p.alpha, b = p.beta;
-            v00 = make_float2(a * v00.x + (b != 0.f ? b * o00.x : 0.f), a * v00.y + (b != 0.f ? b * o00.y : 0.f));
-            v01 = make_float2(a * v01.x + (b != 0.f ? b * o01.x : 0.f), a * v01.y + (b != 0.f ? b * o01.y : 0.f));
-            v10 = make_float2(a * v10.x + (b != 0.f ? b * o10.x : 0.f), a * v10.y + (b != 0.f ? b * o10.y : 0.f));
-            v11 = make_float2(a * v11.x + (b != 0.f ? b * o11.x : 0.f), a * v11.y + (b != 0.f ? b * o11.y : 0.f));
-        }
-        *reinterpret_cast<float2 *>(out + r0 * 16 + c0) = v00;
-        *reinterpret_cast<float2 *>(out + r0 * 16 + c0 + 8) = v01;
-        *reinterpret_cast<float2 *>(out + r1 * 16 + c0) = v10;
-        *reinterpret_cast<float2 *>(out + r1 * 16 + c0 + 8) = v11;
-    }
-    else
-    {
-        uint16_t *out = reinterpret_cast<uint16_t *>(p.vc) + c * 256;
-        const bool bf = p.out_type == KAMI_BF16;
-        auto cvt = [&](float x, uint16_t old) -> uint16_t {
-            float y = p.alpha * x;
-            if (p.beta != 0.f)
-                y += p.beta * to_float(old, bf);
-            return bf ? __bfloat16_as_ushort(__float2bfloat16_rn(y)) : __half_as_ushort(__float2half_rn(y));
-        };
-        const int offs[4] = {r0 * 16 + c0, r0 * 16 + c0 + 8, r1 * 16 + c0, r1 * 16 + c0 + 8};
-        const float vals[4][2] = {{acc0[0], acc0[1]}, {acc1[0], acc1[1]}, {acc0[2], acc0[3]}, {acc1[2], acc1[3]}};
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-        {
-            uint32_t *dst = reinterpret_cast<uint32_t *>(out + offs[q]);
-            const uint32_t old = p.beta != 0.f ? *dst : 0u;
-            const uint16_t lo16 = cvt(vals[q][0], (uint16_t)(old & 0xffff));
-            const uint16_t hi16 = cvt(vals[q][1], (uint16_t)(old >> 16));
-            *dst = (uint32_t)lo16 | ((uint32_t)hi16 << 16);
-        }
-    }
+    store_tile_frag(p.vc, c, p.out_type, p.alpha, p.beta, gq, tq, acc0, acc1);
 }
 
 template <bool BF16>
@@ -558,40 +500,6 @@ constexpr int kRowWarps = 8;
 constexpr int kMaxATiles = 32;   // 16 KB of A tiles (about 28 KB per CTA: 8 CTAs per SM)
 constexpr int kMaxBList = 2048;  // 8 KB of B column indices
 
-// byte offset of row r, 16-byte chunk c of a 16 x 16 16-bit tile (32-byte
-// rows): the chunk is flipped for rows 4-7 and 12-15 so that the eight rows
-// of an ldmatrix phase fall in distinct banks
-__device__ __forceinline__ int tile_swz(int r, int c) { return r * 32 + ((c ^ ((r >> 2) & 1)) << 4); }
-
-// copy one 512-byte tile (16 bytes per lane) into a swizzled shared tile
-__device__ __forceinline__ void stage_tile(uint8_t *dst, const uint16_t *src, int lane)
-{
-    const uint4 v = __ldg(reinterpret_cast<const uint4 *>(src) + lane);
-    *reinterpret_cast<uint4 *>(dst + tile_swz(lane >> 1, lane & 1)) = v;
-}
-
-// ldmatrix address of lane for the x4 load of a swizzled tile: matrices
-// (rows 0-7, chunk 0), (rows 8-15, chunk 0), (rows 0-7, chunk 1), (8-15, 1)
-__device__ __forceinline__ uint32_t tile_ldsm_addr(uint32_t base, int lane)
-{
-    const int m = lane >> 3, i = lane & 7;
-    return base + tile_swz((m & 1) * 8 + i, m >> 1);
-}
-
-__device__ __forceinline__ void ldsm4(uint32_t a, uint32_t (&r)[4])
-{
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(a));
-}
-
-__device__ __forceinline__ void ldsm4_t(uint32_t a, uint32_t (&r)[4])
-{
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(a));
-}
-
 template <bool BF16>
 __global__ void __launch_bounds__(kRowWarps * 32) spgemm_numeric_row_kernel(const SpNumArgs p)
 {
@@ -602,8 +510,9 @@ __global__ void __launch_bounds__(kRowWarps * 32) spgemm_numeric_row_kernel(cons
     __shared__ int sK[kMaxATiles];
     const int i = blockIdx.x;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int c0 = p.rpc[i], c1 = p.rpc[i + 1];
-    if (c0 == c1)
+    const int c0 = p.rpc[i];
+    const int c1 = (int)min((int64_t)p.rpc[i + 1], p.nnzc); // tiles past the caller's bound are untouched
+    if (c1 <= c0)
         return;
     const int a0 = p.rpa[i], na = p.rpa[i + 1] - a0;
     const bool a_staged = na <= kMaxATiles;
@@ -849,6 +758,14 @@ int symbolic_fused(int mb, int nb, const int *rpa, const int *cia, const int *rp
 
 } // namespace
 
+int spgemm_tc05_launch(bool bf16, int mb, int64_t nnzc, const int *rpa, const int *cia, const int *rpb, const int *cib,
+                       const int *rpc, const int *cic, const void *va, const void *vb, void *vc, int out_type,
+                       double alpha, double beta, int num_iter, cudaStream_t s);
+
+// AUTO's choice of the numeric kernel: the mma.sync row kernel (false) or
+// the tcgen05 kernel (true).
+bool spgemm_auto_tc05() { return false; }
+
 int spgemm_read_error(int *flag)
 {
     int v = 0, z = 0;
@@ -979,6 +896,19 @@ int kami_spgemm_bsr_numeric(kami_dtype_t in_type, kami_dtype_t out_type, int bsr
                             const int *col_idx_b, const void *val_b, const int *row_ptr_c, const int *col_idx_c,
                             void *val_c, int64_t nnz_c, double alpha, double beta, int num_iter, void *stream)
 {
+    return kami_spgemm_bsr_numeric_variant(KAMI_VARIANT_AUTO, in_type, out_type, bsr, mb, kb, nb, row_ptr_a,
+                                           col_idx_a, val_a, row_ptr_b, col_idx_b, val_b, row_ptr_c, col_idx_c,
+                                           val_c, nnz_c, alpha, beta, num_iter, stream);
+}
+
+int kami_spgemm_bsr_numeric_variant(kami_variant_t variant, kami_dtype_t in_type, kami_dtype_t out_type, int bsr,
+                                    int mb, int kb, int nb, const int *row_ptr_a, const int *col_idx_a,
+                                    const void *val_a, const int *row_ptr_b, const int *col_idx_b, const void *val_b,
+                                    const int *row_ptr_c, const int *col_idx_c, void *val_c, int64_t nnz_c,
+                                    double alpha, double beta, int num_iter, void *stream)
+{
+    if (variant != KAMI_VARIANT_AUTO && variant != KAMI_VARIANT_MMA_SYNC && variant != KAMI_VARIANT_TCGEN05)
+        return fail(KAMI_ERR_INVALID_VALUE, "spgemm numeric: variant must be AUTO, MMA_SYNC or TCGEN05");
     int st = check_bsr_args(bsr, mb, kb, nb, row_ptr_a, col_idx_a, row_ptr_b, col_idx_b);
     if (st)
         return st;
@@ -1017,7 +947,14 @@ int kami_spgemm_bsr_numeric(kami_dtype_t in_type, kami_dtype_t out_type, int bsr
     if (grid > 0x7fffffff)
         return fail(KAMI_ERR_UNSUPPORTED, "spgemm numeric: too many C tiles");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    const bool rowwise = !(reinterpret_cast<uintptr_t>(val_a) & 15) && !(reinterpret_cast<uintptr_t>(val_b) & 15);
+    const bool aligned16 = !(reinterpret_cast<uintptr_t>(val_a) & 15) && !(reinterpret_cast<uintptr_t>(val_b) & 15);
+    const bool tc_ok = aligned16 && !(reinterpret_cast<uintptr_t>(val_c) & 15);
+    if (variant == KAMI_VARIANT_TCGEN05 && !tc_ok)
+        return fail(KAMI_ERR_MISALIGNED, "spgemm numeric (tcgen05): tile arrays must be 16-byte aligned");
+    if (variant == KAMI_VARIANT_TCGEN05 || (variant == KAMI_VARIANT_AUTO && tc_ok && spgemm_auto_tc05()))
+        return spgemm_tc05_launch(in_type == KAMI_BF16, mb, nnz_c, row_ptr_a, col_idx_a, row_ptr_b, col_idx_b, row_ptr_c,
+                                  col_idx_c, val_a, val_b, val_c, out_type, alpha, beta, num_iter, s);
+    const bool rowwise = aligned16;
     if (rowwise) // one CTA per block-row, staged operands
     {
         if (in_type == KAMI_BF16)

@@ -256,6 +256,47 @@ __device__ __forceinline__ uint64_t desc_mnmajor_sw128(uint32_t addr, uint32_t l
     return d;
 }
 
+// Descriptors of 16 x 16 16-bit tiles stored with 32-byte swizzling (rows of
+// 32 bytes, 8-row atoms of 256 bytes on 256-byte boundaries, the 16-byte
+// chunk of rows 4-7 of each atom flipped): layout type 6 (SWIZZLE_32B),
+// SBO = 256 bytes to the next 8 rows.  K-major: row = M (or N) index, K
+// contiguous; MN-major: row = K index, 16 MN elements contiguous (LBO, the
+// step to the next 16 MN elements, is unused for N = 16).
+__device__ __forceinline__ uint64_t desc_kmajor_sw32(uint32_t addr)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((addr & 0x3FFFF) >> 4);
+    d |= (uint64_t)1 << 16;          // LBO (ignored for swizzled K-major)
+    d |= (uint64_t)(256 >> 4) << 32; // SBO
+    d |= (uint64_t)1 << 46;          // version
+    d |= (uint64_t)6 << 61;          // SWIZZLE_32B
+    return d;
+}
+
+__device__ __forceinline__ uint64_t desc_mnmajor_sw32(uint32_t addr)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((addr & 0x3FFFF) >> 4);
+    d |= (uint64_t)(512 >> 4) << 16; // LBO: next 16 MN elements (unused at N = 16)
+    d |= (uint64_t)(256 >> 4) << 32; // SBO: next 8 K rows
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)6 << 61;
+    return d;
+}
+
+// D[tmem] += A * B^T (kind::f16, both operands in shared memory) with the
+// lanes of D whose bit is set in `off` (bit l % 32 of off[l / 32]) left
+// unchanged -- the accumulators of other tiles that share these columns.
+__device__ __forceinline__ void mma_f16_ss_lanes(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                                 const uint32_t (&off)[4])
+{
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "setp.ne.b32 p, 1, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%4, %5, %6, %7}, p;\n\t}" ::"r"(d_tmem),
+                 "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(off[0]), "r"(off[1]), "r"(off[2]), "r"(off[3])
+                 : "memory");
+}
+
 // Instruction descriptor of tcgen05.mma kind::f16: FP32 accumulator, given
 // M (64 or 128), N (multiple of 16, <= 256) and the operand majors
 // (0 = K-major, 1 = MN-major).
