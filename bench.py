@@ -522,6 +522,10 @@ def run_secondary(args):
                 api.spgemm_fill_colidx(A, B, r, nnzc)
 
             ms_sym = _time_ms(symbolic, W, K_, flush)
+            ms_var = {}
+            for variant in ("mma_sync", "tcgen05"):
+                ms_var[variant] = _time_ms(lambda: api.spgemm_numeric(A, B, rpc, cic, C_values=vc, variant=variant),
+                                           W, K_, flush)
             ms_num = _time_ms(lambda: api.spgemm_numeric(A, B, rpc, cic, C_values=vc), W, K_, flush)
             # the same product with no host round trip: on-device symbolic pass
             # into a capacity of nnzCub (an upper bound of nnzC), then numeric
@@ -543,7 +547,9 @@ def run_secondary(args):
                    "symbolic_ms": min(ms_sym), "tflops_numeric": fl / t / 1e9,
                    "hbm_gbs_numeric": by / t / 1e6, "frac_hbm": by / t / 1e6 / peak_bw,
                    "tflops_end_to_end": fl / (t + min(ms_sym)) / 1e9, "symbolic_device_ms": min(ms_symd),
-                   "end_to_end_device_ms": min(ms_dev), "tflops_end_to_end_device": fl / min(ms_dev) / 1e9})
+                   "end_to_end_device_ms": min(ms_dev), "tflops_end_to_end_device": fl / min(ms_dev) / 1e9,
+                   "numeric_ms_by_variant": {v: statistics.fmean(m) for v, m in ms_var.items()},
+                   "frac_hbm_by_variant": {v: by / statistics.fmean(m) / 1e6 / peak_bw for v, m in ms_var.items()}})
         return
 
     if args.workload == "spmm":
@@ -631,6 +637,48 @@ def run_secondary(args):
                        "hbm_gbs": by / t / 1e6 if by else None})
 
         sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        # CUTLASS's own sm_100a batched GEMM (tcgen05 / TMA / TMEM collectives,
+        # cluster 1 x 1 x 1) on the same buffers, reference B layout (N x K)
+        import ctypes
+        from kami_b200 import build as kbuild
+        cmp_path = kbuild.build_comparators()
+        if cmp_path:
+            CL = ctypes.CDLL(cmp_path)
+            CL.kami_cmp_cutlass_gemm_batched.argtypes = [ctypes.c_int] * 6 + [ctypes.c_int64] + \
+                [ctypes.c_void_p] * 4 + [ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t), ctypes.c_void_p]
+            dtc = {torch.float16: 0, torch.bfloat16: 1, torch.float32: 3}
+            for (b, n, idt, odt) in ((4 * sms, 128, torch.float16, torch.float32),
+                                     (4 * sms, 128, torch.float16, torch.float16),
+                                     (2048, 128, torch.bfloat16, torch.bfloat16),
+                                     (4096, 64, torch.bfloat16, torch.bfloat16),
+                                     (8192, 64, torch.float16, torch.float32)):
+                A = torch.tensor(rng.uniform(-1, 1, (b, n, n)), device=dev).to(idt)
+                B = torch.tensor(rng.uniform(-1, 1, (b, n, n)), device=dev).to(idt)
+                C1 = torch.empty((b, n, n), dtype=odt, device=dev)
+                C2 = torch.empty((b, n, n), dtype=odt, device=dev)
+                need = ctypes.c_size_t(0)
+                tile = 64 if n == 64 else 128
+                args0 = (dtc[idt], dtc[odt], tile, n, n, n, b, A.data_ptr(), B.data_ptr(), C2.data_ptr())
+                CL.kami_cmp_cutlass_gemm_batched(*args0, None, 0, ctypes.byref(need), None)
+                ws = torch.empty(max(int(need.value), 16), dtype=torch.uint8, device=dev)
+                strm = torch.cuda.current_stream(dev).cuda_stream
+
+                def cutlass_run():
+                    st = CL.kami_cmp_cutlass_gemm_batched(*args0, ws.data_ptr(), ws.numel(), None, strm)
+                    if st != 0:
+                        raise RuntimeError(f"CUTLASS comparator returned {st}")
+
+                name = f"{str(idt).split('.')[-1]} {n}^3 x {b} streamed, {str(odt).split('.')[-1]} out, B as N x K"
+                for impl, fn in (("kami_b200", lambda: api.gemm_batched(A, B, C1)), ("cutlass_sm100", cutlass_run)):
+                    t = statistics.fmean(_time_ms(fn, W, K_, flush))
+                    by = b * n * n * (2 + 2 + C1.element_size())
+                    _emit({"workload": "comparators", "case": name, "impl": impl, "ms": t,
+                           "tflops": 2.0 * n ** 3 * b / t / 1e9, "hbm_gbs": by / t / 1e6,
+                           "frac_hbm": by / t / 1e6 / peak_bw})
+                diff = float((C1.float() - C2.float()).abs().max())
+                _emit({"workload": "comparators", "case": name, "max_abs_diff_kami_vs_cutlass": diff})
+        else:
+            _emit({"workload": "comparators", "impl": "cutlass_sm100", "unavailable": "CUTLASS headers not found"})
         # FP16 128^3 x (4 x SMs), streamed (one product per problem)
         b, n = 4 * sms, 128
         A = torch.tensor(rng.uniform(-1, 1, (b, n, n)), device=dev).half()

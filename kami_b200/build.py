@@ -72,9 +72,58 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
     return LIB
 
 
+CMP_DIR = os.path.join(HERE, "cmp")
+CMP_LIB = os.path.join(HERE, "libkami_cmp.so")
+
+
+def cutlass_include():
+    """The CUTLASS / CuTe header tree shipped in this image (flashinfer's copy),
+    or $KAMI_CUTLASS_ROOT; None when absent."""
+    roots = [os.environ.get("KAMI_CUTLASS_ROOT")]
+    try:
+        import importlib.util
+        spec = importlib.util.find_spec("flashinfer")
+        if spec and spec.origin:
+            roots.append(os.path.join(os.path.dirname(spec.origin), "data", "cutlass"))
+    except Exception:
+        pass
+    for r in roots:
+        if r and os.path.exists(os.path.join(r, "include", "cute", "arch", "mma_sm100_umma.hpp")):
+            return r
+    return None
+
+
+def build_comparators(force: bool = False, verbose: bool = False):
+    """Comparator library (not the product): CUTLASS's own sm_100a batched GEMM
+    (kami_b200/cmp/*.cu) for the benchmark's side-by-side lines.  Skipped,
+    returning None, when the CUTLASS headers are absent or it fails to build."""
+    srcs = sorted(glob.glob(os.path.join(CMP_DIR, "*.cu")))
+    root = cutlass_include()
+    if not srcs or root is None:
+        return None
+    newest = max(os.path.getmtime(x) for x in srcs)
+    if not force and os.path.exists(CMP_LIB) and os.path.getmtime(CMP_LIB) >= newest:
+        return CMP_LIB
+    tmp = CMP_LIB + ".tmp"
+    cmd = [nvcc()] + ARCH + ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", "-DNDEBUG",
+                             "-diag-suppress", "20012", "-I", os.path.join(root, "include"),
+                             "-I", os.path.join(root, "tools", "util", "include"), "-shared", "-o", tmp] + srcs
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(f"comparator build skipped:\n{r.stderr[-2000:]}\n")
+        return None
+    os.replace(tmp, CMP_LIB)
+    if verbose:
+        print(f"linked {CMP_LIB}")
+    return CMP_LIB
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
     ap.add_argument("-j", type=int, default=None)
+    ap.add_argument("--comparators", action="store_true", help="also build the CUTLASS comparator library")
     a = ap.parse_args()
     print(build(force=a.force, jobs=a.j, verbose=True))
+    if a.comparators:
+        print(build_comparators(force=a.force, verbose=True))

@@ -500,15 +500,13 @@ constexpr int kRowWarps = 8;
 constexpr int kMaxATiles = 32;   // 16 KB of A tiles (about 28 KB per CTA: 8 CTAs per SM)
 constexpr int kMaxBList = 2048;  // 8 KB of B column indices
 
-template <bool BF16>
-__global__ void __launch_bounds__(kRowWarps * 32) spgemm_numeric_row_kernel(const SpNumArgs p)
+// The row's C tiles pulled one at a time (the per-tile search form); the
+// CTA's shared buffers are passed in: sA kMaxATiles * 512 bytes, sB
+// kRowWarps * 512, sList kMaxBList ints, sOff kMaxATiles + 1, sK kMaxATiles.
+template <bool BF16, int WARPS>
+__device__ __forceinline__ void numeric_row_pull(const SpNumArgs &p, const int i, uint8_t *sA, uint8_t *sB,
+                                                 int *sList, int *sOff, int *sK)
 {
-    __shared__ __align__(16) uint8_t sA[kMaxATiles * 512];
-    __shared__ __align__(16) uint8_t sB[kRowWarps * 512]; // one B tile slot per warp
-    __shared__ int sList[kMaxBList];
-    __shared__ int sOff[kMaxATiles + 1];
-    __shared__ int sK[kMaxATiles];
-    const int i = blockIdx.x;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int c0 = p.rpc[i];
     const int c1 = (int)min((int64_t)p.rpc[i + 1], p.nnzc); // tiles past the caller's bound are untouched
@@ -521,7 +519,7 @@ __global__ void __launch_bounds__(kRowWarps * 32) spgemm_numeric_row_kernel(cons
     bool l_staged = false;
     if (a_staged)
     {
-        for (int e = warp; e < na; e += kRowWarps)
+        for (int e = warp; e < na; e += WARPS)
             stage_tile(sA + e * 512, p.va + (int64_t)(a0 + e) * 256, lane);
         if (warp == 0)
         {
@@ -555,7 +553,7 @@ __global__ void __launch_bounds__(kRowWarps * 32) spgemm_numeric_row_kernel(cons
         __syncthreads();
         l_staged = sOff[na] <= kMaxBList;
         if (l_staged)
-            for (int e = warp; e < na; e += kRowWarps)
+            for (int e = warp; e < na; e += WARPS)
             {
                 const int b0 = p.rpb[sK[e]], len = sOff[e + 1] - sOff[e];
                 for (int q = lane; q < len; q += 32)
@@ -568,7 +566,7 @@ __global__ void __launch_bounds__(kRowWarps * 32) spgemm_numeric_row_kernel(cons
     const uint32_t sA_u = (uint32_t)__cvta_generic_to_shared(sA);
     const uint32_t slot = (uint32_t)__cvta_generic_to_shared(sB + warp * 512);
     uint8_t *slot_p = sB + warp * 512;
-    for (int c = c0 + warp; c < c1; c += kRowWarps)
+    for (int c = c0 + warp; c < c1; c += WARPS)
     {
         const int j = p.cic[c];
         float acc0[4] = {0.f, 0.f, 0.f, 0.f}; // C columns 0..7
@@ -648,6 +646,248 @@ __global__ void __launch_bounds__(kRowWarps * 32) spgemm_numeric_row_kernel(cons
             }
         store_c_tile(p, c, gq, tq, acc0, acc1);
     }
+}
+
+template <bool BF16>
+__global__ void __launch_bounds__(kRowWarps * 32) spgemm_numeric_row_kernel(const SpNumArgs p)
+{
+    __shared__ __align__(16) uint8_t sA[kMaxATiles * 512];
+    __shared__ __align__(16) uint8_t sB[kRowWarps * 512]; // one B tile slot per warp
+    __shared__ int sList[kMaxBList];
+    __shared__ int sOff[kMaxATiles + 1];
+    __shared__ int sK[kMaxATiles];
+    numeric_row_pull<BF16, kRowWarps>(p, blockIdx.x, sA, sB, sList, sOff, sK);
+}
+
+// ---------------------------------------------------------------------------
+// numeric, one CTA per block-row of C, products pushed to their tiles
+//
+// The per-tile search above costs one binary search per (C tile, A entry)
+// pair -- about ten per tile at 1 % density -- in dependent shared-memory
+// loads, and each tile's B tile load is exposed.  Here the row's products
+// are enumerated once: all threads walk the flattened (A entry, B entry)
+// space, find each product's C position by one binary search in the row's
+// ColIdxC (staged in shared memory), and a counting sort by position
+// groups them per C tile (each tile's short list then re-sorted by
+// enumeration index, so products still accumulate in ascending k).  The
+// warps then take the tiles in turn; each streams its products' B tiles
+// with 16-byte cp.async into a two-slot ring (the next product's tile in
+// flight while the current one is multiplied), A tiles read from the staged
+// row.  Rows beyond the staging capacities fall back to the per-tile form.
+// ---------------------------------------------------------------------------
+constexpr int kPushWarps = 4;     // 4-warp CTAs, ~31 KB each: seven per SM, every row of a 1024-row matrix in one wave
+constexpr int kPushMaxC = 512;    // C tiles of a row
+constexpr int kPushMaxProd = 512; // products of a row
+
+template <bool BF16>
+__global__ void __launch_bounds__(kPushWarps * 32) spgemm_numeric_push_kernel(const SpNumArgs p)
+{
+    constexpr int kRowWarps = kPushWarps;
+    __shared__ __align__(16) uint8_t sA[kMaxATiles * 512];
+    __shared__ __align__(16) uint8_t sB[kRowWarps * 2 * 512]; // two B slots per warp
+    // one pool of indices (the per-tile fallback uses its first kMaxBList
+    // entries as its list buffer): the row's ColIdxC, then per tile the
+    // product count / range end; per product (A entry << 16) | C position
+    // (-1 when absent), its B entry, and the products grouped by C tile
+    __shared__ int sPool[5 * kPushMaxC];
+    static_assert(5 * kPushMaxC >= kMaxBList && kPushMaxProd == kPushMaxC, "fallback list buffer");
+    int *sCol = sPool, *sCnt = sPool + kPushMaxC, *sPep = sPool + 2 * kPushMaxC, *sPb = sPool + 3 * kPushMaxC,
+        *sOrd = sPool + 4 * kPushMaxC;
+    __shared__ int sOff[kMaxATiles + 1];
+    __shared__ int sK[kMaxATiles];
+    __shared__ int sRb[kMaxATiles];
+    const int i = blockIdx.x;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    constexpr int kT = kRowWarps * 32;
+    const int c0 = p.rpc[i];
+    const int c1 = (int)min((int64_t)p.rpc[i + 1], p.nnzc); // tiles past the caller's bound are untouched
+    if (c1 <= c0)
+        return;
+    const int nt = c1 - c0;
+    const int a0 = p.rpa[i], na = p.rpa[i + 1] - a0;
+    if (nt > kPushMaxC || na > kMaxATiles)
+    {
+        numeric_row_pull<BF16, kPushWarps>(p, i, sA, sB, sPool, sOff, sK);
+        return;
+    }
+    // ---- stage: ColIdxC, B row ranges and their prefix, A tiles ----
+    for (int t = tid; t < nt; t += kT)
+    {
+        sCol[t] = p.cic[c0 + t];
+        sCnt[t] = 0;
+    }
+    if (warp == 0)
+    {
+        int len = 0;
+        if (lane < na)
+        {
+            const int k = p.cia[a0 + lane];
+            const int rb = p.rpb[k];
+            len = p.rpb[k + 1] - rb;
+            sK[lane] = k;
+            sRb[lane] = rb;
+        }
+        int pre = len;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            const int y = __shfl_up_sync(0xffffffffu, pre, o);
+            if (lane >= o)
+                pre += y;
+        }
+        if (lane < na)
+            sOff[lane] = pre - len;
+        if (lane == 31)
+            sOff[na] = pre;
+    }
+    for (int e = warp; e < na; e += kRowWarps)
+        stage_tile(sA + e * 512, p.va + (int64_t)(a0 + e) * 256, lane);
+    __syncthreads();
+    const int np = sOff[na];
+    if (np > kPushMaxProd)
+    {
+        __syncthreads();
+        numeric_row_pull<BF16, kPushWarps>(p, i, sA, sB, sPool, sOff, sK);
+        return;
+    }
+    // ---- enumerate the products and count them per C tile ----
+    for (int f = tid; f < np; f += kT)
+    {
+        int lo = 0, hi = na - 1; // entry e with sOff[e] <= f < sOff[e + 1]
+        while (lo < hi)
+        {
+            const int m = (lo + hi + 1) >> 1;
+            if (sOff[m] <= f)
+                lo = m;
+            else
+                hi = m - 1;
+        }
+        const int e = lo;
+        const int eb = sRb[e] + (f - sOff[e]);
+        const int j = p.cib[eb];
+        int l = 0, h = nt;
+        while (l < h)
+        {
+            const int m = (l + h) >> 1;
+            if (sCol[m] < j)
+                l = m + 1;
+            else
+                h = m;
+        }
+        const bool hit = l < nt && sCol[l] == j;
+        sPep[f] = hit ? ((e << 16) | l) : -1;
+        sPb[f] = eb;
+        if (hit)
+            atomicAdd(&sCnt[l], 1);
+    }
+    __syncthreads();
+    // ---- exclusive scan of the counts (warp 0, 32 consecutive entries per lane) ----
+    if (warp == 0)
+    {
+        const int per = (nt + 31) >> 5;
+        const int b0 = lane * per, b1 = min(nt, b0 + per);
+        int run = 0;
+        for (int t = b0; t < b1; ++t)
+            run += sCnt[t];
+        int pre = run;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            const int y = __shfl_up_sync(0xffffffffu, pre, o);
+            if (lane >= o)
+                pre += y;
+        }
+        int acc = pre - run;
+        for (int t = b0; t < b1; ++t)
+        {
+            const int c = sCnt[t];
+            sCnt[t] = acc;
+            acc += c;
+        }
+    }
+    __syncthreads();
+    // ---- scatter: afterwards sCnt[t] is the end of tile t's range ----
+    for (int f = tid; f < np; f += kT)
+    {
+        const int v = sPep[f];
+        if (v >= 0)
+            sOrd[atomicAdd(&sCnt[v & 0xffff], 1)] = f;
+    }
+    __syncthreads();
+    // ---- each tile's products in enumeration order (ascending k) ----
+    for (int t = tid; t < nt; t += kT)
+    {
+        const int b = t ? sCnt[t - 1] : 0, e = sCnt[t];
+        for (int x = b + 1; x < e; ++x)
+        {
+            const int v = sOrd[x];
+            int y = x - 1;
+            while (y >= b && sOrd[y] > v)
+            {
+                sOrd[y + 1] = sOrd[y];
+                --y;
+            }
+            sOrd[y + 1] = v;
+        }
+    }
+    __syncthreads();
+
+    // ---- multiply: warp w takes tiles w, w + 8, ...; B tiles two in flight ----
+    const int gq = lane >> 2, tq = lane & 3;
+    const uint32_t sA_u = (uint32_t)__cvta_generic_to_shared(sA);
+    const uint32_t slots = (uint32_t)__cvta_generic_to_shared(sB + warp * 1024);
+    const int swz = tile_swz(lane >> 1, lane & 1);
+    auto tile_begin = [&](int t) { return t ? sCnt[t - 1] : 0; };
+    // issue cursor over the warp's products: tile it, position iq
+    int it = warp, iq = it < nt ? tile_begin(it) : 0;
+    auto settle = [&]() {
+        while (it < nt && iq >= sCnt[it])
+        {
+            it += kRowWarps;
+            if (it < nt)
+                iq = tile_begin(it);
+        }
+    };
+    int issued = 0;
+    auto issue = [&]() {
+        settle();
+        if (it < nt)
+        {
+            const int eb = sPb[sOrd[iq]];
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(slots + (issued & 1) * 512 + swz),
+                         "l"(p.vb + (int64_t)eb * 256 + lane * 8)
+                         : "memory");
+            ++iq;
+            ++issued;
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    issue();
+    int used = 0;
+    for (int t = warp; t < nt; t += kRowWarps)
+    {
+        float acc0[4] = {0.f, 0.f, 0.f, 0.f};
+        float acc1[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int q = tile_begin(t), qe = sCnt[t]; q < qe; ++q)
+        {
+            issue(); // the next product's B tile, into the other slot
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+            __syncwarp();
+            const int e = sPep[sOrd[q]] >> 16;
+            uint32_t a[4], b[4];
+            ldsm4(tile_ldsm_addr(sA_u + e * 512, lane), a);
+            ldsm4_t(tile_ldsm_addr(slots + (used & 1) * 512, lane), b);
+            ++used;
+            for (int r = 0; r < p.num_iter; ++r)
+            {
+                mma16816<BF16>(acc0, a[0], a[1], a[2], a[3], b[0], b[1]);
+                mma16816<BF16>(acc1, a[0], a[1], a[2], a[3], b[2], b[3]);
+            }
+            __syncwarp(); // every lane's fragments are read before the slot is refilled
+        }
+        store_c_tile(p, (int64_t)c0 + t, gq, tq, acc0, acc1);
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
 int bitmap_launch(int nb, int *warps_per_cta, size_t *smem)
@@ -955,12 +1195,12 @@ int kami_spgemm_bsr_numeric_variant(kami_variant_t variant, kami_dtype_t in_type
         return spgemm_tc05_launch(in_type == KAMI_BF16, mb, nnz_c, row_ptr_a, col_idx_a, row_ptr_b, col_idx_b, row_ptr_c,
                                   col_idx_c, val_a, val_b, val_c, out_type, alpha, beta, num_iter, s);
     const bool rowwise = aligned16;
-    if (rowwise) // one CTA per block-row, staged operands
+    if (rowwise) // one CTA per block-row, staged operands, products pushed to their tiles
     {
         if (in_type == KAMI_BF16)
-            spgemm_numeric_row_kernel<true><<<(unsigned)mb, kRowWarps * 32, 0, s>>>(p);
+            spgemm_numeric_push_kernel<true><<<(unsigned)mb, kPushWarps * 32, 0, s>>>(p);
         else
-            spgemm_numeric_row_kernel<false><<<(unsigned)mb, kRowWarps * 32, 0, s>>>(p);
+            spgemm_numeric_push_kernel<false><<<(unsigned)mb, kPushWarps * 32, 0, s>>>(p);
     }
     else if (in_type == KAMI_BF16)
         spgemm_numeric_kernel<true><<<(unsigned)grid, 256, 0, s>>>(p);
