@@ -14,12 +14,36 @@ kernel reads A, B and dC once and writes both gradients.
 
 All three products accumulate in FP32 (FP16/BF16 inputs) or FP64 and are
 returned in the input dtype, as torch.bmm does.
+
+The default path (the library's kernel choice) is the C++ operator
+torch.ops.kami.bmm (kami_b200/torch_ops/kami_torch_ops.cpp): the same two
+launches with its forward, backward node and argument handling in C++, so
+the host time per step stays below the kernels' time.
 """
 from __future__ import annotations
 
+import os
+
 import torch
 
-from . import api
+from . import _lib, api
+
+_OPS_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libkami_torch_ops.so")
+_ops_state = None
+
+
+def ops_available() -> bool:
+    """Load torch.ops.kami (the C++ operator library) once; False when it was
+    not built, in which case bmm runs the Python autograd.Function (the same
+    kernels, more host time per step)."""
+    global _ops_state
+    if _ops_state is None:
+        _ops_state = False
+        if os.path.exists(_OPS_PATH):
+            _lib.load()  # the kernels' library first, so both loaders share one copy
+            torch.ops.load_library(_OPS_PATH)
+            _ops_state = True
+    return _ops_state
 
 
 def _out_dtype(dt):
@@ -58,6 +82,15 @@ class KamiBmm(torch.autograd.Function):
         return dA, dB, None, None
 
 
+_OP_DTYPES = (torch.float16, torch.bfloat16, torch.float64)
+
+
 def bmm(A: torch.Tensor, B: torch.Tensor, partition: str = "auto", variant: str = "auto") -> torch.Tensor:
-    """torch.bmm semantics, computed by the KAMI block-GEMM kernels."""
+    """torch.bmm semantics, computed by the KAMI block-GEMM kernels.  With the
+    library's kernel choice (partition and variant "auto") on 3-D CUDA
+    operands it is the C++ operator torch.ops.kami.bmm (forward and backward
+    dispatched without Python); otherwise the Python KamiBmm function."""
+    if (partition == "auto" and variant == "auto" and A.dim() == 3 and B.dim() == 3 and A.is_cuda
+            and A.dtype in _OP_DTYPES and ops_available()):
+        return torch.ops.kami.bmm(A, B)
     return KamiBmm.apply(A, B, partition, variant)

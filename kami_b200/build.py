@@ -72,6 +72,36 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
     return LIB
 
 
+OPS_SRC = os.path.join(HERE, "torch_ops", "kami_torch_ops.cpp")
+OPS_LIB = os.path.join(HERE, "libkami_torch_ops.so")
+
+
+def build_torch_ops(force: bool = False, verbose: bool = False) -> str:
+    """torch.ops.kami (the differentiable batched GEMM as a C++ torch operator,
+    kami_b200/torch_ops/) linked against libkami_b200.so and libtorch."""
+    import torch
+    tdir = os.path.dirname(torch.__file__)
+    srcs = [OPS_SRC, os.path.join(INCLUDE, "kami.h")]
+    if not force and os.path.exists(OPS_LIB) and os.path.getmtime(OPS_LIB) >= max(os.path.getmtime(x) for x in srcs) \
+            and os.path.getmtime(OPS_LIB) >= os.path.getmtime(LIB):
+        return OPS_LIB
+    cuda_home = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+    abi = int(torch._C._GLIBCXX_USE_CXX11_ABI)
+    tmp = OPS_LIB + ".tmp"
+    cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", f"-D_GLIBCXX_USE_CXX11_ABI={abi}",
+           "-I", os.path.join(tdir, "include"), "-I", os.path.join(tdir, "include", "torch", "csrc", "api", "include"),
+           "-I", os.path.join(cuda_home, "include"), "-I", INCLUDE, OPS_SRC, "-o", tmp,
+           "-L", os.path.join(tdir, "lib"), "-ltorch", "-ltorch_cpu", "-lc10", "-lc10_cuda",
+           "-L", HERE, "-l:libkami_b200.so", "-Wl,-rpath,$ORIGIN", "-Wl,-rpath," + os.path.join(tdir, "lib")]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"torch operator build failed:\n{r.stderr[-3000:]}")
+    os.replace(tmp, OPS_LIB)
+    if verbose:
+        print(f"linked {OPS_LIB}")
+    return OPS_LIB
+
+
 CMP_DIR = os.path.join(HERE, "cmp")
 CMP_LIB = os.path.join(HERE, "libkami_cmp.so")
 
@@ -125,5 +155,6 @@ if __name__ == "__main__":
     ap.add_argument("--comparators", action="store_true", help="also build the CUTLASS comparator library")
     a = ap.parse_args()
     print(build(force=a.force, jobs=a.j, verbose=True))
+    print(build_torch_ops(force=a.force, verbose=True))
     if a.comparators:
         print(build_comparators(force=a.force, verbose=True))

@@ -503,7 +503,7 @@ constexpr int kMaxBList = 2048;  // 8 KB of B column indices
 // The row's C tiles pulled one at a time (the per-tile search form); the
 // CTA's shared buffers are passed in: sA kMaxATiles * 512 bytes, sB
 // kRowWarps * 512, sList kMaxBList ints, sOff kMaxATiles + 1, sK kMaxATiles.
-template <bool BF16, int WARPS>
+template <bool BF16, int WARPS, int MAXA = kMaxATiles>
 __device__ __forceinline__ void numeric_row_pull(const SpNumArgs &p, const int i, uint8_t *sA, uint8_t *sB,
                                                  int *sList, int *sOff, int *sK)
 {
@@ -513,7 +513,7 @@ __device__ __forceinline__ void numeric_row_pull(const SpNumArgs &p, const int i
     if (c1 <= c0)
         return;
     const int a0 = p.rpa[i], na = p.rpa[i + 1] - a0;
-    const bool a_staged = na <= kMaxATiles;
+    const bool a_staged = na <= MAXA;
 
     // ---- staging (whole CTA): A tiles, B row lengths, their prefix, lists ----
     bool l_staged = false;
@@ -678,13 +678,15 @@ __global__ void __launch_bounds__(kRowWarps * 32) spgemm_numeric_row_kernel(cons
 constexpr int kPushWarps = 4;     // 4-warp CTAs, ~31 KB each: seven per SM, every row of a 1024-row matrix in one wave
 constexpr int kPushMaxC = 512;    // C tiles of a row
 constexpr int kPushMaxProd = 512; // products of a row
+constexpr int kPushMaxA = 24;     // A tiles of a row staged (12 KB)
+constexpr int kPushDepth = 4;     // B tiles in flight per warp
 
 template <bool BF16>
 __global__ void __launch_bounds__(kPushWarps * 32) spgemm_numeric_push_kernel(const SpNumArgs p)
 {
     constexpr int kRowWarps = kPushWarps;
-    __shared__ __align__(16) uint8_t sA[kMaxATiles * 512];
-    __shared__ __align__(16) uint8_t sB[kRowWarps * 2 * 512]; // two B slots per warp
+    __shared__ __align__(16) uint8_t sA[kPushMaxA * 512];
+    __shared__ __align__(16) uint8_t sB[kRowWarps * kPushDepth * 512]; // B slots per warp
     // one pool of indices (the per-tile fallback uses its first kMaxBList
     // entries as its list buffer): the row's ColIdxC, then per tile the
     // product count / range end; per product (A entry << 16) | C position
@@ -693,9 +695,9 @@ __global__ void __launch_bounds__(kPushWarps * 32) spgemm_numeric_push_kernel(co
     static_assert(5 * kPushMaxC >= kMaxBList && kPushMaxProd == kPushMaxC, "fallback list buffer");
     int *sCol = sPool, *sCnt = sPool + kPushMaxC, *sPep = sPool + 2 * kPushMaxC, *sPb = sPool + 3 * kPushMaxC,
         *sOrd = sPool + 4 * kPushMaxC;
-    __shared__ int sOff[kMaxATiles + 1];
-    __shared__ int sK[kMaxATiles];
-    __shared__ int sRb[kMaxATiles];
+    __shared__ int sOff[kPushMaxA + 1];
+    __shared__ int sK[kPushMaxA];
+    __shared__ int sRb[kPushMaxA];
     const int i = blockIdx.x;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     constexpr int kT = kRowWarps * 32;
@@ -705,9 +707,9 @@ __global__ void __launch_bounds__(kPushWarps * 32) spgemm_numeric_push_kernel(co
         return;
     const int nt = c1 - c0;
     const int a0 = p.rpa[i], na = p.rpa[i + 1] - a0;
-    if (nt > kPushMaxC || na > kMaxATiles)
+    if (nt > kPushMaxC || na > kPushMaxA)
     {
-        numeric_row_pull<BF16, kPushWarps>(p, i, sA, sB, sPool, sOff, sK);
+        numeric_row_pull<BF16, kPushWarps, kPushMaxA>(p, i, sA, sB, sPool, sOff, sK);
         return;
     }
     // ---- stage: ColIdxC, B row ranges and their prefix, A tiles ----
@@ -747,7 +749,7 @@ __global__ void __launch_bounds__(kPushWarps * 32) spgemm_numeric_push_kernel(co
     if (np > kPushMaxProd)
     {
         __syncthreads();
-        numeric_row_pull<BF16, kPushWarps>(p, i, sA, sB, sPool, sOff, sK);
+        numeric_row_pull<BF16, kPushWarps, kPushMaxA>(p, i, sA, sB, sPool, sOff, sK);
         return;
     }
     // ---- enumerate the products and count them per C tile ----
@@ -832,10 +834,10 @@ __global__ void __launch_bounds__(kPushWarps * 32) spgemm_numeric_push_kernel(co
     }
     __syncthreads();
 
-    // ---- multiply: warp w takes tiles w, w + 8, ...; B tiles two in flight ----
+    // ---- multiply: warp w takes tiles w, w + W, ...; kPushDepth B tiles in flight ----
     const int gq = lane >> 2, tq = lane & 3;
     const uint32_t sA_u = (uint32_t)__cvta_generic_to_shared(sA);
-    const uint32_t slots = (uint32_t)__cvta_generic_to_shared(sB + warp * 1024);
+    const uint32_t slots = (uint32_t)__cvta_generic_to_shared(sB + warp * kPushDepth * 512);
     const int swz = tile_swz(lane >> 1, lane & 1);
     auto tile_begin = [&](int t) { return t ? sCnt[t - 1] : 0; };
     // issue cursor over the warp's products: tile it, position iq
@@ -854,7 +856,7 @@ __global__ void __launch_bounds__(kPushWarps * 32) spgemm_numeric_push_kernel(co
         if (it < nt)
         {
             const int eb = sPb[sOrd[iq]];
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(slots + (issued & 1) * 512 + swz),
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(slots + (issued % kPushDepth) * 512 + swz),
                          "l"(p.vb + (int64_t)eb * 256 + lane * 8)
                          : "memory");
             ++iq;
@@ -862,7 +864,9 @@ __global__ void __launch_bounds__(kPushWarps * 32) spgemm_numeric_push_kernel(co
         }
         asm volatile("cp.async.commit_group;" ::: "memory");
     };
-    issue();
+#pragma unroll
+    for (int d = 0; d < kPushDepth - 1; ++d)
+        issue();
     int used = 0;
     for (int t = warp; t < nt; t += kRowWarps)
     {
@@ -870,13 +874,13 @@ __global__ void __launch_bounds__(kPushWarps * 32) spgemm_numeric_push_kernel(co
         float acc1[4] = {0.f, 0.f, 0.f, 0.f};
         for (int q = tile_begin(t), qe = sCnt[t]; q < qe; ++q)
         {
-            issue(); // the next product's B tile, into the other slot
-            asm volatile("cp.async.wait_group 1;" ::: "memory");
+            issue(); // kPushDepth - 1 products ahead, into the slot read last
+            asm volatile("cp.async.wait_group %0;" ::"n"(kPushDepth - 1) : "memory");
             __syncwarp();
             const int e = sPep[sOrd[q]] >> 16;
             uint32_t a[4], b[4];
             ldsm4(tile_ldsm_addr(sA_u + e * 512, lane), a);
-            ldsm4_t(tile_ldsm_addr(slots + (used & 1) * 512, lane), b);
+            ldsm4_t(tile_ldsm_addr(slots + (used % kPushDepth) * 512, lane), b);
             ++used;
             for (int r = 0; r < p.num_iter; ++r)
             {

@@ -210,3 +210,16 @@ def test_host_tensors_are_rejected_before_any_launch():
         api.split_f64_gemm(A.double(), A.double())
     with pytest.raises(ValueError, match="CUDA tensors"):
         api._device_index(_FakeCuda(0), A)
+
+
+def test_torch_operator_registers_without_gpu():
+    """torch.ops.kami.bmm (the C++ autograd operator) loads, has the
+    torch.bmm schema, and refuses host tensors (CUDA kernel only)."""
+    import torch
+    from kami_b200 import autograd
+    if not autograd.ops_available():
+        pytest.skip("libkami_torch_ops.so not built")
+    assert str(torch.ops.kami.bmm.default._schema) == "kami::bmm(Tensor a, Tensor b) -> Tensor"
+    A = torch.zeros((1, 8, 8), dtype=torch.float16)
+    with pytest.raises(NotImplementedError):
+        torch.ops.kami.bmm(A, A)

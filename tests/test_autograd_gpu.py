@@ -115,3 +115,23 @@ def test_grads_match_torch_bmm_rectangular_fused(cuda):
     torch.bmm(Af, Bf).backward(G.float())
     for got, ref in [(A.grad, Af.grad), (B.grad, Bf.grad)]:
         assert ((got.float() - ref).abs().max() / ref.abs().max()) <= 2 * 2.0 ** -8
+
+
+def test_default_path_is_the_cpp_operator(cuda):
+    """With the library's kernel choice the step runs through the C++
+    operator torch.ops.kami.bmm (its backward node is the C++ function), and
+    its gradients are the Python function's."""
+    from kami_b200 import autograd
+    assert autograd.ops_available()
+    torch.manual_seed(4)
+    A0 = (torch.rand(64, 64, 64, device="cuda") * 2 - 1).bfloat16()
+    B0 = (torch.rand(64, 64, 64, device="cuda") * 2 - 1).bfloat16()
+    G = (torch.rand(64, 64, 64, device="cuda") * 2 - 1).bfloat16()
+    A, B = A0.clone().requires_grad_(), B0.clone().requires_grad_()
+    C = bmm(A, B)
+    assert "KamiBmmFunction" in C.grad_fn.name()
+    C.backward(G)
+    A2, B2 = A0.clone().requires_grad_(), B0.clone().requires_grad_()
+    C2 = autograd.KamiBmm.apply(A2, B2, "auto", "auto")
+    C2.backward(G)
+    assert torch.equal(C, C2) and torch.equal(A.grad, A2.grad) and torch.equal(B.grad, B2.grad)
