@@ -267,6 +267,12 @@ int kami_gemm_describe(kami_dtype_t in_type, kami_dtype_t out_type,
 #define KAMI_PLAN_MMA_SYNC 2
 #define KAMI_PLAN_TCGEN05 4
 #define KAMI_PLAN_STAGED 8
+/* tcgen05 plans put up to four problems of at most 64 rows and 64 columns
+ * (rounded to 16) in one work item -- their A rows stacked in one 128-row
+ * tile, their B rows in another, C on the accumulator's diagonal -- so one
+ * chain of MMAs and one accumulator hand-off serve them all; this flag
+ * gives every problem its own item. */
+#define KAMI_PLAN_NO_PACK 16
 typedef struct kami_grouped_plan kami_grouped_plan;
 
 int kami_gemm_grouped_plan_create(kami_dtype_t in_type, kami_dtype_t out_type, int count,

@@ -295,7 +295,8 @@ class GroupedPlan:
     when autotuned), "mma_sync", "tcgen05" or "staged" (KAMI_PLAN_MMA_SYNC /
     KAMI_PLAN_TCGEN05 / KAMI_PLAN_STAGED)."""
 
-    def __init__(self, shapes, dtype=torch.float16, out_dtype=None, *, autotune=False, offsets=None, kernel=None):
+    def __init__(self, shapes, dtype=torch.float16, out_dtype=None, *, autotune=False, offsets=None, kernel=None,
+                 pack=True):
         import numpy as np
         sh = np.asarray(shapes, dtype=np.int64).reshape(-1, 3)
         self.count = len(sh)
@@ -316,7 +317,8 @@ class GroupedPlan:
         check(load().kami_gemm_grouped_plan_create(_DT[dtype], _DT[self.out_dtype], self.count,
                                                    M.ctypes.data, N.ctypes.data, K.ctypes.data, ao.ctypes.data,
                                                    bo.ctypes.data, co.ctypes.data,
-                                                   (1 if autotune else 0) | {None: 0, "mma_sync": 2, "tcgen05": 4, "staged": 8}[kernel],
+                                                   (1 if autotune else 0) | (0 if pack else 16)
+                                                   | {None: 0, "mma_sync": 2, "tcgen05": 4, "staged": 8}[kernel],
                                                    ctypes.byref(h)))
         self._h = h
 

@@ -582,7 +582,7 @@ static int free_plan(kami_grouped_plan *pl)
 static int build_plan(int in_type, int out_type, int count, const int *M, const int *N, const int *K,
                       const int64_t *ao, const int64_t *bo, const int64_t *co, const int *cfg,
                       kami_grouped_plan **out, const int *lda = nullptr, const int *ldb = nullptr,
-                      const int *ldc = nullptr, int kernel = 0)
+                      const int *ldc = nullptr, int kernel = 0, bool pack = true)
 {
     int dev = 0, sms = 0, occ = 0;
     cudaError_t e;
@@ -623,20 +623,92 @@ static int build_plan(int in_type, int out_type, int count, const int *M, const 
         order[i] = i;
         pl->flops += (int64_t)fl;
         pl->bytes += (int64_t)by;
-        if (tc)
-            (M[i] <= 64 ? pl->tc_m64 : pl->tc_m128)++;
-        else if (!staged)
+        if (!tc && !staged)
             pl->cfg_hist[cfg[i]]++;
     }
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    // Work items.  tcgen05 plans put several small problems in one item: their
+    // A rows stacked in the item's 128-row A tile, their B rows (each problem's
+    // rounded up to 16) in its 128-row B tile, so that one chain of MMAs computes
+    // every problem's C block on the accumulator's diagonal (the off-diagonal
+    // blocks are computed and never read) and the issuing thread, the loaders
+    // and the epilogue pay their fixed per-item costs once for all of them.
+    // pk[i]: row offset | column offset << 8 | problems in the item << 16.
+    std::vector<std::vector<int>> items;
+    std::vector<int> pk(count, 0);
+    if (tc && pack)
+    {
+        std::vector<int> small;
+        for (int i = 0; i < count; ++i)
+        {
+            if (M[i] <= 64 && ((N[i] + 15) & ~15) <= 64)
+                small.push_back(i);
+            else
+                items.push_back({i});
+        }
+        // similar K together (an item runs to its largest K), then tall first
+        std::stable_sort(small.begin(), small.end(), [&](int a, int b) {
+            return K[a] != K[b] ? K[a] > K[b] : M[a] > M[b];
+        });
+        struct Bin
+        {
+            int item, m, n, k0;
+        };
+        std::vector<Bin> open; // the most recent bins, first fit
+        for (int i : small)
+        {
+            const int n16 = (N[i] + 15) & ~15;
+            bool placed = false;
+            for (Bin &b : open)
+                if (b.m + M[i] <= 128 && b.n + n16 <= 128 && (int)items[b.item].size() < 4 && b.k0 - K[i] <= 32)
+                {
+                    pk[i] = b.m | (b.n << 8);
+                    items[b.item].push_back(i);
+                    b.m += M[i];
+                    b.n += n16;
+                    placed = true;
+                    break;
+                }
+            if (!placed)
+            {
+                items.push_back({i});
+                open.push_back(Bin{(int)items.size() - 1, M[i], n16, K[i]});
+                if (open.size() > 16)
+                    open.erase(open.begin());
+            }
+        }
+        for (const auto &it : items)
+            for (int i : it)
+                pk[i] |= (int)it.size() << 16;
+    }
+    else
+        for (int i : order)
+            items.push_back({i});
+    if (tc)
+        for (const auto &it : items)
+        {
+            int mt = 0;
+            for (int i : it)
+                mt += M[i];
+            (mt <= 64 ? pl->tc_m64 : pl->tc_m128) += (int)it.size();
+        }
+    std::vector<double> icost(items.size(), 2048.0);
+    std::vector<int> iorder(items.size());
+    for (size_t t = 0; t < items.size(); ++t)
+    {
+        for (int i : items[t])
+            icost[t] += cost[i] - 2048.0;
+        iorder[t] = (int)t;
+    }
+    std::stable_sort(iorder.begin(), iorder.end(), [&](int a, int b) { return icost[a] > icost[b]; });
     typedef std::pair<double, int> Load;
     std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
     for (int c = 0; c < ctas; ++c)
         heap.push(Load(0.0, c));
-    std::vector<std::vector<int>> lists(ctas);
+    std::vector<std::vector<int>> lists(ctas); // work items per CTA
     std::vector<int> smalls;
-    for (int i : order)
+    for (int t : iorder)
     {
+        const int i = items[t][0];
         if (cfg[i] == 7 && kernel == 0)
         {
             smalls.push_back(i); // longest first, spread over all warps round-robin
@@ -644,8 +716,8 @@ static int build_plan(int in_type, int out_type, int count, const int *M, const 
         }
         Load l = heap.top();
         heap.pop();
-        lists[l.second].push_back(i);
-        heap.push(Load(l.first + cost[i], l.second));
+        lists[l.second].push_back(t);
+        heap.push(Load(l.first + icost[t], l.second));
     }
     std::vector<GroupedDesc> desc;
     desc.reserve(count);
@@ -653,9 +725,10 @@ static int build_plan(int in_type, int out_type, int count, const int *M, const 
     for (int c = 0; c < ctas; ++c)
     {
         begin[c] = (int)desc.size();
-        for (int i : lists[c])
-            desc.push_back(GroupedDesc{M[i], N[i], K[i], cfg[i], ao[i], bo[i], co[i], lda ? lda[i] : K[i],
-                                       ldb ? ldb[i] : K[i], ldc ? ldc[i] : N[i], 0});
+        for (int t : lists[c])
+            for (int i : items[t])
+                desc.push_back(GroupedDesc{M[i], N[i], K[i], tc ? pk[i] : cfg[i], ao[i], bo[i], co[i],
+                                           lda ? lda[i] : K[i], ldb ? ldb[i] : K[i], ldc ? ldc[i] : N[i], 0});
     }
     begin[ctas] = (int)desc.size();
     pl->small_begin = (int)desc.size();
@@ -808,7 +881,7 @@ int kami_gemm_grouped_plan_create(kami_dtype_t in_type, kami_dtype_t out_type, i
     if (count < 0 || (count > 0 && (!M || !N || !K || !a_offsets || !b_offsets || !c_offsets)))
         return fail(KAMI_ERR_INVALID_VALUE, "grouped: bad count or null shape/offset arrays");
     const bool force_mma = (flags & KAMI_PLAN_MMA_SYNC) != 0, force_tc = (flags & KAMI_PLAN_TCGEN05) != 0,
-               force_st = (flags & KAMI_PLAN_STAGED) != 0;
+               force_st = (flags & KAMI_PLAN_STAGED) != 0, pack = (flags & KAMI_PLAN_NO_PACK) == 0;
     if ((int)force_mma + (int)force_tc + (int)force_st > 1)
         return fail(KAMI_ERR_INVALID_VALUE,
                     "grouped: KAMI_PLAN_MMA_SYNC, KAMI_PLAN_TCGEN05 and KAMI_PLAN_STAGED are exclusive");
@@ -928,14 +1001,14 @@ int kami_gemm_grouped_plan_create(kami_dtype_t in_type, kami_dtype_t out_type, i
         return build_plan(in_type, out_type, count, M, N, K, a_offsets, b_offsets, c_offsets, cfg.data(), plan);
     if (force_tc || force_st || !tune || count == 0)
         return build_plan(in_type, out_type, count, M, N, K, a_offsets, b_offsets, c_offsets, cfg.data(), plan,
-                          nullptr, nullptr, nullptr, alt);
+                          nullptr, nullptr, nullptr, alt, pack);
     // autotuned, kernel not forced: build both kernels' plans, time each on
     // scratch buffers of the plan's extent, keep the faster
     kami_grouped_plan *pl[2] = {nullptr, nullptr};
     for (int k = 0; k < 2; ++k)
     {
         int st = build_plan(in_type, out_type, count, M, N, K, a_offsets, b_offsets, c_offsets, cfg.data(), &pl[k],
-                            nullptr, nullptr, nullptr, k == 0 ? 0 : alt);
+                            nullptr, nullptr, nullptr, k == 0 ? 0 : alt, pack);
         if (st)
         {
             free_plan(pl[0]);

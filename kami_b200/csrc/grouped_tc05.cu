@@ -74,12 +74,20 @@ constexpr int kAccCols = 128;             // TMEM columns of one accumulator (N 
 constexpr int kTmemCols = kAccs * kAccCols;
 constexpr int kBars = 2 * kSlots + 2 * kAccs + 1;
 
-// compact copy of a GroupedDesc for the shared-memory cache
+// compact copy of a GroupedDesc for the shared-memory cache.  pk (the
+// descriptor's cfg field in tcgen05 plans): the problem's row offset in its
+// work item's A tile (bits 0-7), its column offset in the item's B tile and
+// accumulator (bits 8-15, a multiple of 16) and the item's problem count
+// (bits 16-23); the problems of an item are consecutive descriptors.
 struct SDesc
 {
-    int M, N, K, lda, ldb, ldc;
+    int M, N, K, lda, ldb, ldc, pk;
     int64_t a_off, b_off, c_off;
 };
+__device__ __forceinline__ int pk_m(int pk) { return pk & 0xff; }
+__device__ __forceinline__ int pk_n(int pk) { return (pk >> 8) & 0xff; }
+__device__ __forceinline__ int pk_count(int pk) { return max(1, (pk >> 16) & 0xff); }
+constexpr int kMaxPack = 4; // problems per work item
 constexpr int kDescCache = 256; // descriptors per CTA held in shared memory
 constexpr int kSmem =
     kSlots * kSlotBytes + kEpiWarps * kEpiTileBytes + kDescCache * (int)sizeof(SDesc) + kBars * 8 + 16 + 1024;
@@ -90,7 +98,27 @@ __device__ __forceinline__ SDesc get_desc(const SDesc *cache, const GroupedDesc 
     if (i - begin < kDescCache)
         return cache[i - begin];
     const GroupedDesc d = g[i];
-    return SDesc{d.M, d.N, d.K, d.lda, d.ldb, d.ldc, d.a_off, d.b_off, d.c_off};
+    return SDesc{d.M, d.N, d.K, d.lda, d.ldb, d.ldc, d.cfg, d.a_off, d.b_off, d.c_off};
+}
+
+// extent of the work item starting at descriptor i: rows of A (Mt), rows of
+// B rounded per problem to 16 (Nt), the largest K, and the problem count
+struct Item
+{
+    int n, Mt, Nt, Kt;
+};
+__device__ __forceinline__ Item item_at(const SDesc *cache, const GroupedDesc *g, int begin, int i)
+{
+    const SDesc d0 = get_desc(cache, g, begin, i);
+    Item it{pk_count(d0.pk), 0, 0, 0};
+    for (int t = 0; t < it.n; ++t)
+    {
+        const SDesc d = t ? get_desc(cache, g, begin, i + t) : d0;
+        it.Mt = max(it.Mt, pk_m(d.pk) + d.M);
+        it.Nt = max(it.Nt, pk_n(d.pk) + ((d.N + 15) & ~15));
+        it.Kt = max(it.Kt, d.K);
+    }
+    return it;
 }
 
 struct GtParams
@@ -163,7 +191,7 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_tc05_kernel(const __grid_
     for (int i = threadIdx.x; i < end - begin && i < kDescCache; i += kThreads)
     {
         const GroupedDesc d = p.desc[begin + i];
-        dcache[i] = SDesc{d.M, d.N, d.K, d.lda, d.ldb, d.ldc, d.a_off, d.b_off, d.c_off};
+        dcache[i] = SDesc{d.M, d.N, d.K, d.lda, d.ldb, d.ldc, d.cfg, d.a_off, d.b_off, d.c_off};
     }
     tc::tc_fence_before();
     __syncthreads();
@@ -180,11 +208,31 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_tc05_kernel(const __grid_
         const uint32_t slots = tc::smem_u32(smem);
         int j = 0;
         bool ok = true;
-        for (int i = begin; i < end && ok; ++i)
+        for (int i = begin; i < end && ok;)
         {
-            const SDesc d = get_desc(dcache, p.desc, begin, i);
-            const uint8_t *Ab = A + d.a_off * 2, *Bb = B + d.b_off * 2;
-            for (int k0 = 0; k0 < d.K; k0 += 64, ++j)
+            // the work item's problems: A rows [m0, m1) and B rows [n0, n0 + N)
+            // of the item's tiles belong to problem t
+            const Item itm = item_at(dcache, p.desc, begin, i);
+            int mlo[kMaxPack], m1[kMaxPack], nlo[kMaxPack], nhi[kMaxPack], kk[kMaxPack], lda[kMaxPack],
+                ldb[kMaxPack];
+            int64_t aoff[kMaxPack], boff[kMaxPack];
+#pragma unroll
+            for (int t = 0; t < kMaxPack; ++t)
+                if (t < itm.n)
+                {
+                    const SDesc d = get_desc(dcache, p.desc, begin, i + t);
+                    mlo[t] = pk_m(d.pk);
+                    m1[t] = mlo[t] + d.M;
+                    nlo[t] = pk_n(d.pk);
+                    nhi[t] = nlo[t] + d.N;
+                    kk[t] = d.K;
+                    lda[t] = d.lda;
+                    ldb[t] = d.ldb;
+                    aoff[t] = d.a_off;
+                    boff[t] = d.b_off;
+                }
+            i += itm.n;
+            for (int k0 = 0; k0 < itm.Kt; k0 += 64, ++j)
             {
                 const int s = j % kSlots;
                 if (j >= kSlots && !tc::mbar_wait_bounded(&empty[s], ((j / kSlots) - 1) & 1, limit))
@@ -195,19 +243,27 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_tc05_kernel(const __grid_
                 }
                 const uint32_t sa = slots + s * kSlotBytes, sb = sa + kSlotBytes / 2;
                 // 16-byte chunks per row that the MMAs read: whole k-steps of 16
-                const int kc = ((min(64, d.K - k0) + 15) >> 4) * 2;
+                const int kc = ((min(64, itm.Kt - k0) + 15) >> 4) * 2;
                 const bool live = c < kc;
-                const bool kval = k0 + 8 * c < d.K;
-                for (int row = rsub; row < d.M + d.N; row += kLoaders / 8)
+                for (int row = rsub; row < itm.Mt + itm.Nt; row += kLoaders / 8)
                 {
                     if (!live)
                         break;
-                    const bool isA = row < d.M;
-                    const int r = isA ? row : row - d.M;
-                    const uint8_t *src = isA ? Ab + ((int64_t)r * d.lda + k0 + 8 * c) * 2
-                                             : Bb + ((int64_t)r * d.ldb + k0 + 8 * c) * 2;
+                    const bool isA = row < itm.Mt;
+                    const int r = isA ? row : row - itm.Mt;
+                    // the problem owning this row (members in ascending offsets)
+                    int t = 0;
+#pragma unroll
+                    for (int u = 1; u < kMaxPack; ++u)
+                        if (u < itm.n && (isA ? r >= m1[u - 1] : r >= nlo[u]))
+                            t = u;
+                    if (!isA && r >= nhi[t])
+                        continue; // padding row of a problem's 16-column group: never read
+                    const bool kval = k0 + 8 * c < kk[t];
+                    const uint8_t *src = isA ? A + (aoff[t] + (int64_t)(r - mlo[t]) * lda[t] + k0 + 8 * c) * 2
+                                             : B + (boff[t] + (int64_t)(r - nlo[t]) * ldb[t] + k0 + 8 * c) * 2;
                     const uint32_t dst = (isA ? sa : sb) + r * 128 + ((c ^ (r & 7)) << 4);
-                    cp16(dst, kval ? (const void *)src : (const void *)Ab, kval);
+                    cp16(dst, kval ? (const void *)src : (const void *)A, kval);
                 }
                 // this thread's arrival on full[s] happens when its copies land
                 cp_arrive_on(&full[s]);
@@ -223,9 +279,11 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_tc05_kernel(const __grid_
             const uint32_t slots = tc::smem_u32(smem);
             int j = 0, pi = 0;
             bool ok = true;
-            for (int i = begin; i < end && ok; ++i, ++pi)
+            for (int i = begin; i < end && ok; ++pi)
             {
-                const SDesc d = get_desc(dcache, p.desc, begin, i);
+                const Item itm = item_at(dcache, p.desc, begin, i);
+                i += itm.n;
+                const SDesc d{itm.Mt, itm.Nt, itm.Kt, 0, 0, 0, 0, 0, 0, 0}; // the item as one problem
                 const uint32_t idesc = tc::idesc_f16(BF16, mma_m(d.M), mma_n(d.N));
                 const int b = pi % kAccs;
                 const uint32_t acc = tmem + b * kAccCols;
@@ -279,9 +337,14 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_tc05_kernel(const __grid_
         g.alpha = p.alpha;
         g.beta = p.beta;
         const int osz = p.out_type == KAMI_F32 ? 4 : 2;
-        for (int pi = grp; begin + pi < end; pi += kEpiGroups)
+        int i = begin; // first descriptor of item pi
+        for (int pi = 0; i < end; ++pi)
         {
-            const SDesc d = get_desc(dcache, p.desc, begin, begin + pi);
+            const Item itm = item_at(dcache, p.desc, begin, i);
+            const int i0 = i;
+            i += itm.n;
+            if (pi % kEpiGroups != grp)
+                continue;
             const int b = pi % kAccs;
             // tcgen05.ld is .sync.aligned: the outcome must be warp-uniform
             const bool done = __all_sync(0xffffffffu, tc::mbar_wait_bounded(&accf[b], (pi / kAccs) & 1, limit));
@@ -291,28 +354,35 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_tc05_kernel(const __grid_
                 gt_flag(5);
                 break;
             }
-            g.M = d.M;
-            g.N = d.N;
-            g.ldc = d.ldc;
-            g.c_vec = ((d.ldc & 1) == 0) && ((d.c_off & 1) == 0);
-            g.c_vec4 = ((d.ldc & 3) == 0) && ((d.c_off & 3) == 0);
-            void *Cb = reinterpret_cast<char *>(p.C) + d.c_off * osz;
-            const bool m128 = d.M > 64;
-            const int row_base = m128 ? q * 32 : q * 16;
-            const int bn = mma_n(d.N);
-            if (row_base < d.M)
+            // this warp's band of accumulator rows: 32 rows (M = 128 MMAs) or
+            // 16 (M = 64, rows 16q .. in lanes 32q ..)
+            const bool m128 = itm.Mt > 64;
+            const int row_base = m128 ? q * 32 : q * 16, nrows = m128 ? 32 : 16;
+            for (int t = 0; t < itm.n; ++t)
             {
+                const SDesc d = get_desc(dcache, p.desc, begin, i0 + t);
+                const int m0 = pk_m(d.pk), n0 = pk_n(d.pk);
+                if (m0 >= row_base + nrows || m0 + d.M <= row_base)
+                    continue; // none of this problem's rows in the band
+                g.M = d.M;
+                g.N = d.N;
+                g.ldc = d.ldc;
+                g.c_vec = ((d.ldc & 1) == 0) && ((d.c_off & 1) == 0);
+                g.c_vec4 = ((d.ldc & 3) == 0) && ((d.c_off & 3) == 0);
+                void *Cb = reinterpret_cast<char *>(p.C) + d.c_off * osz;
+                const int bn = mma_n(d.N);
                 for (int c0 = 0; c0 < bn; c0 += 16)
                 {
                     uint32_t v[16];
-                    tc::tmem_ld16(tmem + b * kAccCols + lane_addr + c0, v);
+                    tc::tmem_ld16(tmem + b * kAccCols + lane_addr + n0 + c0, v);
                     tc::tmem_ld_wait();
                     tc::tmem_regs_ready(v);
                     float f[16];
 #pragma unroll
                     for (int e = 0; e < 16; ++e)
                         f[e] = __uint_as_float(v[e]);
-                    store_chunk(g, Cb, f, row_base, m128 ? 32 : 16, c0, T);
+                    // band row lr is the problem's row row_base - m0 + lr
+                    store_chunk(g, Cb, f, row_base - m0, nrows, c0, T);
                 }
             }
             tc::tc_fence_before();

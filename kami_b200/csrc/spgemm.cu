@@ -834,54 +834,83 @@ __global__ void __launch_bounds__(kPushWarps * 32) spgemm_numeric_push_kernel(co
     }
     __syncthreads();
 
-    // ---- multiply: warp w takes tiles w, w + W, ...; kPushDepth B tiles in flight ----
+    // ---- multiply: warp w takes the contiguous tile range [t0, t1), whose
+    //      products are contiguous in sOrd (ascending tile, then k); their
+    //      indices are read 32 at a time, one per lane, and broadcast, so a
+    //      product costs no dependent shared-memory lookups; kPushDepth B
+    //      tiles in flight ----
     const int gq = lane >> 2, tq = lane & 3;
     const uint32_t sA_u = (uint32_t)__cvta_generic_to_shared(sA);
     const uint32_t slots = (uint32_t)__cvta_generic_to_shared(sB + warp * kPushDepth * 512);
     const int swz = tile_swz(lane >> 1, lane & 1);
-    auto tile_begin = [&](int t) { return t ? sCnt[t - 1] : 0; };
-    // issue cursor over the warp's products: tile it, position iq
-    int it = warp, iq = it < nt ? tile_begin(it) : 0;
-    auto settle = [&]() {
-        while (it < nt && iq >= sCnt[it])
-        {
-            it += kRowWarps;
-            if (it < nt)
-                iq = tile_begin(it);
-        }
-    };
-    int issued = 0;
-    auto issue = [&]() {
-        settle();
-        if (it < nt)
-        {
-            const int eb = sPb[sOrd[iq]];
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(slots + (issued % kPushDepth) * 512 + swz),
-                         "l"(p.vb + (int64_t)eb * 256 + lane * 8)
-                         : "memory");
-            ++iq;
-            ++issued;
-        }
-        asm volatile("cp.async.commit_group;" ::: "memory");
-    };
-#pragma unroll
-    for (int d = 0; d < kPushDepth - 1; ++d)
-        issue();
-    int used = 0;
-    for (int t = warp; t < nt; t += kRowWarps)
+    const int t0 = (nt * warp) / kRowWarps, t1 = (nt * (warp + 1)) / kRowWarps;
+    if (t0 < t1)
     {
+        const int q0 = t0 ? sCnt[t0 - 1] : 0, q1 = sCnt[t1 - 1]; // this warp's products
+        // product q's (A entry << 16 | tile) and B entry, for q = base + lane
+        auto load_info = [&](int base, int &pep, int &pb) {
+            const int q = base + lane;
+            pep = 0;
+            pb = 0;
+            if (q < q1)
+            {
+                const int f = sOrd[q];
+                pep = sPep[f];
+                pb = sPb[f];
+            }
+        };
+        int ib = q0, i_pep, i_pb; // issue side: info chunk at ib
+        load_info(ib, i_pep, i_pb);
+        int qi = q0, issued = 0;
+        auto issue = [&]() {
+            if (qi < q1)
+            {
+                if (qi - ib >= 32)
+                {
+                    ib += 32;
+                    load_info(ib, i_pep, i_pb);
+                }
+                const int eb = __shfl_sync(0xffffffffu, i_pb, qi - ib);
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(slots + (issued % kPushDepth) * 512 +
+                                                                                swz),
+                             "l"(p.vb + (int64_t)eb * 256 + lane * 8)
+                             : "memory");
+                ++qi;
+                ++issued;
+            }
+            asm volatile("cp.async.commit_group;" ::: "memory");
+        };
+#pragma unroll
+        for (int d = 0; d < kPushDepth - 1; ++d)
+            issue();
+        int cb = q0, c_pep, c_pb; // consumer side: info chunk at cb
+        load_info(cb, c_pep, c_pb);
         float acc0[4] = {0.f, 0.f, 0.f, 0.f};
         float acc1[4] = {0.f, 0.f, 0.f, 0.f};
-        for (int q = tile_begin(t), qe = sCnt[t]; q < qe; ++q)
+        int tile = t0;
+        for (int qc = q0; qc < q1; ++qc)
         {
             issue(); // kPushDepth - 1 products ahead, into the slot read last
+            if (qc - cb >= 32)
+            {
+                cb += 32;
+                load_info(cb, c_pep, c_pb);
+            }
+            const int pep = __shfl_sync(0xffffffffu, c_pep, qc - cb);
+            const int pt = pep & 0xffff, e = pep >> 16;
+            while (tile < pt) // the previous tile is complete (tiles without products store zeros)
+            {
+                store_c_tile(p, (int64_t)c0 + tile, gq, tq, acc0, acc1);
+#pragma unroll
+                for (int x = 0; x < 4; ++x)
+                    acc0[x] = acc1[x] = 0.f;
+                ++tile;
+            }
             asm volatile("cp.async.wait_group %0;" ::"n"(kPushDepth - 1) : "memory");
             __syncwarp();
-            const int e = sPep[sOrd[q]] >> 16;
             uint32_t a[4], b[4];
             ldsm4(tile_ldsm_addr(sA_u + e * 512, lane), a);
-            ldsm4_t(tile_ldsm_addr(slots + (used % kPushDepth) * 512, lane), b);
-            ++used;
+            ldsm4_t(tile_ldsm_addr(slots + ((qc - q0) % kPushDepth) * 512, lane), b);
             for (int r = 0; r < p.num_iter; ++r)
             {
                 mma16816<BF16>(acc0, a[0], a[1], a[2], a[3], b[0], b[1]);
@@ -889,7 +918,13 @@ __global__ void __launch_bounds__(kPushWarps * 32) spgemm_numeric_push_kernel(co
             }
             __syncwarp(); // every lane's fragments are read before the slot is refilled
         }
-        store_c_tile(p, (int64_t)c0 + t, gq, tq, acc0, acc1);
+        for (; tile < t1; ++tile)
+        {
+            store_c_tile(p, (int64_t)c0 + tile, gq, tq, acc0, acc1);
+#pragma unroll
+            for (int x = 0; x < 4; ++x)
+                acc0[x] = acc1[x] = 0.f;
+        }
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
 }

@@ -276,3 +276,32 @@ def test_grouped_rejects_bad_shapes(cuda):
         api.GroupedPlan([[8, 8, 8]], torch.float64, kernel="tcgen05")
     with pytest.raises(Exception):
         api.GroupedPlan([[8, 8, 8]], torch.float16, kernel="staged")
+
+
+@pytest.mark.parametrize("dtype", [torch.float16, torch.bfloat16])
+@pytest.mark.parametrize("num_iter", [1, 2])
+def test_grouped_tcgen05_packed_items(cuda, dtype, num_iter):
+    """Small problems packed several to a work item (rows stacked in one A
+    tile, 16-column groups of B, C on the accumulator's diagonal) give the
+    oracle's results, as do the same problems unpacked: M, N up to 64 with
+    odd sizes, K that differ inside an item (zero-filled), a single row,
+    M = 64 and M = 128 items, and problems too large to pack between them."""
+    rng = np.random.default_rng(30 + num_iter)
+    shapes = np.stack([rng.choice([1, 8, 16, 17, 24, 33, 40, 64], 500), rng.choice([8, 16, 24, 40, 56, 64], 500),
+                       rng.choice([8, 16, 24, 64, 72, 120, 128], 500)], 1)
+    shapes[::37] = [128, 96, 64]
+    As, Bs, A, B = make_inputs(shapes, dtype, 31)
+    for pack in (True, False):
+        plan = api.GroupedPlan(shapes, dtype, kernel="tcgen05", pack=pack)
+        C = torch.full((plan.sizes[2],), float("nan"), dtype=torch.float32, device="cuda")
+        plan.run(A, B, C, num_iter=num_iter)
+        torch.cuda.synchronize()
+        Ch = C.double().cpu().numpy() / num_iter
+        for i, (m, n, k) in enumerate(plan.shapes):
+            ref = oracle.gemm(As[i][None], Bs[i][None])[0]
+            got = Ch[plan.offsets[2][i]:plan.offsets[2][i] + m * n].reshape(m, n)
+            assert np.array_equal(got, ref), (pack, i, m, n, k)
+    import ctypes
+    from kami_b200 import _lib
+    code = ctypes.c_int(0)
+    assert _lib.load().kami_device_status(ctypes.byref(code)) == 0 and code.value == 0
