@@ -88,9 +88,10 @@ __device__ __forceinline__ int pk_m(int pk) { return pk & 0xff; }
 __device__ __forceinline__ int pk_n(int pk) { return (pk >> 8) & 0xff; }
 __device__ __forceinline__ int pk_count(int pk) { return max(1, (pk >> 16) & 0xff); }
 constexpr int kMaxPack = 4; // problems per work item
-constexpr int kDescCache = 256; // descriptors per CTA held in shared memory
+constexpr int kDescCache = 224; // descriptors per CTA held in shared memory
 constexpr int kSmem =
     kSlots * kSlotBytes + kEpiWarps * kEpiTileBytes + kDescCache * (int)sizeof(SDesc) + kBars * 8 + 16 + 1024;
+static_assert(kSmem <= 232448, "grouped tcgen05 kernel: more than 227 KB of shared memory per CTA");
 
 // descriptor i of the CTA's list: from the cache when it is there
 __device__ __forceinline__ SDesc get_desc(const SDesc *cache, const GroupedDesc *g, int begin, int i)
