@@ -457,9 +457,10 @@ def run_secondary(args):
         count = 20000
         x = np.exp(rng.uniform(np.log(8), np.log(128), (count, 3)))
         shapes = np.clip(8 * np.round(x / 8), 8, 128).astype(np.int64)
-        for dt in (torch.float16, torch.float64):
-            for tune in (False, True):
-                plan = api.GroupedPlan(shapes, dt, autotune=tune)
+        for dt, tune, pack in ((torch.float16, False, True), (torch.float16, False, False),
+                               (torch.float16, True, True), (torch.float64, False, True), (torch.float64, True, True)):
+            if True:
+                plan = api.GroupedPlan(shapes, dt, autotune=tune, pack=pack)
                 info = plan.info()
                 A = torch.rand(plan.sizes[0], device=dev).to(dt)
                 B = torch.rand(plan.sizes[1], device=dev).to(dt)
@@ -472,7 +473,7 @@ def run_secondary(args):
                 ms = _time_ms(gph.replay, W, K_, flush)
                 t = min(ms)
                 _emit({"workload": "uneven", "dtype": str(dt).replace("torch.", ""), "autotune": tune,
-                       "problems": count, "launches_per_step": 1, "cuda_graph": True, "ms": t,
+                       "kernel": info["kernel"], "packed": pack and info["kernel"] == "tcgen05", "problems": count, "launches_per_step": 1, "cuda_graph": True, "ms": t,
                        "tflops": info["flops"] / t / 1e9, "hbm_gbs": info["bytes"] / t / 1e6,
                        "frac_hbm": info["bytes"] / t / 1e6 / peak_bw, "ctas": info["ctas"],
                        "partitions": info["partitions"], "flops": info["flops"], "bytes": info["bytes"]})

@@ -214,8 +214,7 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_tc05_kernel(const __grid_
             // the work item's problems: A rows [m0, m1) and B rows [n0, n0 + N)
             // of the item's tiles belong to problem t
             const Item itm = item_at(dcache, p.desc, begin, i);
-            int mlo[kMaxPack], m1[kMaxPack], nlo[kMaxPack], nhi[kMaxPack], kk[kMaxPack], lda[kMaxPack],
-                ldb[kMaxPack];
+            int mlo[kMaxPack], nlo[kMaxPack], nhi[kMaxPack], kk[kMaxPack], lda[kMaxPack], ldb[kMaxPack];
             int64_t aoff[kMaxPack], boff[kMaxPack];
 #pragma unroll
             for (int t = 0; t < kMaxPack; ++t)
@@ -223,7 +222,6 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_tc05_kernel(const __grid_
                 {
                     const SDesc d = get_desc(dcache, p.desc, begin, i + t);
                     mlo[t] = pk_m(d.pk);
-                    m1[t] = mlo[t] + d.M;
                     nlo[t] = pk_n(d.pk);
                     nhi[t] = nlo[t] + d.N;
                     kk[t] = d.K;
@@ -252,17 +250,24 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_tc05_kernel(const __grid_
                         break;
                     const bool isA = row < itm.Mt;
                     const int r = isA ? row : row - itm.Mt;
-                    // the problem owning this row (members in ascending offsets)
-                    int t = 0;
+                    // the problem owning this row (members in ascending offsets),
+                    // selected with constant indices so the arrays stay in registers
+                    int lo = isA ? mlo[0] : nlo[0], hi = nhi[0], kt = kk[0], ld = isA ? lda[0] : ldb[0];
+                    int64_t off = isA ? aoff[0] : boff[0];
 #pragma unroll
                     for (int u = 1; u < kMaxPack; ++u)
-                        if (u < itm.n && (isA ? r >= m1[u - 1] : r >= nlo[u]))
-                            t = u;
-                    if (!isA && r >= nhi[t])
+                        if (u < itm.n && (isA ? r >= mlo[u] : r >= nlo[u]))
+                        {
+                            lo = isA ? mlo[u] : nlo[u];
+                            hi = nhi[u];
+                            kt = kk[u];
+                            ld = isA ? lda[u] : ldb[u];
+                            off = isA ? aoff[u] : boff[u];
+                        }
+                    if (!isA && r >= hi)
                         continue; // padding row of a problem's 16-column group: never read
-                    const bool kval = k0 + 8 * c < kk[t];
-                    const uint8_t *src = isA ? A + (aoff[t] + (int64_t)(r - mlo[t]) * lda[t] + k0 + 8 * c) * 2
-                                             : B + (boff[t] + (int64_t)(r - nlo[t]) * ldb[t] + k0 + 8 * c) * 2;
+                    const bool kval = k0 + 8 * c < kt;
+                    const uint8_t *src = (isA ? A : B) + (off + (int64_t)(r - lo) * ld + k0 + 8 * c) * 2;
                     const uint32_t dst = (isA ? sa : sb) + r * 128 + ((c ^ (r & 7)) << 4);
                     cp16(dst, kval ? (const void *)src : (const void *)A, kval);
                 }
