@@ -9,7 +9,8 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libkami_b200.so")
+# $KAMI_B200_LIB selects another build of the library (A/B timing of kernel variants)
+LIB_PATH = os.environ.get("KAMI_B200_LIB") or os.path.join(HERE, "libkami_b200.so")
 
 # enums of include/kami.h
 KAMI_OK = 0

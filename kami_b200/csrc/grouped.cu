@@ -726,9 +726,21 @@ static int build_plan(int in_type, int out_type, int count, const int *M, const 
     {
         begin[c] = (int)desc.size();
         for (int t : lists[c])
+        {
+            // tcgen05 plans: the item's extent in every member (see item_at in
+            // grouped_tc05.cu): count | Mt << 3 | (Nt / 16) << 11 | Kt << 15
+            int mt = 0, nt = 0, kt = 0;
+            for (int i : items[t])
+            {
+                mt = std::max(mt, (pk[i] & 0xff) + M[i]);
+                nt = std::max(nt, ((pk[i] >> 8) & 0xff) + ((N[i] + 15) & ~15));
+                kt = std::max(kt, K[i]);
+            }
+            const int ext = tc ? (int)items[t].size() | (mt << 3) | ((nt / 16) << 11) | (kt << 15) : 0;
             for (int i : items[t])
                 desc.push_back(GroupedDesc{M[i], N[i], K[i], tc ? pk[i] : cfg[i], ao[i], bo[i], co[i],
-                                           lda ? lda[i] : K[i], ldb ? ldb[i] : K[i], ldc ? ldc[i] : N[i], 0});
+                                           lda ? lda[i] : K[i], ldb ? ldb[i] : K[i], ldc ? ldc[i] : N[i], ext});
+        }
     }
     begin[ctas] = (int)desc.size();
     pl->small_begin = (int)desc.size();

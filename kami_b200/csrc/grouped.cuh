@@ -13,7 +13,8 @@ struct GroupedDesc
 {
     int M, N, K, cfg;
     int64_t a_off, b_off, c_off;
-    int lda, ldb, ldc, pad_;
+    int lda, ldb, ldc;
+    int ext; // tcgen05 plans: extent of the work item this problem belongs to (grouped_tc05.cu, item_at)
 };
 
 struct GroupedParams

@@ -81,7 +81,7 @@ constexpr int kBars = 2 * kSlots + 2 * kAccs + 1;
 // (bits 16-23); the problems of an item are consecutive descriptors.
 struct SDesc
 {
-    int M, N, K, lda, ldb, ldc, pk;
+    int M, N, K, lda, ldb, ldc, pk, it; // it: the item's extent (see item_at)
     int64_t a_off, b_off, c_off;
 };
 __device__ __forceinline__ int pk_m(int pk) { return pk & 0xff; }
@@ -99,27 +99,21 @@ __device__ __forceinline__ SDesc get_desc(const SDesc *cache, const GroupedDesc 
     if (i - begin < kDescCache)
         return cache[i - begin];
     const GroupedDesc d = g[i];
-    return SDesc{d.M, d.N, d.K, d.lda, d.ldb, d.ldc, d.cfg, d.a_off, d.b_off, d.c_off};
+    return SDesc{d.M, d.N, d.K, d.lda, d.ldb, d.ldc, d.cfg, d.ext, d.a_off, d.b_off, d.c_off};
 }
 
-// extent of the work item starting at descriptor i: rows of A (Mt), rows of
-// B rounded per problem to 16 (Nt), the largest K, and the problem count
+// extent of the work item starting at descriptor i, precomputed by the plan
+// in every member's descriptor (GroupedDesc::ext = n | Mt << 3 | (Nt / 16)
+// << 11 | Kt << 15): its problem count, rows of A (Mt), rows of B with each
+// problem's rounded up to 16 (Nt) and its largest K
 struct Item
 {
     int n, Mt, Nt, Kt;
 };
 __device__ __forceinline__ Item item_at(const SDesc *cache, const GroupedDesc *g, int begin, int i)
 {
-    const SDesc d0 = get_desc(cache, g, begin, i);
-    Item it{pk_count(d0.pk), 0, 0, 0};
-    for (int t = 0; t < it.n; ++t)
-    {
-        const SDesc d = t ? get_desc(cache, g, begin, i + t) : d0;
-        it.Mt = max(it.Mt, pk_m(d.pk) + d.M);
-        it.Nt = max(it.Nt, pk_n(d.pk) + ((d.N + 15) & ~15));
-        it.Kt = max(it.Kt, d.K);
-    }
-    return it;
+    const int v = i - begin < kDescCache ? cache[i - begin].it : g[i].ext;
+    return Item{max(1, v & 7), (v >> 3) & 0xff, ((v >> 11) & 0xf) * 16, (v >> 15) & 0xff};
 }
 
 struct GtParams
@@ -192,7 +186,7 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_tc05_kernel(const __grid_
     for (int i = threadIdx.x; i < end - begin && i < kDescCache; i += kThreads)
     {
         const GroupedDesc d = p.desc[begin + i];
-        dcache[i] = SDesc{d.M, d.N, d.K, d.lda, d.ldb, d.ldc, d.cfg, d.a_off, d.b_off, d.c_off};
+        dcache[i] = SDesc{d.M, d.N, d.K, d.lda, d.ldb, d.ldc, d.cfg, d.ext, d.a_off, d.b_off, d.c_off};
     }
     tc::tc_fence_before();
     __syncthreads();
@@ -244,32 +238,28 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_tc05_kernel(const __grid_
                 // 16-byte chunks per row that the MMAs read: whole k-steps of 16
                 const int kc = ((min(64, itm.Kt - k0) + 15) >> 4) * 2;
                 const bool live = c < kc;
-                for (int row = rsub; row < itm.Mt + itm.Nt; row += kLoaders / 8)
+                // member by member, so each copy's base, leading dimension and
+                // K bound are loop constants; this thread copies chunk c of the
+                // rows r = rsub (mod 16) of every member's A and B rows
+                if (live)
                 {
-                    if (!live)
-                        break;
-                    const bool isA = row < itm.Mt;
-                    const int r = isA ? row : row - itm.Mt;
-                    // the problem owning this row (members in ascending offsets),
-                    // selected with constant indices so the arrays stay in registers
-                    int lo = isA ? mlo[0] : nlo[0], hi = nhi[0], kt = kk[0], ld = isA ? lda[0] : ldb[0];
-                    int64_t off = isA ? aoff[0] : boff[0];
 #pragma unroll
-                    for (int u = 1; u < kMaxPack; ++u)
-                        if (u < itm.n && (isA ? r >= mlo[u] : r >= nlo[u]))
-                        {
-                            lo = isA ? mlo[u] : nlo[u];
-                            hi = nhi[u];
-                            kt = kk[u];
-                            ld = isA ? lda[u] : ldb[u];
-                            off = isA ? aoff[u] : boff[u];
-                        }
-                    if (!isA && r >= hi)
-                        continue; // padding row of a problem's 16-column group: never read
-                    const bool kval = k0 + 8 * c < kt;
-                    const uint8_t *src = (isA ? A : B) + (off + (int64_t)(r - lo) * ld + k0 + 8 * c) * 2;
-                    const uint32_t dst = (isA ? sa : sb) + r * 128 + ((c ^ (r & 7)) << 4);
-                    cp16(dst, kval ? (const void *)src : (const void *)A, kval);
+                    for (int t = 0; t < kMaxPack; ++t)
+                    {
+                        if (t >= itm.n)
+                            break;
+                        const bool kval = k0 + 8 * c < kk[t];
+                        const int a0 = mlo[t], a1 = t + 1 < itm.n ? mlo[t + 1 < kMaxPack ? t + 1 : t] : itm.Mt;
+                        const uint8_t *Ab = A + (aoff[t] + k0 + 8 * c) * 2;
+                        for (int r = a0 + ((rsub - a0) & 15); r < a1; r += kLoaders / 8)
+                            cp16(sa + r * 128 + ((c ^ (r & 7)) << 4),
+                                 kval ? (const void *)(Ab + (int64_t)(r - a0) * lda[t] * 2) : (const void *)A, kval);
+                        const int b0 = nlo[t], b1 = nhi[t]; // rows past N in the 16-row group are never read
+                        const uint8_t *Bb = B + (boff[t] + k0 + 8 * c) * 2;
+                        for (int r = b0 + ((rsub - b0) & 15); r < b1; r += kLoaders / 8)
+                            cp16(sb + r * 128 + ((c ^ (r & 7)) << 4),
+                                 kval ? (const void *)(Bb + (int64_t)(r - b0) * ldb[t] * 2) : (const void *)A, kval);
+                    }
                 }
                 // this thread's arrival on full[s] happens when its copies land
                 cp_arrive_on(&full[s]);
@@ -289,7 +279,7 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_tc05_kernel(const __grid_
             {
                 const Item itm = item_at(dcache, p.desc, begin, i);
                 i += itm.n;
-                const SDesc d{itm.Mt, itm.Nt, itm.Kt, 0, 0, 0, 0, 0, 0, 0}; // the item as one problem
+                const SDesc d{itm.Mt, itm.Nt, itm.Kt, 0, 0, 0, 0, 0, 0, 0, 0}; // the item as one problem
                 const uint32_t idesc = tc::idesc_f16(BF16, mma_m(d.M), mma_n(d.N));
                 const int b = pi % kAccs;
                 const uint32_t acc = tmem + b * kAccCols;
