@@ -465,6 +465,7 @@ struct kami_grouped_plan
     int kernel = 0; // 0: mma.sync warp grids (grouped_kernel), 1: tcgen05 (grouped_tc05_kernel),
                     // 2: staged FP64 DMMA (grouped_f64_kernel)
     int tc_m64 = 0, tc_m128 = 0; // tcgen05 plans: problems on M = 64 / M = 128 MMAs
+    bool packed = false;         // tcgen05 plans: some work item holds several problems
     int small_begin = 0, small_end = 0; // desc range of single-warp problems
     GroupedDesc *d_desc = nullptr;
     int *d_begin = nullptr;
@@ -551,7 +552,7 @@ static int launch_grouped(const kami_grouped_plan *plan, const void *A, const vo
     p.small_begin = plan->small_begin;
     p.small_end = plan->small_end;
     if (plan->kernel == 1)
-        return grouped_tc05_launch(p, plan->in_type == KAMI_BF16, plan->ctas, s);
+        return grouped_tc05_launch(p, plan->in_type == KAMI_BF16, plan->packed, plan->ctas, s);
     if (plan->kernel == 2)
         return grouped_f64s_launch(p, plan->ctas, s);
     void *args[] = {&p};
@@ -591,10 +592,13 @@ static int build_plan(int in_type, int out_type, int count, const int *M, const 
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
         return cuda_fail(e, "cudaDeviceGetAttribute");
     const bool tc = kernel == 1, staged = kernel == 2;
-    const void *fn = tc ? grouped_tc05_fn(in_type == KAMI_BF16) : staged ? grouped_f64s_fn() : grouped_fn(in_type);
+    const void *fn = tc ? grouped_tc05_fn(in_type == KAMI_BF16, false) : staged ? grouped_f64s_fn() : grouped_fn(in_type);
     const int smem = tc ? grouped_tc05_smem() : staged ? grouped_f64s_smem() : grouped_smem(in_type);
     const int threads = tc ? grouped_tc05_threads() : staged ? grouped_f64s_threads() : kThreads;
     if ((e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
+        return cuda_fail(e, "cudaFuncSetAttribute(grouped kernel)");
+    if (tc && (e = cudaFuncSetAttribute(grouped_tc05_fn(in_type == KAMI_BF16, true),
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
         return cuda_fail(e, "cudaFuncSetAttribute(grouped kernel)");
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, smem)) != cudaSuccess)
         return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
@@ -677,8 +681,11 @@ static int build_plan(int in_type, int out_type, int count, const int *M, const 
             }
         }
         for (const auto &it : items)
+        {
             for (int i : it)
                 pk[i] |= (int)it.size() << 16;
+            pl->packed = pl->packed || it.size() > 1;
+        }
     }
     else
         for (int i : order)

@@ -32,10 +32,10 @@ struct GroupedParams
 
 // tcgen05 grouped kernel (grouped_tc05.cu): entry point, launch geometry and
 // the device status of its bounded waits.
-const void *grouped_tc05_fn(bool bf16);
+const void *grouped_tc05_fn(bool bf16, bool packed);
 int grouped_tc05_threads();
 int grouped_tc05_smem();
-int grouped_tc05_launch(const GroupedParams &p, bool bf16, int ctas, cudaStream_t s);
+int grouped_tc05_launch(const GroupedParams &p, bool bf16, bool packed, int ctas, cudaStream_t s);
 int grouped_tc05_read_error(int *flag);
 
 // staged FP64 grouped kernel (grouped_f64.cu)

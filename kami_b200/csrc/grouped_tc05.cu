@@ -143,7 +143,10 @@ __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.a
 __device__ __forceinline__ int mma_m(int M) { return M <= 64 ? 64 : 128; }
 __device__ __forceinline__ int mma_n(int N) { return (N + 15) & ~15; }
 
-template <bool BF16>
+// PACKED: the plan has work items of several problems (each role walks the
+// items); otherwise every item is one problem and the roles index problems
+// directly.
+template <bool BF16, bool PACKED>
 __global__ void __launch_bounds__(kThreads, 1) grouped_tc05_kernel(const __grid_constant__ GtParams gp)
 {
     const GroupedParams &p = gp.p;
@@ -203,6 +206,41 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_tc05_kernel(const __grid_
         const uint32_t slots = tc::smem_u32(smem);
         int j = 0;
         bool ok = true;
+        if constexpr (!PACKED)
+            for (int i = begin; i < end && ok; ++i)
+            {
+                const SDesc d = get_desc(dcache, p.desc, begin, i);
+                const uint8_t *Ab = A + d.a_off * 2, *Bb = B + d.b_off * 2;
+                for (int k0 = 0; k0 < d.K; k0 += 64, ++j)
+                {
+                    const int s = j % kSlots;
+                    if (j >= kSlots && !tc::mbar_wait_bounded(&empty[s], ((j / kSlots) - 1) & 1, limit))
+                    {
+                        gt_flag(1);
+                        ok = false;
+                        break;
+                    }
+                    const uint32_t sa = slots + s * kSlotBytes, sb = sa + kSlotBytes / 2;
+                    // 16-byte chunks per row that the MMAs read: whole k-steps of 16
+                    const int kc = ((min(64, d.K - k0) + 15) >> 4) * 2;
+                    const bool live = c < kc;
+                    const bool kval = k0 + 8 * c < d.K;
+                    for (int row = rsub; row < d.M + d.N; row += kLoaders / 8)
+                    {
+                        if (!live)
+                            break;
+                        const bool isA = row < d.M;
+                        const int r = isA ? row : row - d.M;
+                        const uint8_t *src = isA ? Ab + ((int64_t)r * d.lda + k0 + 8 * c) * 2
+                                                 : Bb + ((int64_t)r * d.ldb + k0 + 8 * c) * 2;
+                        const uint32_t dst = (isA ? sa : sb) + r * 128 + ((c ^ (r & 7)) << 4);
+                        cp16(dst, kval ? (const void *)src : (const void *)Ab, kval);
+                    }
+                    // this thread's arrival on full[s] happens when its copies land
+                    cp_arrive_on(&full[s]);
+                }
+            }
+        else
         for (int i = begin; i < end && ok;)
         {
             // the work item's problems: A rows [m0, m1) and B rows [n0, n0 + N)
@@ -334,13 +372,25 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_tc05_kernel(const __grid_
         g.beta = p.beta;
         const int osz = p.out_type == KAMI_F32 ? 4 : 2;
         int i = begin; // first descriptor of item pi
-        for (int pi = 0; i < end; ++pi)
+        for (int pi = PACKED ? 0 : grp; i < end; pi += PACKED ? 1 : kEpiGroups)
         {
-            const Item itm = item_at(dcache, p.desc, begin, i);
-            const int i0 = i;
-            i += itm.n;
-            if (pi % kEpiGroups != grp)
-                continue;
+            int i0;
+            Item itm;
+            if constexpr (PACKED)
+            {
+                itm = item_at(dcache, p.desc, begin, i);
+                i0 = i;
+                i += itm.n;
+                if (pi % kEpiGroups != grp)
+                    continue;
+            }
+            else
+            {
+                i0 = begin + pi;
+                if (i0 >= end)
+                    break;
+                itm = item_at(dcache, p.desc, begin, i0);
+            }
             const int b = pi % kAccs;
             // tcgen05.ld is .sync.aligned: the outcome must be warp-uniform
             const bool done = __all_sync(0xffffffffu, tc::mbar_wait_bounded(&accf[b], (pi / kAccs) & 1, limit));
@@ -378,7 +428,7 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_tc05_kernel(const __grid_
                     for (int e = 0; e < 16; ++e)
                         f[e] = __uint_as_float(v[e]);
                     // band row lr is the problem's row row_base - m0 + lr
-                    store_chunk(g, Cb, f, row_base - m0, nrows, c0, T);
+                    store_chunk<PACKED>(g, Cb, f, row_base - m0, nrows, c0, T);
                 }
             }
             tc::tc_fence_before();
@@ -399,22 +449,24 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_tc05_kernel(const __grid_
 
 } // namespace
 
-const void *grouped_tc05_fn(bool bf16)
+const void *grouped_tc05_fn(bool bf16, bool packed)
 {
-    return bf16 ? (const void *)&grouped_tc05_kernel<true> : (const void *)&grouped_tc05_kernel<false>;
+    if (packed)
+        return bf16 ? (const void *)&grouped_tc05_kernel<true, true> : (const void *)&grouped_tc05_kernel<false, true>;
+    return bf16 ? (const void *)&grouped_tc05_kernel<true, false> : (const void *)&grouped_tc05_kernel<false, false>;
 }
 
 int grouped_tc05_threads() { return kThreads; }
 
 int grouped_tc05_smem() { return kSmem; }
 
-int grouped_tc05_launch(const GroupedParams &p, bool bf16, int ctas, cudaStream_t s)
+int grouped_tc05_launch(const GroupedParams &p, bool bf16, bool packed, int ctas, cudaStream_t s)
 {
     GtParams gp{};
     gp.p = p;
     gp.timeout_ns = (uint64_t)(2e9 + (double)p.num_iter * 1e6); // generous: a chunk takes microseconds
     void *args[] = {&gp};
-    cudaError_t e = cudaLaunchKernel(grouped_tc05_fn(bf16), dim3(ctas), dim3(kThreads), args, kSmem, s);
+    cudaError_t e = cudaLaunchKernel(grouped_tc05_fn(bf16, packed), dim3(ctas), dim3(kThreads), args, kSmem, s);
     if (e != cudaSuccess)
         return cuda_fail(e, "cudaLaunchKernel(grouped_tc05_kernel)");
     return KAMI_OK;

@@ -67,8 +67,9 @@ __device__ __forceinline__ uint32_t pack2(float x, float y, bool bf)
 
 // f: the calling thread's 16 values of row (row_base + lane), columns
 // c0..c0+15; nrows: rows this warp holds (32, or 16 for M = 64 MMAs).  Rows
-// outside [0, g.M) -- a band that starts before the problem (row_base < 0,
-// several problems in one accumulator) or runs past its end -- are skipped.
+// past g.M are skipped, and with kRowsBelowZero rows below 0 too (a band that
+// starts before the problem: several problems in one accumulator).
+template <bool kRowsBelowZero = false>
 __device__ __forceinline__ void store_chunk(const GemmArgs &g, void *Cb, const float (&f)[16], int row_base,
                                             int nrows, int c0, float *T)
 {
@@ -93,7 +94,7 @@ __device__ __forceinline__ void store_chunk(const GemmArgs &g, void *Cb, const f
             const int r = row_base + lr;
             const int c = c0 + cq;
             const float4 x = *reinterpret_cast<const float4 *>(T + lr * kEpiStride + cq);
-            if (r < 0)
+            if (kRowsBelowZero && r < 0)
                 continue;
             if (plain && r < g.M && c + 3 < g.N)
             {
