@@ -296,7 +296,7 @@ class GroupedPlan:
     KAMI_PLAN_TCGEN05 / KAMI_PLAN_STAGED)."""
 
     def __init__(self, shapes, dtype=torch.float16, out_dtype=None, *, autotune=False, offsets=None, kernel=None,
-                 pack=True):
+                 pack=False):
         import numpy as np
         sh = np.asarray(shapes, dtype=np.int64).reshape(-1, 3)
         self.count = len(sh)
@@ -317,7 +317,7 @@ class GroupedPlan:
         check(load().kami_gemm_grouped_plan_create(_DT[dtype], _DT[self.out_dtype], self.count,
                                                    M.ctypes.data, N.ctypes.data, K.ctypes.data, ao.ctypes.data,
                                                    bo.ctypes.data, co.ctypes.data,
-                                                   (1 if autotune else 0) | (0 if pack else 16)
+                                                   (1 if autotune else 0) | (16 if pack else 0)
                                                    | {None: 0, "mma_sync": 2, "tcgen05": 4, "staged": 8}[kernel],
                                                    ctypes.byref(h)))
         self._h = h

@@ -583,7 +583,7 @@ static int free_plan(kami_grouped_plan *pl)
 static int build_plan(int in_type, int out_type, int count, const int *M, const int *N, const int *K,
                       const int64_t *ao, const int64_t *bo, const int64_t *co, const int *cfg,
                       kami_grouped_plan **out, const int *lda = nullptr, const int *ldb = nullptr,
-                      const int *ldc = nullptr, int kernel = 0, bool pack = true)
+                      const int *ldc = nullptr, int kernel = 0, bool pack = false)
 {
     int dev = 0, sms = 0, occ = 0;
     cudaError_t e;
@@ -900,7 +900,7 @@ int kami_gemm_grouped_plan_create(kami_dtype_t in_type, kami_dtype_t out_type, i
     if (count < 0 || (count > 0 && (!M || !N || !K || !a_offsets || !b_offsets || !c_offsets)))
         return fail(KAMI_ERR_INVALID_VALUE, "grouped: bad count or null shape/offset arrays");
     const bool force_mma = (flags & KAMI_PLAN_MMA_SYNC) != 0, force_tc = (flags & KAMI_PLAN_TCGEN05) != 0,
-               force_st = (flags & KAMI_PLAN_STAGED) != 0, pack = (flags & KAMI_PLAN_NO_PACK) == 0;
+               force_st = (flags & KAMI_PLAN_STAGED) != 0, pack = (flags & KAMI_PLAN_PACK) != 0;
     if ((int)force_mma + (int)force_tc + (int)force_st > 1)
         return fail(KAMI_ERR_INVALID_VALUE,
                     "grouped: KAMI_PLAN_MMA_SYNC, KAMI_PLAN_TCGEN05 and KAMI_PLAN_STAGED are exclusive");
