@@ -65,9 +65,13 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="block",
                     choices=["block", "block-sweep", "fp64", "split", "uneven", "spgemm", "spmm", "bmm",
-                             "comparators", "ksplit"],
+                             "comparators", "ksplit", "case"],
                     help="block (default, the headline line) or one of the other configurations; "
                          "non-default workloads print one JSON line per measured case")
+    ap.add_argument("--case", default="block128",
+                    choices=["block128", "stream128", "fp64-64", "spgemm-numeric", "spgemm-symbolic", "uneven-f16",
+                             "bmm-bf16"],
+                    help="--workload case: run one benchmark case three times, untimed (for profiler captures)")
     return ap.parse_args()
 
 
@@ -347,6 +351,72 @@ def _time_ms(fn, warmup, steps, flush=None):
 
 def _emit(d):
     print(json.dumps(d), flush=True)
+
+
+def run_case(args):
+    """One benchmark case, three times, untimed: the command the profiles under
+    profiles/ were captured with (ncu -k <kernel> -s 2 -c 1 python bench.py
+    --workload case --case <name>)."""
+    import numpy as np
+    import torch
+
+    import oracle
+    from kami_b200 import api
+    from kami_b200.autograd import bmm
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    g = torch.Generator().manual_seed(0)
+    c = args.case
+    if c in ("block128", "stream128"):
+        b = 4 * sms
+        A = (torch.rand((b, 128, 128), generator=g) * 2 - 1).half().to(dev)
+        B = (torch.rand((b, 128, 128), generator=g) * 2 - 1).half().to(dev)
+        C = torch.empty((b, 128, 128), dtype=torch.float32, device=dev)
+        it = args.num_iter if c == "block128" else 1
+        fn = lambda: api.gemm_batched(A, B, C, variant=args.variant, partition=args.partition, num_iter=it)
+    elif c == "fp64-64":
+        A = (torch.rand((8192, 64, 64), generator=g, dtype=torch.float64) * 2 - 1).to(dev)
+        B = (torch.rand((8192, 64, 64), generator=g, dtype=torch.float64) * 2 - 1).to(dev)
+        C = torch.empty((8192, 64, 64), dtype=torch.float64, device=dev)
+        fn = lambda: api.gemm_batched(A, B, C)
+    elif c in ("spgemm-numeric", "spgemm-symbolic"):
+        nb = 1024
+        rpa, cia = oracle.bsr_pattern(nb, nb, 0.01, 1)
+        rpb, cib = oracle.bsr_pattern(nb, nb, 0.01, 2)
+        rng = np.random.default_rng(0)
+        va = torch.tensor(rng.uniform(-1, 1, (len(cia), 16, 16)), dtype=torch.float16, device=dev)
+        vb = torch.tensor(rng.uniform(-1, 1, (len(cib), 16, 16)), dtype=torch.float16, device=dev)
+        Am = api.BSR(torch.tensor(rpa, device=dev), torch.tensor(cia, device=dev), va, nb)
+        Bm = api.BSR(torch.tensor(rpb, device=dev), torch.tensor(cib, device=dev), vb, nb)
+        rpc, nnzc = api.spgemm_symbolic(Am, Bm)
+        cic = api.spgemm_fill_colidx(Am, Bm, rpc, nnzc)
+        vc = torch.empty((nnzc, 16, 16), dtype=torch.float32, device=dev)
+        cap = oracle.spgemm_nnzcub(cia, rpb)
+        variant = args.variant if args.variant in ("mma_sync", "tcgen05") else "auto"
+        fn = (lambda: api.spgemm_numeric(Am, Bm, rpc, cic, C_values=vc, variant=variant)) if c == "spgemm-numeric" \
+            else (lambda: api.spgemm_symbolic_device(Am, Bm, cap))
+    elif c == "uneven-f16":
+        rng = np.random.default_rng(0)
+        x = np.exp(rng.uniform(np.log(8), np.log(128), (20000, 3)))
+        plan = api.GroupedPlan(np.clip(8 * np.round(x / 8), 8, 128).astype(np.int64), torch.float16)
+        A = torch.rand(plan.sizes[0], device=dev).half()
+        B = torch.rand(plan.sizes[1], device=dev).half()
+        C = torch.empty(plan.sizes[2], dtype=torch.float32, device=dev)
+        fn = lambda: plan.run(A, B, C)
+    else:  # bmm-bf16: autograd forward + backward, 4096 x 64^3
+        A = (torch.rand((4096, 64, 64), generator=g) * 2 - 1).bfloat16().to(dev).requires_grad_()
+        B = (torch.rand((4096, 64, 64), generator=g) * 2 - 1).bfloat16().to(dev).requires_grad_()
+        G = (torch.rand((4096, 64, 64), generator=g) * 2 - 1).bfloat16().to(dev)
+
+        def fn():
+            A.grad = B.grad = None
+            bmm(A, B).backward(G)
+    for _ in range(3):
+        fn()
+    torch.cuda.synchronize()
+    print(json.dumps({"workload": "case", "case": c, "done": 3}), flush=True)
 
 
 def run_secondary(args):
@@ -633,9 +703,10 @@ def run_secondary(args):
 
         def pair(name, ours, theirs, flops, by):
             for impl, fn in (("kami_b200", ours), ("cublas", theirs)):
-                t = min(_time_ms(fn, W, K_, flush))
-                _emit({"workload": "comparators", "case": name, "impl": impl, "ms": t, "tflops": flops / t / 1e9,
-                       "hbm_gbs": by / t / 1e6 if by else None})
+                ms = _time_ms(fn, W, K_, flush)
+                t = min(ms)
+                _emit({"workload": "comparators", "case": name, "impl": impl, "ms": t, "ms_mean": statistics.fmean(ms),
+                       "tflops": flops / t / 1e9, "hbm_gbs": by / t / 1e6 if by else None})
 
         sms = torch.cuda.get_device_properties(dev).multi_processor_count
         # CUTLASS's own sm_100a batched GEMM (tcgen05 / TMA / TMEM collectives,
@@ -671,11 +742,12 @@ def run_secondary(args):
 
                 name = f"{str(idt).split('.')[-1]} {n}^3 x {b} streamed, {str(odt).split('.')[-1]} out, B as N x K"
                 for impl, fn in (("kami_b200", lambda: api.gemm_batched(A, B, C1)), ("cutlass_sm100", cutlass_run)):
-                    t = statistics.fmean(_time_ms(fn, W, K_, flush))
+                    ms = _time_ms(fn, W, K_, flush)
+                    t = min(ms)
                     by = b * n * n * (2 + 2 + C1.element_size())
                     _emit({"workload": "comparators", "case": name, "impl": impl, "ms": t,
-                           "tflops": 2.0 * n ** 3 * b / t / 1e9, "hbm_gbs": by / t / 1e6,
-                           "frac_hbm": by / t / 1e6 / peak_bw})
+                           "ms_mean": statistics.fmean(ms), "tflops": 2.0 * n ** 3 * b / t / 1e9,
+                           "hbm_gbs": by / t / 1e6, "frac_hbm": by / t / 1e6 / peak_bw})
                 diff = float((C1.float() - C2.float()).abs().max())
                 _emit({"workload": "comparators", "case": name, "max_abs_diff_kami_vs_cutlass": diff})
         else:
@@ -757,6 +829,9 @@ def run_secondary(args):
 
 def main():
     args = parse()
+    if args.workload == "case":
+        run_case(args)
+        return
     if args.workload != "block":
         run_secondary(args)
         return
