@@ -1161,47 +1161,32 @@ __global__ void __launch_bounds__(128) tc05_bwd_kernel(const __grid_constant__ C
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int M = p.M, N = p.N, K = p.K;
-    // two operand buffers (problem j in buffer j % 2), each dC: N / 64 boxes of
-    // M rows x 128 B, then A: K / 64 boxes of M rows, then B: N / 64 boxes of K rows
-    const size_t tile = (size_t)(M * N + M * K + K * N) * 2;
-    float *epi = reinterpret_cast<float *>(smem + 2 * tile);
+    uint8_t *sG = smem;                          // dC: N / 64 boxes of M rows x 128 B
+    uint8_t *sA = sG + (size_t)M * N * 2;        // A:  K / 64 boxes of M rows
+    uint8_t *sB = sA + (size_t)M * K * 2;        // B:  N / 64 boxes of K rows
+    float *epi = reinterpret_cast<float *>(sB + (size_t)K * N * 2);
     uint64_t *bars = reinterpret_cast<uint64_t *>(reinterpret_cast<uint8_t *>(epi) + 4 * kEpiTileBytes);
-    uint64_t *full = bars;     // [2] a buffer's loads have landed
-    uint64_t *mma = bars + 2;  // the problem's MMAs are complete
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 3);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2);
     int *ok_slot = reinterpret_cast<int *>(tmem_slot + 1);
     const int warp = threadIdx.x >> 5;
-    const int64_t grid = gridDim.x;
-    const int nloc = (int)((p.batch - (int64_t)blockIdx.x + grid - 1) / grid); // problems of this CTA
-
-    // TMA loads of local problem j into buffer j % 2 (one thread)
-    auto issue = [&](int j) {
-        const int prob = (int)(blockIdx.x + (int64_t)j * grid);
-        uint8_t *sG = smem + (size_t)(j & 1) * tile;
-        uint8_t *sA = sG + (size_t)M * N * 2;
-        uint8_t *sB = sA + (size_t)M * K * 2;
-        uint64_t *f = &full[j & 1];
-        tc::mbar_expect_tx(f, (uint32_t)tile);
-        for (int b = 0; b < N / 64; ++b)
-            tc::tma_load_3d(sG + (size_t)b * M * 128, &tmG, f, b * 64, 0, prob);
-        for (int b = 0; b < K / 64; ++b)
-            tc::tma_load_3d(sA + (size_t)b * M * 128, &tmA, f, b * 64, 0, prob);
-        for (int b = 0; b < N / 64; ++b)
-            tc::tma_load_3d(sB + (size_t)b * K * 128, &tmB, f, b * 64, 0, prob);
-    };
+    const int prob = blockIdx.x;
 
     if (threadIdx.x == 0)
     {
-        tc::mbar_init(&full[0], 1);
-        tc::mbar_init(&full[1], 1);
-        tc::mbar_init(mma, 1);
+        tc::mbar_init(&bars[0], 1);
+        tc::mbar_init(&bars[1], 1);
         tc::fence_mbar_init();
         *ok_slot = 1;
         tc::prefetch_tmap(&tmG);
         tc::prefetch_tmap(&tmA);
         tc::prefetch_tmap(&tmB);
-        if (nloc > 0)
-            issue(0);
+        tc::mbar_expect_tx(&bars[0], (uint32_t)((M * N + M * K + K * N) * 2));
+        for (int b = 0; b < N / 64; ++b)
+            tc::tma_load_3d(sG + (size_t)b * M * 128, &tmG, &bars[0], b * 64, 0, prob);
+        for (int b = 0; b < K / 64; ++b)
+            tc::tma_load_3d(sA + (size_t)b * M * 128, &tmA, &bars[0], b * 64, 0, prob);
+        for (int b = 0; b < N / 64; ++b)
+            tc::tma_load_3d(sB + (size_t)b * K * 128, &tmB, &bars[0], b * 64, 0, prob);
     }
     if (warp == 0)
     {
@@ -1213,71 +1198,54 @@ __global__ void __launch_bounds__(128) tc05_bwd_kernel(const __grid_constant__ C
     tc::tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
-    int issued = nloc > 0 ? 1 : 0; // problems whose loads were started (thread 0)
-    int landed = 0;                 // problems whose loads were seen complete (thread 0)
-    for (int j = 0; j < nloc; ++j)
+    if (threadIdx.x == 0)
     {
-        const int prob = (int)(blockIdx.x + (int64_t)j * grid);
-        uint8_t *sG = smem + (size_t)(j & 1) * tile;
-        uint8_t *sA = sG + (size_t)M * N * 2;
-        uint8_t *sB = sA + (size_t)M * K * 2;
-        if (threadIdx.x == 0)
+        if (!tc::mbar_wait_bounded(&bars[0], 0, p.timeout_ns))
         {
-            // the next problem's loads overlap this one's MMAs and epilogue: its
-            // buffer's previous contents (problem j - 1) were last read before
-            // the barrier that ended iteration j - 1
-            if (j + 1 < nloc)
-            {
-                issue(j + 1);
-                issued = j + 2;
-            }
-            if (!tc::mbar_wait_bounded(&full[j & 1], (j >> 1) & 1, p.timeout_ns))
-            {
-                tc05_flag(1);
-                *ok_slot = 0;
-                tc::mbar_arrive(mma);
-            }
-            else
-            {
-                landed = j + 1;
-                tc::tc_fence_after();
-                const uint32_t g0 = tc::smem_u32(sG), a0 = tc::smem_u32(sA), b0 = tc::smem_u32(sB);
-                if (p.dA)
-                {
-                    // dA = dC B^T: K-major operands, k-step of 16 n = +32 B, next
-                    // 64-column box after 4 steps
-                    for (int ks = 0; ks < N / 16; ++ks)
-                    {
-                        const uint32_t ga = g0 + (uint32_t)((ks >> 2) * M * 128 + (ks & 3) * 32);
-                        const uint32_t bb = b0 + (uint32_t)((ks >> 2) * K * 128 + (ks & 3) * 32);
-                        tc::mma_f16_ss(tmem, tc::desc_kmajor_sw128(ga), tc::desc_kmajor_sw128(bb), p.idesc_a,
-                                       ks > 0 ? 1u : 0u);
-                    }
-                }
-                if (p.dB)
-                {
-                    // dB = A^T dC: MN-major operands, k-step of 16 m-rows = +2 KB,
-                    // the next 64-element MN chunk one box (M rows) away
-                    for (int ks = 0; ks < M / 16; ++ks)
-                        tc::mma_f16_ss(tmem + (uint32_t)K,
-                                       tc::desc_mnmajor_sw128(a0 + ks * 2048, (uint32_t)M * 128),
-                                       tc::desc_mnmajor_sw128(g0 + ks * 2048, (uint32_t)M * 128), p.idesc_b,
-                                       ks > 0 ? 1u : 0u);
-                }
-                tc::mma_commit(mma);
-            }
+            tc05_flag(1);
+            *ok_slot = 0;
+            tc::mbar_wait_bounded(&bars[0], 0, p.timeout_ns); // copies still in flight
+            tc::mbar_arrive(&bars[1]);
         }
-        __syncwarp();
+        else
+        {
+            tc::tc_fence_after();
+            const uint32_t g0 = tc::smem_u32(sG), a0 = tc::smem_u32(sA), b0 = tc::smem_u32(sB);
+            if (p.dA)
+            {
+                // dA = dC B^T: K-major operands, k-step of 16 n = +32 B, next
+                // 64-column box after 4 steps
+                for (int ks = 0; ks < N / 16; ++ks)
+                {
+                    const uint32_t ga = g0 + (uint32_t)((ks >> 2) * M * 128 + (ks & 3) * 32);
+                    const uint32_t bb = b0 + (uint32_t)((ks >> 2) * K * 128 + (ks & 3) * 32);
+                    tc::mma_f16_ss(tmem, tc::desc_kmajor_sw128(ga), tc::desc_kmajor_sw128(bb), p.idesc_a,
+                                   ks > 0 ? 1u : 0u);
+                }
+            }
+            if (p.dB)
+            {
+                // dB = A^T dC: MN-major operands, k-step of 16 m-rows = +2 KB,
+                // the next 64-element MN chunk one box (M rows) away
+                for (int ks = 0; ks < M / 16; ++ks)
+                    tc::mma_f16_ss(tmem + (uint32_t)K, tc::desc_mnmajor_sw128(a0 + ks * 2048, (uint32_t)M * 128),
+                                   tc::desc_mnmajor_sw128(g0 + ks * 2048, (uint32_t)M * 128), p.idesc_b,
+                                   ks > 0 ? 1u : 0u);
+            }
+            tc::mma_commit(&bars[1]);
+        }
+    }
+    __syncwarp();
 
-        const bool done_w = __all_sync(0xffffffffu, tc::mbar_wait_bounded(mma, j & 1, p.timeout_ns));
-        tc::tc_fence_after();
-        if (!done_w)
-            tc05_flag(2);
-        // block-uniform outcome: the epilogue below holds block barriers
-        const bool done = __syncthreads_and(done_w);
-        const bool ok = done && *reinterpret_cast<volatile int *>(ok_slot);
-        if (!ok)
-            break;
+    const bool done_w = __all_sync(0xffffffffu, tc::mbar_wait_bounded(&bars[1], 0, p.timeout_ns));
+    tc::tc_fence_after();
+    if (!done_w)
+        tc05_flag(2);
+    // block-uniform outcome: the epilogue below holds a block barrier
+    const bool done = __syncthreads_and(done_w);
+    const bool ok = done && *reinterpret_cast<volatile int *>(ok_slot);
+    if (ok)
+    {
         const uint32_t lane_addr = (uint32_t)(warp * 32) << 16;
         const int osz = p.out_type == KAMI_F32 ? 4 : 2;
         float *T = epi + warp * (kEpiTileBytes / 4);
@@ -1300,17 +1268,17 @@ __global__ void __launch_bounds__(128) tc05_bwd_kernel(const __grid_constant__ C
             void *Cb = reinterpret_cast<char *>(out) + (int64_t)prob * rows * cols * osz;
             const int row_base = rows == 128 ? warp * 32 : warp * 16;
             const int slots = which == 0 ? p.slots_a : p.slots_b;
-            // dB's staging may overlap boxes of another warp's dA stores: every
-            // warp's dA boxes have been read first (each warp waits for its
-            // own stores at the end of its pass)
+            // dB's staging (or transpose tiles) may overlap boxes of another
+            // warp's dA stores: every warp's dA boxes have been read first
+            // (each warp waits for its own stores at the end of its pass)
             if (which == 1 && p.dA && p.slots_a > 0)
                 __syncthreads();
             if (slots > 0)
             {
-                // staged in this problem's dC / A / B tiles, dead after the MMAs
+                // staged in the dC / A / B tiles, dead after the MMAs
                 const BulkOut o{p.out_type, rows, cols, rows, cols, 1, slots};
                 epilogue_bulk(o, which == 0 ? &tmDA : &tmDB, tmem + lane_addr + col0,
-                              sG + (size_t)warp * slots * (rows == 128 ? 32 : 16) * 128, row_base, prob);
+                              smem + (size_t)warp * slots * (rows == 128 ? 32 : 16) * 128, row_base, prob);
                 continue;
             }
             for (int c0 = 0; c0 < cols; c0 += 16)
@@ -1325,17 +1293,7 @@ __global__ void __launch_bounds__(128) tc05_bwd_kernel(const __grid_constant__ C
                 store_chunk(g, Cb, f, row_base, rows == 128 ? 32 : 16, c0, T);
             }
         }
-        // this problem's accumulators are drained and its staging boxes read
-        // before the next problem's MMAs and the loads into this buffer
-        tc::tc_fence_before();
-        __syncthreads();
-        tc::tc_fence_after();
     }
-    // after an early exit, loads may still be landing in shared memory: wait
-    // (bounded) for every started problem's loads before the CTA leaves
-    if (threadIdx.x == 0)
-        for (int j = landed; j < issued; ++j)
-            tc::mbar_wait_bounded(&full[j & 1], (j >> 1) & 1, p.timeout_ns);
     tc::tc_fence_before();
     __syncthreads();
     if (warp == 0)
@@ -1382,12 +1340,10 @@ int tc05_backward_launch(int in_type, int out_type, int M, int N, int K, int64_t
         cols <<= 1;
     p.tmem_cols = cols;
     p.timeout_ns = (uint64_t)(5e8 + (double)(M + N) * 4000.0);
-    // two operand buffers (the next problem's loads in flight), the epilogue
-    // transpose tiles, barriers
-    const size_t smem = (size_t)(M * N + M * K + K * N) * 2 * 2 + 4 * kEpiTileBytes + 64 + 1024;
-    // bulk stores of each gradient, staged in the problem's own operand tiles
+    const size_t smem = (size_t)(M * N + M * K + K * N) * 2 + 4 * kEpiTileBytes + 64 + 1024;
+    // bulk stores of each gradient, staged in the operand and transpose tiles
     CUtensorMap mda = mg, mdb = mg;
-    const int region = (M * N + M * K + K * N) * 2;
+    const int region = (M * N + M * K + K * N) * 2 + 4 * kEpiTileBytes;
     const int bcols = out_type == KAMI_F32 ? 32 : 64;
     if (dA && make_store_map(&mda, out_type, dA, K, M, batch, K, (int64_t)M * K, K, M == 128 ? 32 : 16))
         p.slots_a = std::min(K / bcols, region / (4 * (M == 128 ? 32 : 16) * 128));
@@ -1401,17 +1357,8 @@ int tc05_backward_launch(int in_type, int out_type, int M, int N, int K, int64_t
     });
     if (e != cudaSuccess)
         return cuda_fail(e, "cudaFuncSetAttribute(tc05_bwd_kernel)");
-    // persistent: as many CTAs as stay resident (shared memory and tensor-memory
-    // columns), each walking problems blockIdx.x, + grid, ...
-    int dev = 0, sms = 0, occ = 0;
-    if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
-        (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
-        (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 128, smem)) != cudaSuccess)
-        return cuda_fail(e, "tc05_bwd_kernel occupancy");
-    occ = std::max(1, std::min(occ, 512 / (int)cols));
-    const int64_t grid = std::min<int64_t>(batch, (int64_t)sms * occ);
     void *args[] = {&mg, &ma, &mb, &mda, &mdb, &p};
-    e = cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(128), args, smem, stream);
+    e = cudaLaunchKernel(fn, dim3((unsigned)batch), dim3(128), args, smem, stream);
     if (e != cudaSuccess)
         return cuda_fail(e, "cudaLaunchKernel(tc05_bwd_kernel)");
     return KAMI_OK;
