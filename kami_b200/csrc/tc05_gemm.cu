@@ -421,6 +421,8 @@ struct Tc05StreamParams
     int tma_store;   // C written by bulk tensor stores (plain stores only)
     int store_bufs;  // staging boxes per epilogue warp (1 or 2)
     int issuers;     // MMA-issuing threads (2 only with even stages and naccs)
+    int pair;        // 64 x 64 problems two per unit: A rows and B rows of problems 2u, 2u + 1
+                     // stacked in one 128 x 128 MMA tile, C on the accumulator's diagonal
 };
 
 constexpr int kStoreBoxBytes = 4096; // one staging box: up to 32 rows x 128 bytes
@@ -451,11 +453,30 @@ __global__ void __launch_bounds__(96 + 128 * kStreamMaxGroups, 1) tc05_stream_ke
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tempty + NA);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // work units: problems, or with sp.pair problem pairs (2u, 2u + 1)
     const int64_t nprob = g.batch;
-    // one problem's A and B into slot st (the producer thread)
+    const int64_t nunit = sp.pair ? (nprob + 1) / 2 : nprob;
+    // one unit's A and B into slot st (the producer thread)
     auto load_slot = [&](int st, int64_t prob) {
         uint8_t *sA = smem + (size_t)st * sp.stage_bytes;
         uint8_t *sB = sA + p.nkb * a_box;
+        if (sp.pair)
+        {
+            // problem 2u + q: its 64 A rows (or MN chunk) and 64 B rows (or MN
+            // chunk) at +q * 8 KB inside every 64-element K box
+            const int nq = 2 * prob + 1 < nprob ? 2 : 1;
+            tc::mbar_expect_tx(&full[st], (uint32_t)(sp.stage_bytes / 2 * nq));
+            for (int q = 0; q < nq; ++q)
+                for (int kb = 0; kb < p.nkb; ++kb)
+                {
+                    const int pr = (int)(2 * prob + q);
+                    tc::tma_load_3d(sA + kb * a_box + q * 8192, &tmA, &full[st], p.a_mn ? 0 : kb * 64,
+                                    p.a_mn ? kb * 64 : 0, pr);
+                    tc::tma_load_3d(sB + kb * b_box + q * 8192, &tmB, &full[st], p.b_mn ? 0 : kb * 64,
+                                    p.b_mn ? kb * 64 : 0, pr);
+                }
+            return;
+        }
         tc::mbar_expect_tx(&full[st], (uint32_t)sp.stage_bytes);
         for (int kb = 0; kb < p.nkb; ++kb)
         {
@@ -487,7 +508,7 @@ __global__ void __launch_bounds__(96 + 128 * kStreamMaxGroups, 1) tc05_stream_ke
         tc::fence_mbar_init();
         // every slot is free: the first loads start before the TMEM
         // allocation and the block barrier
-        for (int64_t prob = blockIdx.x; prob < nprob && j0 < S; prob += gridDim.x, ++j0)
+        for (int64_t prob = blockIdx.x; prob < nunit && j0 < S; prob += gridDim.x, ++j0)
             load_slot(j0, prob);
     }
     __syncwarp();
@@ -507,7 +528,7 @@ __global__ void __launch_bounds__(96 + 128 * kStreamMaxGroups, 1) tc05_stream_ke
         if (lane == 0)
         {
             int j = j0;
-            for (int64_t prob = blockIdx.x + (int64_t)j0 * gridDim.x; prob < nprob; prob += gridDim.x, ++j)
+            for (int64_t prob = blockIdx.x + (int64_t)j0 * gridDim.x; prob < nunit; prob += gridDim.x, ++j)
             {
                 const int st = j % S;
                 if (j >= S && !tc::mbar_wait_bounded(&empty[st], ((j / S) - 1) & 1, limit))
@@ -530,7 +551,7 @@ __global__ void __launch_bounds__(96 + 128 * kStreamMaxGroups, 1) tc05_stream_ke
         if (lane == 0)
         {
             int j = t;
-            for (int64_t prob = blockIdx.x + (int64_t)t * gridDim.x; prob < nprob;
+            for (int64_t prob = blockIdx.x + (int64_t)t * gridDim.x; prob < nunit;
                  prob += (int64_t)sp.issuers * gridDim.x, j += sp.issuers)
             {
                 const int st = j % S, b = j % NA;
@@ -572,7 +593,12 @@ __global__ void __launch_bounds__(96 + 128 * kStreamMaxGroups, 1) tc05_stream_ke
         // 2, 3, 0, 1
         const int quad = warp & 3;
         const int grp = (warp - 2) >> 2;
-        const int row_base = p.bm == 128 ? quad * 32 : quad * 16;
+        // with pairs, quadrants 0-1 hold problem 2u's rows, 2-3 problem 2u + 1's,
+        // whose columns are the accumulator's 64..127
+        const int pq = sp.pair ? quad >> 1 : 0;
+        const int row_base = sp.pair ? (quad & 1) * 32 : p.bm == 128 ? quad * 32 : quad * 16;
+        const int ucols = sp.pair ? 64 : p.bn;     // accumulator columns of this warp's problem
+        const uint32_t ucol0 = (uint32_t)(pq * 64); // and the first of them
         const uint32_t lane_addr = (uint32_t)(quad * 32) << 16;
         const int osz = g.out_type == KAMI_F32 ? 4 : 2;
         float *T = epi + (warp - 2) * (kEpiTileBytes / 4);
@@ -584,9 +610,10 @@ __global__ void __launch_bounds__(96 + 128 * kStreamMaxGroups, 1) tc05_stream_ke
             const bool f32 = g.out_type == KAMI_F32, bf = g.out_type == KAMI_BF16;
             uint8_t *stg = epi_base + (size_t)(warp - 2) * sp.store_bufs * kStoreBoxBytes;
             int nb = 0;
-            for (int64_t prob = blockIdx.x + (int64_t)grp * gridDim.x; prob < nprob;
-                 prob += (int64_t)G * gridDim.x, j += G)
+            for (int64_t unit = blockIdx.x + (int64_t)grp * gridDim.x; unit < nunit;
+                 unit += (int64_t)G * gridDim.x, j += G)
             {
+                const int64_t prob = sp.pair ? 2 * unit + pq : unit;
                 const int b = j % NA;
                 const bool ok = __all_sync(0xffffffffu, tc::mbar_wait_bounded(&tfull[b], (j / NA) & 1, limit));
                 if (!ok)
@@ -595,7 +622,7 @@ __global__ void __launch_bounds__(96 + 128 * kStreamMaxGroups, 1) tc05_stream_ke
                     break;
                 }
                 tc::tc_fence_after();
-                for (int c0 = 0; c0 < p.bn; c0 += bcols)
+                for (int c0 = 0; c0 < ucols; c0 += bcols)
                 {
                     // this thread's 128 bytes of row (row_base + lane), columns c0..c0+bcols-1
                     uint32_t w[32];
@@ -603,7 +630,7 @@ __global__ void __launch_bounds__(96 + 128 * kStreamMaxGroups, 1) tc05_stream_ke
                     for (int h = 0; h < 2; ++h)
                     {
                         uint32_t v[16], u[16];
-                        const uint32_t col = tmem + lane_addr + (uint32_t)(b * p.bn + c0);
+                        const uint32_t col = tmem + lane_addr + (uint32_t)(b * p.bn + c0) + ucol0;
                         if (f32)
                         {
                             tc::tmem_ld16(col + 16 * h, v);
@@ -625,7 +652,7 @@ __global__ void __launch_bounds__(96 + 128 * kStreamMaxGroups, 1) tc05_stream_ke
                             }
                         }
                     }
-                    if (c0 + bcols >= p.bn)
+                    if (c0 + bcols >= ucols)
                     {
                         // the accumulator's last columns are in registers: free it
                         tc::tc_fence_before();
@@ -654,7 +681,7 @@ __global__ void __launch_bounds__(96 + 128 * kStreamMaxGroups, 1) tc05_stream_ke
                     __syncwarp();
                     if (lane == 0)
                     {
-                        if (row_base < g.M && c0 < g.N)
+                        if (row_base < g.M && c0 < g.N && prob < nprob)
                             tc::tma_store_3d(&tmC, box, c0, row_base, (int)prob);
                         tc::bulk_commit();
                     }
@@ -665,9 +692,10 @@ __global__ void __launch_bounds__(96 + 128 * kStreamMaxGroups, 1) tc05_stream_ke
                 tc::bulk_wait_all();
         }
         else
-        for (int64_t prob = blockIdx.x + (int64_t)grp * gridDim.x; prob < nprob;
-             prob += (int64_t)G * gridDim.x, j += G)
+        for (int64_t unit = blockIdx.x + (int64_t)grp * gridDim.x; unit < nunit;
+             unit += (int64_t)G * gridDim.x, j += G)
         {
+            const int64_t prob = sp.pair ? 2 * unit + pq : unit;
             const int b = j % NA;
             const bool ok = __all_sync(0xffffffffu, tc::mbar_wait_bounded(&tfull[b], (j / NA) & 1, limit));
             if (!ok)
@@ -677,16 +705,17 @@ __global__ void __launch_bounds__(96 + 128 * kStreamMaxGroups, 1) tc05_stream_ke
             }
             tc::tc_fence_after();
             void *Cb = reinterpret_cast<char *>(g.C) + prob * g.sC * osz;
-            for (int c0 = 0; c0 < p.bn; c0 += 16)
+            for (int c0 = 0; c0 < ucols; c0 += 16)
             {
                 uint32_t v[16];
-                tc::tmem_ld16(tmem + lane_addr + (uint32_t)(b * p.bn + c0), v);
+                tc::tmem_ld16(tmem + lane_addr + (uint32_t)(b * p.bn + c0) + ucol0, v);
                 tc::tmem_ld_wait();
                 float f[16];
 #pragma unroll
                 for (int e = 0; e < 16; ++e)
                     f[e] = __uint_as_float(v[e]);
-                store_chunk(g, Cb, f, row_base, p.bm == 128 ? 32 : 16, c0, T);
+                if (prob < nprob)
+                    store_chunk(g, Cb, f, row_base, p.bm == 128 ? 32 : 16, c0, T);
             }
             tc::tc_fence_before();
             __syncwarp();
@@ -974,9 +1003,19 @@ static bool make_c_map(CUtensorMap *map, const GemmArgs &g, int bn, int box_rows
 // accumulators are both even; need_two: launch nothing (KAMI_ERR_UNSUPPORTED,
 // no message) when that layout is not possible.
 static int stream_launch(CUtensorMap &ma, CUtensorMap &mb, Tc05Params &p, bool bf16, cudaStream_t stream,
-                         bool need_two)
+                         bool need_two, bool pair = false)
 {
     Tc05StreamParams sp{};
+    if (pair)
+    {
+        // two 64 x 64 problems per unit: one M = 128, N = 128 MMA chain whose
+        // diagonal 64 x 64 blocks are the two C (the off-diagonal blocks cost
+        // tensor time the streamed regime has to spare and are never read)
+        p.bm = 128;
+        p.bn = 128;
+        p.idesc = tc::idesc_f16(bf16, 128, 128, p.a_mn, p.b_mn);
+        sp.pair = 1;
+    }
     sp.t = p;
     sp.stage_bytes = p.nkb * (p.bm + p.bn) * 128;
     CUtensorMap mc = ma;
@@ -1031,7 +1070,7 @@ static int stream_launch(CUtensorMap &ma, CUtensorMap &mb, Tc05Params &p, bool b
                    [&] { e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024); });
     if (e != cudaSuccess)
         return cuda_fail(e, "cudaFuncSetAttribute(tc05_stream_kernel)");
-    const int64_t grid = std::min<int64_t>(p.g.batch, sms);
+    const int64_t grid = std::min<int64_t>(pair ? (p.g.batch + 1) / 2 : p.g.batch, sms);
     sp.issuers = sp.stage_bytes < 32768 && sp.stages % 2 == 0 && sp.naccs % 2 == 0 ? 2 : 1;
     if (need_two && sp.issuers != 2)
         return KAMI_ERR_UNSUPPORTED; // nothing launched: the caller runs one CTA per problem
@@ -1088,6 +1127,12 @@ int tc05_launch(const GemmArgs &g, int in_type, int partition, int P, void *, si
     // against 31.6 us one CTA per problem, FP16 64^3 x 8192 with FP32 C 51.3
     // against 52.2 us (with one issuer 32.6 and 55.3).
     const int stage_bytes = s.nkb * (s.bm + s.bn) * 128;
+    // 64 x 64 problems stream two to a unit (one 128 x 128 MMA chain, half the
+    // issue, commit and hand-off work per problem)
+    if (s.part == KAMI_PARTITION_1D && !s.a_tmem && g.num_iter <= 4 && s.bm == 64 && s.bn == 64 && g.M == 64 &&
+        g.N == 64 && g.batch >= 2 && 4 * stage_bytes <= 227 * 1024 - 1024 - 512 - 8 * kEpiTileBytes &&
+        !std::getenv("KAMI_STREAM_NO_PAIR"))
+        return stream_launch(ma, mb, p, bf16, stream, false, true);
     if (s.part == KAMI_PARTITION_1D && !s.a_tmem && g.num_iter <= 4 && stage_bytes >= 16384 &&
         2 * stage_bytes <= 227 * 1024 - 1024 - 512 - 8 * kEpiTileBytes)
     {

@@ -236,3 +236,26 @@ def test_tc05_streamed_alpha_beta_many_per_cta(cuda, M, N, K):
     torch.cuda.synchronize()
     _status_clean()
     assert np.array_equal(C.double().cpu().numpy(), 2 * oracle.gemm(A64, B64) - C64)
+
+
+@pytest.mark.parametrize("K", [64, 32, 128, 40])
+@pytest.mark.parametrize("batch", [2, 9, 1201])
+@pytest.mark.parametrize("a_layout,b_layout", [("row_mk", "ref_nk"), ("row_mk", "row_kn"), ("col_mk", "row_kn")])
+@pytest.mark.parametrize("out_dtype", [torch.float32, torch.bfloat16])
+def test_tc05_stream_pairs_exact(cuda, K, batch, a_layout, b_layout, out_dtype):
+    """Streamed 64 x 64 problems run two to a unit (one 128 x 128 MMA chain,
+    C on the accumulator's diagonal): odd batches (a last unit of one problem),
+    K of one, a partial and two K boxes, every operand layout; exact on
+    integer inputs."""
+    rng = np.random.default_rng(batch + K)
+    A = rng.integers(-2, 3, (batch, 64, K)).astype(np.float64)
+    Bt = rng.integers(-2, 3, (batch, K, 64)).astype(np.float64)  # K x N
+    tA = torch.tensor(A, dtype=torch.bfloat16)
+    tA = (tA if a_layout == "row_mk" else tA.transpose(1, 2).contiguous()).cuda()
+    tB = torch.tensor(Bt, dtype=torch.bfloat16)
+    tB = (tB.transpose(1, 2).contiguous() if b_layout == "ref_nk" else tB).cuda()
+    C = api.gemm_batched(tA, tB, a_layout=a_layout, b_layout=b_layout, out_dtype=out_dtype)
+    torch.cuda.synchronize()
+    _status_clean()
+    ref = np.matmul(A, Bt)
+    assert np.array_equal(C.double().cpu().numpy(), torch.tensor(ref).to(out_dtype).double().numpy())
