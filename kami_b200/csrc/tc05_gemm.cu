@@ -1130,8 +1130,7 @@ int tc05_launch(const GemmArgs &g, int in_type, int partition, int P, void *, si
     // 64 x 64 problems stream two to a unit (one 128 x 128 MMA chain, half the
     // issue, commit and hand-off work per problem)
     if (s.part == KAMI_PARTITION_1D && !s.a_tmem && g.num_iter <= 4 && s.bm == 64 && s.bn == 64 && g.M == 64 &&
-        g.N == 64 && g.batch >= 2 && 4 * stage_bytes <= 227 * 1024 - 1024 - 512 - 8 * kEpiTileBytes &&
-        !std::getenv("KAMI_STREAM_NO_PAIR"))
+        g.N == 64 && g.batch >= 2 && 4 * stage_bytes <= 227 * 1024 - 1024 - 512 - 8 * kEpiTileBytes)
         return stream_launch(ma, mb, p, bf16, stream, false, true);
     if (s.part == KAMI_PARTITION_1D && !s.a_tmem && g.num_iter <= 4 && stage_bytes >= 16384 &&
         2 * stage_bytes <= 227 * 1024 - 1024 - 512 - 8 * kEpiTileBytes)
@@ -1193,6 +1192,7 @@ struct Tc05BwdParams
     uint32_t tmem_cols;
     uint64_t timeout_ns;
     int slots_a, slots_b;      // staging boxes per warp for bulk stores of dA / dB (0: per-thread stores)
+    int pair;                  // M = N = K = 64: problems 2c, 2c + 1 in CTA c, stacked in 128-row tiles
 };
 
 template <bool BF16>
@@ -1206,15 +1206,22 @@ __global__ void __launch_bounds__(128) tc05_bwd_kernel(const __grid_constant__ C
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int M = p.M, N = p.N, K = p.K;
-    uint8_t *sG = smem;                          // dC: N / 64 boxes of M rows x 128 B
-    uint8_t *sA = sG + (size_t)M * N * 2;        // A:  K / 64 boxes of M rows
-    uint8_t *sB = sA + (size_t)M * K * 2;        // B:  N / 64 boxes of K rows
-    float *epi = reinterpret_cast<float *>(sB + (size_t)K * N * 2);
+    // with p.pair (64^3): two problems, each region holding problem 0's box
+    // then problem 1's, i.e. 128-row tiles of the stacked problems
+    const int np = p.pair ? 2 : 1;
+    uint8_t *sG = smem;                               // dC: N / 64 boxes of M rows x 128 B (x np)
+    uint8_t *sA = sG + (size_t)np * M * N * 2;        // A:  K / 64 boxes of M rows (x np)
+    uint8_t *sB = sA + (size_t)np * M * K * 2;        // B:  N / 64 boxes of K rows (x np)
+    float *epi = reinterpret_cast<float *>(sB + (size_t)np * K * N * 2);
     uint64_t *bars = reinterpret_cast<uint64_t *>(reinterpret_cast<uint8_t *>(epi) + 4 * kEpiTileBytes);
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2);
     int *ok_slot = reinterpret_cast<int *>(tmem_slot + 1);
     const int warp = threadIdx.x >> 5;
-    const int prob = blockIdx.x;
+    // this warp's problem: with pairs, warps 0-1 hold problem 2c's rows and
+    // warps 2-3 problem 2c + 1's (M = 128 accumulator rows)
+    const int wq = p.pair ? warp >> 1 : 0;
+    const int prob = p.pair ? 2 * blockIdx.x + wq : blockIdx.x;
+    const int nq = p.pair && 2 * (int64_t)blockIdx.x + 1 < p.batch ? 2 : 1; // problems present
 
     if (threadIdx.x == 0)
     {
@@ -1225,13 +1232,18 @@ __global__ void __launch_bounds__(128) tc05_bwd_kernel(const __grid_constant__ C
         tc::prefetch_tmap(&tmG);
         tc::prefetch_tmap(&tmA);
         tc::prefetch_tmap(&tmB);
-        tc::mbar_expect_tx(&bars[0], (uint32_t)((M * N + M * K + K * N) * 2));
-        for (int b = 0; b < N / 64; ++b)
-            tc::tma_load_3d(sG + (size_t)b * M * 128, &tmG, &bars[0], b * 64, 0, prob);
-        for (int b = 0; b < K / 64; ++b)
-            tc::tma_load_3d(sA + (size_t)b * M * 128, &tmA, &bars[0], b * 64, 0, prob);
-        for (int b = 0; b < N / 64; ++b)
-            tc::tma_load_3d(sB + (size_t)b * K * 128, &tmB, &bars[0], b * 64, 0, prob);
+        tc::mbar_expect_tx(&bars[0], (uint32_t)((M * N + M * K + K * N) * 2 * nq));
+        for (int q = 0; q < nq; ++q)
+        {
+            const int pr = (p.pair ? 2 * blockIdx.x : blockIdx.x) + q;
+            const size_t o = (size_t)q * 64 * 128; // pairs: 64^3, one box per operand per problem
+            for (int b = 0; b < N / 64; ++b)
+                tc::tma_load_3d(sG + o + (size_t)b * M * 128, &tmG, &bars[0], b * 64, 0, pr);
+            for (int b = 0; b < K / 64; ++b)
+                tc::tma_load_3d(sA + o + (size_t)b * M * 128, &tmA, &bars[0], b * 64, 0, pr);
+            for (int b = 0; b < N / 64; ++b)
+                tc::tma_load_3d(sB + o + (size_t)b * K * 128, &tmB, &bars[0], b * 64, 0, pr);
+        }
     }
     if (warp == 0)
     {
@@ -1271,9 +1283,10 @@ __global__ void __launch_bounds__(128) tc05_bwd_kernel(const __grid_constant__ C
             if (p.dB)
             {
                 // dB = A^T dC: MN-major operands, k-step of 16 m-rows = +2 KB,
-                // the next 64-element MN chunk one box (M rows) away
+                // the next 64-element MN chunk one box (M rows) away (with
+                // pairs: the other problem's chunk, its own m rows)
                 for (int ks = 0; ks < M / 16; ++ks)
-                    tc::mma_f16_ss(tmem + (uint32_t)K, tc::desc_mnmajor_sw128(a0 + ks * 2048, (uint32_t)M * 128),
+                    tc::mma_f16_ss(tmem + (uint32_t)(np * K), tc::desc_mnmajor_sw128(a0 + ks * 2048, (uint32_t)M * 128),
                                    tc::desc_mnmajor_sw128(g0 + ks * 2048, (uint32_t)M * 128), p.idesc_b,
                                    ks > 0 ? 1u : 0u);
             }
@@ -1300,9 +1313,12 @@ __global__ void __launch_bounds__(128) tc05_bwd_kernel(const __grid_constant__ C
             if (!out)
                 continue;
             const int rows = which == 0 ? M : K, cols = which == 0 ? K : N;
-            const uint32_t col0 = which == 0 ? 0u : (uint32_t)K;
+            // accumulator columns of this warp's problem: dA then dB, each np
+            // problems wide (a pair's diagonal blocks)
+            const uint32_t col0 = (which == 0 ? 0u : (uint32_t)(np * K)) + (uint32_t)(wq * cols);
+            const bool here = wq < nq; // a pair's second problem may be absent
             GemmArgs g{};
-            g.M = rows;
+            g.M = here ? rows : 0;
             g.N = cols;
             g.ldc = cols;
             g.out_type = p.out_type;
@@ -1310,8 +1326,9 @@ __global__ void __launch_bounds__(128) tc05_bwd_kernel(const __grid_constant__ C
             g.c_vec4 = 1;
             g.alpha = 1.0;
             g.beta = 0.0;
-            void *Cb = reinterpret_cast<char *>(out) + (int64_t)prob * rows * cols * osz;
-            const int row_base = rows == 128 ? warp * 32 : warp * 16;
+            void *Cb = reinterpret_cast<char *>(out) + (int64_t)(here ? prob : 0) * rows * cols * osz;
+            const int row_base = p.pair ? (warp & 1) * 32 : rows == 128 ? warp * 32 : warp * 16;
+            const int wrows = p.pair || rows == 128 ? 32 : 16; // accumulator rows this warp holds
             const int slots = which == 0 ? p.slots_a : p.slots_b;
             // dB's staging (or transpose tiles) may overlap boxes of another
             // warp's dA stores: every warp's dA boxes have been read first
@@ -1320,10 +1337,11 @@ __global__ void __launch_bounds__(128) tc05_bwd_kernel(const __grid_constant__ C
                 __syncthreads();
             if (slots > 0)
             {
-                // staged in the dC / A / B tiles, dead after the MMAs
-                const BulkOut o{p.out_type, rows, cols, rows, cols, 1, slots};
+                // staged in the dC / A / B tiles, dead after the MMAs (an absent
+                // problem stages nothing out: rows 0)
+                const BulkOut o{p.out_type, here ? rows : 0, cols, wrows == 32 ? 128 : 64, cols, 1, slots};
                 epilogue_bulk(o, which == 0 ? &tmDA : &tmDB, tmem + lane_addr + col0,
-                              smem + (size_t)warp * slots * (rows == 128 ? 32 : 16) * 128, row_base, prob);
+                              smem + (size_t)warp * slots * wrows * 128, row_base, here ? prob : 0);
                 continue;
             }
             for (int c0 = 0; c0 < cols; c0 += 16)
@@ -1335,7 +1353,7 @@ __global__ void __launch_bounds__(128) tc05_bwd_kernel(const __grid_constant__ C
 #pragma unroll
                 for (int e = 0; e < 16; ++e)
                     f[e] = __uint_as_float(v[e]);
-                store_chunk(g, Cb, f, row_base, rows == 128 ? 32 : 16, c0, T);
+                store_chunk(g, Cb, f, row_base, wrows, c0, T);
             }
         }
     }
@@ -1378,22 +1396,28 @@ int tc05_backward_launch(int in_type, int out_type, int M, int N, int K, int64_t
     p.dA = dA;
     p.dB = dB;
     p.out_type = out_type;
-    p.idesc_a = tc::idesc_f16(bf16, M, K, 0, 0);
-    p.idesc_b = tc::idesc_f16(bf16, K, N, 1, 1);
+    // 64^3 problems two per CTA: both gradients as one 128 x 128 MMA chain each
+    // over the stacked problems, the two C on the accumulators' diagonals (the
+    // off-diagonal blocks cost tensor time this memory-bound pass has to spare)
+    p.pair = M == 64 && N == 64 && K == 64 && batch >= 2;
+    const int np = p.pair ? 2 : 1;
+    p.idesc_a = tc::idesc_f16(bf16, np * M, np * K, 0, 0);
+    p.idesc_b = tc::idesc_f16(bf16, np * K, np * N, 1, 1);
     uint32_t cols = 32;
-    while ((int)cols < K + N)
+    while ((int)cols < np * (K + N))
         cols <<= 1;
     p.tmem_cols = cols;
     p.timeout_ns = (uint64_t)(5e8 + (double)(M + N) * 4000.0);
-    const size_t smem = (size_t)(M * N + M * K + K * N) * 2 + 4 * kEpiTileBytes + 64 + 1024;
+    const size_t smem = (size_t)np * (M * N + M * K + K * N) * 2 + 4 * kEpiTileBytes + 64 + 1024;
     // bulk stores of each gradient, staged in the operand and transpose tiles
     CUtensorMap mda = mg, mdb = mg;
-    const int region = (M * N + M * K + K * N) * 2 + 4 * kEpiTileBytes;
+    const int region = np * (M * N + M * K + K * N) * 2 + 4 * kEpiTileBytes;
     const int bcols = out_type == KAMI_F32 ? 32 : 64;
-    if (dA && make_store_map(&mda, out_type, dA, K, M, batch, K, (int64_t)M * K, K, M == 128 ? 32 : 16))
-        p.slots_a = std::min(K / bcols, region / (4 * (M == 128 ? 32 : 16) * 128));
-    if (dB && make_store_map(&mdb, out_type, dB, N, K, batch, N, (int64_t)K * N, N, K == 128 ? 32 : 16))
-        p.slots_b = std::min(N / bcols, region / (4 * (K == 128 ? 32 : 16) * 128));
+    const int wra = p.pair || M == 128 ? 32 : 16, wrb = p.pair || K == 128 ? 32 : 16; // rows per warp
+    if (dA && make_store_map(&mda, out_type, dA, K, M, batch, K, (int64_t)M * K, K, wra))
+        p.slots_a = std::min(K / bcols, region / (4 * wra * 128));
+    if (dB && make_store_map(&mdb, out_type, dB, N, K, batch, N, (int64_t)K * N, N, wrb))
+        p.slots_b = std::min(N / bcols, region / (4 * wrb * 128));
     const void *fn = bf16 ? (const void *)&tc05_bwd_kernel<true> : (const void *)&tc05_bwd_kernel<false>;
     static std::once_flag once[2];
     cudaError_t e = cudaSuccess;
@@ -1403,7 +1427,7 @@ int tc05_backward_launch(int in_type, int out_type, int M, int N, int K, int64_t
     if (e != cudaSuccess)
         return cuda_fail(e, "cudaFuncSetAttribute(tc05_bwd_kernel)");
     void *args[] = {&mg, &ma, &mb, &mda, &mdb, &p};
-    e = cudaLaunchKernel(fn, dim3((unsigned)batch), dim3(128), args, smem, stream);
+    e = cudaLaunchKernel(fn, dim3((unsigned)(p.pair ? (batch + 1) / 2 : batch)), dim3(128), args, smem, stream);
     if (e != cudaSuccess)
         return cuda_fail(e, "cudaLaunchKernel(tc05_bwd_kernel)");
     return KAMI_OK;

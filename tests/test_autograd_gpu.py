@@ -135,3 +135,24 @@ def test_default_path_is_the_cpp_operator(cuda):
     C2 = autograd.KamiBmm.apply(A2, B2, "auto", "auto")
     C2.backward(G)
     assert torch.equal(C, C2) and torch.equal(A.grad, A2.grad) and torch.equal(B.grad, B2.grad)
+
+
+@pytest.mark.parametrize("batch", [2, 7, 4099])
+@pytest.mark.parametrize("need", [(True, True), (True, False), (False, True)])
+@pytest.mark.parametrize("out_dtype", [torch.float32, torch.bfloat16])
+def test_fused_backward_pairs_exact(cuda, batch, need, out_dtype):
+    """64^3 problems run two per CTA in the fused backward (stacked 128-row
+    tiles, each gradient on a 128 x 128 accumulator's diagonal): odd batches
+    (a last CTA with one problem), either gradient alone; exact on integers."""
+    import numpy as np
+    import oracle
+    from kami_b200 import api
+    A, B, G = _ints((batch, 64, 64), 40 + batch), _ints((batch, 64, 64), 41), _ints((batch, 64, 64), 42)
+    t = lambda x: torch.tensor(x, dtype=torch.bfloat16, device="cuda")
+    dA, dB = api.gemm_backward(t(A), t(B), t(G), need_dA=need[0], need_dB=need[1], out_dtype=out_dtype)
+    rnd = lambda x: torch.tensor(x, dtype=torch.float32).to(out_dtype).double().numpy()
+    if need[0]:
+        assert np.array_equal(dA.double().cpu().numpy(), rnd(oracle.gemm(G, B)))
+    if need[1]:
+        ref = oracle.gemm(np.ascontiguousarray(A.transpose(0, 2, 1)), np.ascontiguousarray(G.transpose(0, 2, 1)))
+        assert np.array_equal(dB.double().cpu().numpy(), rnd(ref))
