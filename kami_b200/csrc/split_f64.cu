@@ -7,8 +7,8 @@
 //      (read from the exponent bits), so every scaled value r satisfies
 //      |r| < 1/2;
 //   2. splitting: each scaled value is rounded to the integer
-//      X = round(r * 2^(beta s)) (built from the mantissa bits with one
-//      shift) and X is written in balanced base 2^beta, least significant
+//      X = round(r * 2^(beta s)) (nearest, ties to even: an exact
+//      power-of-two scaling and one conversion) and X is written in balanced base 2^beta, least significant
 //      digit first: d = ((X + 2^(beta-1)) mod 2^beta) - 2^(beta-1),
 //      X <- (X - d) / 2^beta; the most significant digit d_1 takes what is
 //      left.  So a = 2^eA * sum_p d_p 2^(-beta p) + (at most half a unit of
@@ -34,6 +34,7 @@
 // FP64 arithmetic is used only in step 4; all products run on the tensor
 // cores.  num_iter repeats step 3 on the resident digits (the in-register
 // repeat used to measure the block GEMM).
+#include <cstring>
 #include <mutex>
 
 #include "kami_common.cuh"
@@ -135,59 +136,57 @@ __device__ __forceinline__ uint32_t field_at(uint64_t Y, int lo, uint32_t m, int
     return lo >= up ? (uint32_t)(Y >> (lo - up)) & (m << up) : (uint32_t)(Y << (up - lo)) & (m << up);
 }
 
-// round(x 2^(BS - e)) + H as a uint64 (|x| 2^-e < 1/2, so the rounded value
-// is at most 2^(BS-1) in magnitude and the sum is non-negative).  A normal x
-// is a 53-bit integer m times 2^(be - 1075); its row exponent satisfies
-// e >= be - 1021, so the left shift BS - e + be - 1075 is at most BS - 54 <= 9
-// and one rounding right shift of m 2^10 suffices.  Zero, and subnormal x
-// (rare; only rows whose maximum is tiny), take a slower exact path.
-// round(x 2^(BS - e)) + H as a uint64.  x is an integer m < 2^53 times
-// 2^(E - 1075) (E = the biased exponent, 1 for subnormals), so the value is
-// m 2^sh with sh = E + BS - e - 1075.  With e = floor(log2 max) + G
-// (G = 2 for the 16-bit digits, |x| 2^-e < 1/2 and BS <= 63; G = 3 for the
-// int8 digits, |x| 2^-e < 1/4 and BS <= 64), a normal row maximum gives
-// e >= E - 1023 + G and sh <= BS - 52 - G <= 9: one rounding (half away from
-// zero) right shift of m 2^10 gives the value.  Only rows whose maximum is
-// subnormal reach sh > 9, where the value is m 2^sh exactly.  The result
-// stays below 2^(BS - G + 1) in magnitude; H makes it non-negative.
-template <int BS>
-__device__ __forceinline__ uint64_t offset_fixed(double x, int e, uint64_t H)
+// Power-of-two factors of the fixed-point image: x 2^(BS - e) = (x s.lo) s.hi
+// with s.lo = 2^min(BS - e, 1023) and s.hi = 2^(the rest).  Both products are
+// exact: they only move the exponent, the result stays below 2^62 (no
+// overflow), and a product that lands below the normal range is below 1/2,
+// where any rounding of it still converts to 0.  BS - e >= -1010 (the row
+// exponent is at most 1026), so only rows whose maximum is below about
+// 2^-960 need s.hi != 1.
+struct FixedScale
 {
-    static_assert(BS <= 64, "fixed-point image must fit in 64 bits");
-    const uint64_t u = (uint64_t)__double_as_longlong(x);
-    const int be = (int)(u >> 52) & 0x7FF;
-    const uint64_t m = (u & 0xFFFFFFFFFFFFFull) | ((uint64_t)(be != 0) << 52);
-    const int sh = (be ? be : 1) + BS - e - 1075;
-    uint64_t a;
-    if (sh <= 9)
-    {
-        const int rs = 9 - sh < 63 ? 9 - sh : 63;
-        a = (((m << 10) >> rs) + 1) >> 1;
-    }
-    else
-        a = m << (sh < 63 ? sh : 63);
-    return ((u >> 63) ? (uint64_t)0 - a : a) + H;
+    double lo, hi;
+};
+
+template <int BS>
+__device__ __forceinline__ FixedScale fixed_scale(int e)
+{
+    const int k = BS - e, k1 = k < 1023 ? k : 1023;
+    return {__longlong_as_double((long long)(k1 + 1023) << 52), __longlong_as_double((long long)(k - k1 + 1023) << 52)};
+}
+
+// round(x 2^(BS - e)) + H as a uint64: the exact scaled value, rounded to the
+// nearest integer (ties to even) by one conversion instruction.  With
+// e = floor(log2 max) + G (G = 2 for the 16-bit digits, |x| 2^-e < 1/2 and
+// BS <= 63; G = 3 for the int8 digits, |x| 2^-e < 1/4 and BS <= 64) the
+// rounded value stays below 2^(BS - G + 1) <= 2^62 in magnitude; H makes it
+// non-negative.
+__device__ __forceinline__ uint64_t offset_fixed(double x, FixedScale s, uint64_t H)
+{
+    return (uint64_t)__double2ll_rn((x * s.lo) * s.hi) + H;
 }
 
 // Split 32 values of one operand row (this thread's half of K) into S
 // balanced base-2^beta digits and write digit p (1 = most significant) to
-// tile_row(p).  Eight elements (one 16-byte chunk of each digit tile) at a
+// tile_row(p).  Values 8c..8c+7 of r belong to K group c ^ gx of the
+// row-half (gx = 1 swaps the groups pairwise, as load_row_tiled leaves them).  Eight elements (one 16-byte chunk of each digit tile) at a
 // time: Y = round(x 2^(beta S - e)) + H, then digit p is field S - p of Y
 // minus 2^(beta-1) (the most significant field keeps its carry bit).
 template <int SK, int S, class TileFn>
-__device__ __forceinline__ void split_row(const double (&r)[32], int e, int half, TileFn tile_row)
+__device__ __forceinline__ void split_row(const double (&r)[32], int e, int half, int gx, TileFn tile_row)
 {
     using Code = DigitCode<SK>;
     constexpr int BETA = Code::kBeta, BS = BETA * S;
     constexpr uint64_t H = half_digits<BETA, S>();
     constexpr uint32_t OFF2 = Code::kOff | (Code::kOff << 16);
+    const FixedScale sc = fixed_scale<BS>(e);
 #pragma unroll
     for (int c = 0; c < 4; ++c)
     {
         uint64_t Y[8];
 #pragma unroll
         for (int q = 0; q < 8; ++q)
-            Y[q] = offset_fixed<BS>(r[8 * c + q], e, H);
+            Y[q] = offset_fixed(r[8 * c + q], sc, H);
 #pragma unroll
         for (int k = 0; k < S; ++k)
         {
@@ -200,7 +199,7 @@ __device__ __forceinline__ void split_row(const double (&r)[32], int e, int half
             uint8_t *base;
             int row;
             tile_row(S - k, base, row);
-            *reinterpret_cast<uint4 *>(base + swz(row, half * 4 + c)) = make_uint4(w[0], w[1], w[2], w[3]);
+            *reinterpret_cast<uint4 *>(base + swz(row, half * 4 + (c ^ gx))) = make_uint4(w[0], w[1], w[2], w[3]);
         }
     }
 }
@@ -208,9 +207,9 @@ __device__ __forceinline__ void split_row(const double (&r)[32], int e, int half
 // Load one row-half of an operand into r: `row` of A (is_b = false) or row
 // `row` of the N x K view of B (column `row` of op(B)), K elements
 // [32 half, 32 half + 32), zero outside the problem.  X / ld address the
-// operand in global memory or its staged copy in shared memory (same
-// layout, row stride ld).  Returns the maximum magnitude over the whole row
-// (the two threads of a row are adjacent lanes; one shuffle).
+// operand in global memory (row stride ld).  Returns the maximum magnitude
+// over the whole row (the two threads of a row are adjacent lanes; one
+// shuffle).
 __device__ __forceinline__ double load_row(const SplitParams &p, const double *X, int64_t ld, bool is_b, int row,
                                            int half, double (&r)[32])
 {
@@ -252,6 +251,53 @@ __device__ __forceinline__ double load_row(const SplitParams &p, const double *X
     return fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
 }
 
+// load_row for an operand staged by the tensor copies of the persistent
+// form: its 64 x 64 tile as four boxes of 16 k x 64 rows (8 KB, 128-byte
+// rows; 16-byte chunk c of row r lies at chunk c ^ (r % 8)).  Rows and k
+// outside the problem were zero-filled by the copies, so nothing is checked.
+//   !strided: `row` of the operand, k in [32 half, 32 half + 32): 16 double2
+//             loads.  Half 1 visits its chunks in the order s ^ 4, so the two
+//             threads of a row read different banks; its register pair s then
+//             holds chunk s ^ 4, i.e. its groups of 8 values are swapped
+//             pairwise (split with gx = half).
+//   strided:  B stored K x N (row_kn), boxes of 16 n x 64 k: column `row`
+//             of op(B) is a column of the tile, read in k order.
+// The maximum is a tree of depth 5, not a chain of 16.
+__device__ __forceinline__ double load_row_tiled(const uint8_t *tile, bool strided, int row, int half,
+                                                 double (&r)[32])
+{
+    if (!strided)
+    {
+        const int x = (row & 7) ^ (4 * half);
+        const uint8_t *rb = tile + half * 2 * 8192 + row * 128;
+#pragma unroll
+        for (int s = 0; s < 16; ++s)
+        {
+            const double2 v = *reinterpret_cast<const double2 *>(rb + (s >> 3) * 8192 + (((s & 7) ^ x) << 4));
+            r[2 * s] = v.x;
+            r[2 * s + 1] = v.y;
+        }
+    }
+    else
+    {
+        const uint8_t *cb = tile + (row >> 4) * 8192 + half * 32 * 128 + (row & 1) * 8;
+        const int cn = (row & 15) >> 1;
+#pragma unroll
+        for (int i = 0; i < 32; ++i)
+            r[i] = *reinterpret_cast<const double *>(cb + i * 128 + ((cn ^ (i & 7)) << 4));
+    }
+    double m[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+        m[i] = fmax(fabs(r[2 * i]), fabs(r[2 * i + 1]));
+#pragma unroll
+    for (int w = 8; w >= 1; w >>= 1)
+#pragma unroll
+        for (int i = 0; i < w; ++i)
+            m[i] = fmax(m[i], m[i + w]);
+    return fmax(m[0], __shfl_xor_sync(0xffffffffu, m[0], 1));
+}
+
 // Bytes of four 32-bit words transposed: out[p] = byte p of in[0..3] (in
 // byte order).
 __device__ __forceinline__ void byte_transpose4(const uint32_t (&in)[4], uint32_t (&out)[4])
@@ -269,11 +315,13 @@ __device__ __forceinline__ void byte_transpose4(const uint32_t (&in)[4], uint32_
 // low S bytes of Y ^ H are the S balanced base-256 digits themselves, least
 // significant first (low digits in [-128, 127], the top one within +-65).
 // Digit p (1 = most significant) is byte S - p; eight values (8 bytes of one
-// digit tile row) are transposed and stored at a time.
+// digit tile row, K group c8 ^ gx of the row-half) are transposed and stored
+// at a time.
 template <int S, class TileFn>
-__device__ __forceinline__ void split_row_i8(const double (&r)[32], int e, int half, TileFn tile_row)
+__device__ __forceinline__ void split_row_i8(const double (&r)[32], int e, int half, int gx, TileFn tile_row)
 {
     constexpr uint64_t H = half_digits<8, S - 1>();
+    const FixedScale sc = fixed_scale<8 * S>(e);
 #pragma unroll
     for (int c8 = 0; c8 < 4; ++c8)
     {
@@ -281,7 +329,7 @@ __device__ __forceinline__ void split_row_i8(const double (&r)[32], int e, int h
 #pragma unroll
         for (int q = 0; q < 8; ++q)
         {
-            const uint64_t D = offset_fixed<8 * S>(r[8 * c8 + q], e, H) ^ H;
+            const uint64_t D = offset_fixed(r[8 * c8 + q], sc, H) ^ H;
             lo[q] = (uint32_t)D;
             hi[q] = (uint32_t)(D >> 32);
         }
@@ -294,7 +342,7 @@ __device__ __forceinline__ void split_row_i8(const double (&r)[32], int e, int h
             byte_transpose4(*reinterpret_cast<const uint32_t(*)[4]>(&hi[4]), u1);
         }
         // K index of the first value: 32 half + 8 c8 -> 16-byte chunk and offset
-        const int chunk = half * 2 + (c8 >> 1), off = (c8 & 1) * 8;
+        const int g = c8 ^ gx, chunk = half * 2 + (g >> 1), off = (g & 1) * 8;
 #pragma unroll
         for (int k = 0; k < S; ++k)
         {
@@ -309,10 +357,11 @@ __device__ __forceinline__ void split_row_i8(const double (&r)[32], int e, int h
 
 // Scale and split one loaded row-half (row maximum mx).  Writes the row's
 // exponent (half 0) and its S digits into the digit tiles at `dig` (A: digit
-// p in stack (p-1)/2, row ((p-1)%2)*64 + row; B: digit p in tile p-1).
+// p in stack (p-1)/2, row ((p-1)%2)*64 + row; B: digit p in tile p-1); gx as
+// for split_row.
 template <int SK, int S>
 __device__ __forceinline__ void split_loaded(const double (&r)[32], double mx, int row, int half, uint8_t *dig,
-                                             int *exps)
+                                             int *exps, int gx = 0)
 {
     // e = floor(log2 max) + G, so |x| 2^-e < 2^(1-G): G = 2 keeps every
     // 16-bit digit within 2^(beta-1); G = 3 keeps the top int8 digit within
@@ -340,9 +389,9 @@ __device__ __forceinline__ void split_loaded(const double (&r)[32], double mx, i
         rr = row;
     };
     if constexpr (SK == kSliceI8)
-        split_row_i8<S>(r, e, half, tile_row);
+        split_row_i8<S>(r, e, half, gx, tile_row);
     else
-        split_row<SK, S>(r, e, half, tile_row);
+        split_row<SK, S>(r, e, half, gx, tile_row);
     if constexpr (S & 1)
     {
         // odd digit count: digit S+1 of the last pair is zero (int8 rows use
@@ -372,15 +421,19 @@ __device__ __forceinline__ double pow2(int n)
     return n >= -1074 ? __longlong_as_double(1ll << (n + 1074)) : 0.0;
 }
 
-// v * 2^n for |v| < 2^64 and |n| < 2300.  Exact while the result is normal
-// (a power-of-two factor); a result in the subnormal range may be rounded
-// twice when n < -1022.
+// 2^n as a double for -1022 <= n <= 1023 (a normal power of two)
+__device__ __forceinline__ double pow2n(int n) { return __longlong_as_double((long long)(n + 1023) << 52); }
+
+// v * 2^n for |v| < 2^64 and |n| < 2300, without branches: v 2^n1 2^n2 with
+// n1 = n clamped to the normal exponent range and n2 = the rest clamped the
+// same way (a rest below -1022 arises only where the result is below 2^-1980
+// and rounds to zero either way).  Exact while the result is normal; a result
+// in the subnormal range may be rounded twice when n < -1022.
 __device__ __forceinline__ double scale2(double v, int n)
 {
-    if (n >= -1022 && n <= 1023)
-        return v * pow2(n);
-    const int n1 = n < -1022 ? -1022 : 1023;
-    return v * pow2(n1) * pow2(n - n1 > 1023 ? 1023 : n - n1);
+    const int n1 = min(max(n, -1022), 1023);
+    const int n2 = min(max(n - n1, -1022), 1023);
+    return v * pow2n(n1) * pow2n(n2);
 }
 
 // Row stride (doubles) of the recombination tile for chunks of W columns:
@@ -635,43 +688,42 @@ __global__ void __launch_bounds__(128) split_f64_kernel(const SplitParams p)
 // ---------------------------------------------------------------------------
 // Persistent form for the streamed regime (one launch over all problems, one
 // CTA per SM, 12 warps), so the phases of consecutive problems overlap:
-//   warps 0-7   split: 256 threads, one row-half of A or B each.  With
-//               16-byte aligned rows the inputs of problem j are staged in
-//               shared memory by bulk copies (TMA engine) that the split
-//               warps issued for it while working on problem j-1; once all
-//               eight warps have read problem j out of the stage they issue
-//               the copies of problem j+1, then write the digits of problem
-//               j into buffer j % nbuf once the MMAs of the problem that
-//               last used it have completed;
-//   warps 8-11  recombination of problem j from TMEM (lane quadrants 0-3).
-//               After the last TMEM read of problem j, lane 0 of warp 8
-//               issues the MMAs of problem j+1 (its digits complete), then
-//               the four warps store the last columns of problem j.
+//   warps 0-3   split: 128 threads, one row-half of A and then the same
+//               row-half of B each.  With 16-byte aligned rows the inputs of
+//               problem j are staged in shared memory by eight tensor copies
+//               (TMA engine) that thread 0 issued once the four warps had
+//               read problem j-1 out of the stage; they write the digits of
+//               problem j into buffer j % nbuf once the MMAs of the problem
+//               that last used it have completed;
+//   warps 4-11  recombination of problem j from TMEM: warp w reads lane
+//               quadrant w % 4; warps 4-7 finish output columns 0-31 and
+//               warps 8-11 columns 32-63 (two groups of 128 threads, so two
+//               warps per scheduler hide each other's TMEM and FP64
+//               latencies).  After the last TMEM read of problem j by both
+//               groups, lane 0 of warp 4 issues the MMAs of problem j+1 (its
+//               digits complete), then the groups store their last columns
+//               of problem j.
 // Row and column exponents live in a ring of four entries apart from the
-// digit buffers.  Barriers: sfull (bulk copies, by bytes), dfull[b] (8 split
-// warps), dempty[b] and tfull (MMA commits).
+// digit buffers.  mbarriers: sfull (bulk copies, by bytes), dfull[b] (4 split
+// warps), dempty[b] and tfull (MMA commits).  Named barriers: 2 (split
+// warps), 1 and 3 (one recombination group each), 4 (both groups).
 // Every mbarrier wait is bounded; each warp group agrees on the outcome of
 // its waits with a barrier reduction before acting on it, so a timeout
 // ends the whole group together.
 // ---------------------------------------------------------------------------
-constexpr int kStageLd = 66;                            // staged row stride (doubles): 528 bytes
-constexpr int kStageBytes = 2 * 64 * kStageLd * 8;      // A rows, then B rows
+constexpr int kBoxBytes = 64 * 128;                     // one tensor-copy box: 16 doubles x 64 rows
+constexpr int kStageBytes = 8 * kBoxBytes;              // A's four boxes, then B's
 constexpr int kExpRing = 4;
-
-// Output columns per recombination chunk of the persistent form: 32, except
-// where the 128 KB digit buffer of 7 or 8 digits leaves no room for it.
-template <int S>
-constexpr int persistent_chunk()
-{
-    return S <= 6 ? 32 : 16;
-}
+constexpr int kSplitWarps = 4;
+constexpr int kPersistentW = 16;                        // output columns per recombination chunk
+constexpr int kXferBytes = 2 * 64 * (kPersistentW + 2) * 8; // two groups x 64 rows x xfer_ld<16>()
 
 struct SplitStreamParams
 {
     SplitParams p;
     int nbuf;      // digit buffers (1 or 2)
     int buf_bytes; // digits of A and B of one problem
-    int staged;    // 1: inputs are staged by bulk copies (16-byte aligned rows)
+    int staged;    // 1: inputs are staged by tensor copies (maps tmA / tmB valid)
 };
 
 // AND of `pred` over the `n` threads of named barrier `id` (whole warps)
@@ -686,21 +738,20 @@ __device__ __forceinline__ bool barrier_and(int id, int n, bool pred)
     return out != 0;
 }
 
-// Bulk copies of problem `prob`'s A rows (threads 0..63 of the split group)
-// and B rows (threads 64..127) into the stage; thread 0 first announces the
-// byte count on sfull.
-__device__ __forceinline__ void stage_problem(const SplitParams &p, int64_t prob, int tt, uint8_t *stage,
-                                              uint64_t *sfull)
+// Tensor copies of problem `prob` into the stage (one thread): A's 64 x 64
+// tile as four boxes of 16 k, then B's (16 k of the N x K view, or 16 n of
+// the K x N layout); the copies zero-fill rows and k beyond the problem, so
+// every box carries its full 8 KB.
+__device__ __forceinline__ void stage_problem(const CUtensorMap *tmA, const CUtensorMap *tmB, int64_t prob,
+                                              uint8_t *stage, uint64_t *sfull)
 {
-    const bool refnk = p.b_layout == KAMI_B_REF_NK;
-    const uint32_t a_bytes = (uint32_t)p.K * 8, b_bytes = (uint32_t)(refnk ? p.K : p.N) * 8;
-    const int b_rows = refnk ? p.N : p.K;
-    if (tt == 0)
-        tc::mbar_expect_tx(sfull, (uint32_t)p.M * a_bytes + (uint32_t)b_rows * b_bytes);
-    if (tt < 64 && tt < p.M)
-        tc::bulk_g2s(stage + (size_t)tt * kStageLd * 8, p.A + prob * p.sA + tt * p.lda, a_bytes, sfull);
-    else if (tt >= 64 && tt < 128 && tt - 64 < b_rows)
-        tc::bulk_g2s(stage + (size_t)tt * kStageLd * 8, p.B + prob * p.sB + (tt - 64) * p.ldb, b_bytes, sfull);
+    tc::mbar_expect_tx(sfull, kStageBytes);
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+        tc::tma_load_3d(stage + q * kBoxBytes, tmA, sfull, 16 * q, 0, (int)prob);
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+        tc::tma_load_3d(stage + (4 + q) * kBoxBytes, tmB, sfull, 16 * q, 0, (int)prob);
 }
 
 template <int SK, int S>
@@ -724,8 +775,82 @@ __device__ __forceinline__ void issue_products(const SplitParams &p, uint32_t tm
     tc::mma_commit(tfull);
 }
 
+// Finish the 64 x W chunk j0..j0+W-1 of C from the partial sums of one TMEM
+// lane L (L < 64: the top partial of row L, L >= 64: the bottom partial of
+// row L - 64).  The top thread of row r finishes columns j0..j0+W/2-1 and the
+// bottom thread columns j0+W/2..j0+W-1: each first leaves the half that it
+// does not finish in xfer (64 rows x xfer_ld<W>() doubles), then adds the
+// other thread's half to its own, scales by 2^(eA[r] + eB[col]), applies
+// alpha and beta and stores W/2 consecutive doubles of row r.  Named barrier
+// `bar` over the 128 threads of the group orders xfer.
+template <int W>
+__device__ __forceinline__ void finish_half_chunk(const SplitParams &p, double *Cp, const int *eA, const int *eB,
+                                                  double *xfer, const double (&part)[W], int L, int j0, int bar)
+{
+    constexpr int LD = xfer_ld<W>(), HW = W / 2;
+    const bool top = L < 64;
+    const int r = L & 63;
+    double *xr = xfer + r * LD;
+    named_barrier(bar, 128); // the previous chunk's reads of xfer are done
+#pragma unroll
+    for (int e = 0; e < HW; e += 2)
+    {
+        const double2 v = top ? make_double2(part[HW + e], part[HW + e + 1]) : make_double2(part[e], part[e + 1]);
+        *reinterpret_cast<double2 *>(xr + (top ? HW : 0) + e) = v;
+    }
+    named_barrier(bar, 128);
+    if (r >= p.M)
+        return;
+    const int jb = j0 + (top ? 0 : HW); // first output column this thread finishes
+    const int ea = eA[r];
+    // all shared-memory reads first: HW exponents (16-byte aligned, jb is a
+    // multiple of 8) and the other thread's HW partials
+    int eb[HW];
+#pragma unroll
+    for (int e = 0; e < HW; e += 4)
+        *reinterpret_cast<int4 *>(&eb[e]) = *reinterpret_cast<const int4 *>(eB + jb + e);
+    double o[HW];
+#pragma unroll
+    for (int e = 0; e < HW; e += 2)
+        *reinterpret_cast<double2 *>(&o[e]) = *reinterpret_cast<const double2 *>(xr + (top ? 0 : HW) + e);
+    double v[HW];
+#pragma unroll
+    for (int e = 0; e < HW; ++e)
+        v[e] = p.alpha * scale2((top ? part[e] : part[HW + e]) + o[e], ea + eb[e]);
+    double *dst = Cp + (int64_t)r * p.ldc + jb;
+    if (p.c_vec && jb + HW <= p.N)
+    {
+        if (p.beta_c != 0.0)
+        {
+#pragma unroll
+            for (int e = 0; e < HW; e += 2)
+            {
+                const double2 old = *reinterpret_cast<const double2 *>(dst + e);
+                v[e] += p.beta_c * old.x;
+                v[e + 1] += p.beta_c * old.y;
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < HW; e += 2)
+            *reinterpret_cast<double2 *>(dst + e) = make_double2(v[e], v[e + 1]);
+    }
+    else
+    {
+#pragma unroll
+        for (int e = 0; e < HW; ++e)
+            if (jb + e < p.N)
+            {
+                if (p.beta_c != 0.0)
+                    v[e] += p.beta_c * dst[e];
+                dst[e] = v[e];
+            }
+    }
+}
+
 template <int SK, int S>
-__global__ void __launch_bounds__(384, 1) split_f64_persistent(const SplitStreamParams sp)
+__global__ void __launch_bounds__(384, 1) split_f64_persistent(const SplitStreamParams sp,
+                                                               const __grid_constant__ CUtensorMap tmA,
+                                                               const __grid_constant__ CUtensorMap tmB)
 {
     const SplitParams &p = sp.p;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -733,10 +858,10 @@ __global__ void __launch_bounds__(384, 1) split_f64_persistent(const SplitStream
     // compiler still knows every derived pointer addresses shared memory
     uint8_t *smem = smem_raw + ((1024u - (uint32_t)(reinterpret_cast<uintptr_t>(smem_raw) & 1023u)) & 1023u);
     constexpr int nstack = (S + 1) / 2;
+    constexpr int W = kPersistentW;
     uint8_t *stage = smem + (size_t)sp.nbuf * sp.buf_bytes;
-    constexpr int W = persistent_chunk<S>();
-    double *xfer = reinterpret_cast<double *>(stage + (sp.staged ? kStageBytes : 0)); // 2 x 64 x xfer_ld<W>()
-    int *exps = reinterpret_cast<int *>(xfer + 2 * 64 * xfer_ld<W>());               // kExpRing x 128
+    double *xfer = reinterpret_cast<double *>(stage + (sp.staged ? kStageBytes : 0)); // kXferBytes
+    int *exps = reinterpret_cast<int *>(xfer + kXferBytes / 8);                        // kExpRing x 128
     uint64_t *dfull = reinterpret_cast<uint64_t *>(exps + kExpRing * 128);
     uint64_t *dempty = dfull + 2;
     uint64_t *tfull = dempty + 2;
@@ -750,7 +875,7 @@ __global__ void __launch_bounds__(384, 1) split_f64_persistent(const SplitStream
     {
         for (int i = 0; i < 2; ++i)
         {
-            tc::mbar_init(&dfull[i], 8);
+            tc::mbar_init(&dfull[i], kSplitWarps);
             tc::mbar_init(&dempty[i], 1);
         }
         tc::mbar_init(tfull, 1);
@@ -758,7 +883,7 @@ __global__ void __launch_bounds__(384, 1) split_f64_persistent(const SplitStream
         tc::fence_mbar_init();
     }
     __syncwarp();
-    if (warp == 8)
+    if (warp == kSplitWarps)
     {
         tc::tmem_alloc(tmem_slot, p.tmem_cols);
         tc::tmem_relinquish();
@@ -768,54 +893,71 @@ __global__ void __launch_bounds__(384, 1) split_f64_persistent(const SplitStream
     tc::tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
-    if (warp < 8)
+    if (warp < kSplitWarps)
     {
-        // ---- split role (named barrier 2 over its 256 threads) ----
-        const bool is_b = t >= 128;
-        const int row = (t & 127) >> 1, half = t & 1;
+        // ---- split role (named barrier 2 over its 128 threads) ----
+        const int row = t >> 1, half = t & 1;
+        const bool strided_b = p.b_layout != KAMI_B_REF_NK;
         int issued = 0, consumed = 0; // stage phases started / completed and read
         if (sp.staged && blockIdx.x < nprob)
         {
-            if (t < 128)
-                stage_problem(p, blockIdx.x, t, stage, sfull);
+            if (t == 0)
+                stage_problem(&tmA, &tmB, blockIdx.x, stage, sfull);
             issued = 1;
         }
         int j = 0;
         for (int64_t prob = blockIdx.x; prob < nprob; prob += gridDim.x, ++j)
         {
-            double r[32], mx;
             if (sp.staged)
             {
-                if (!barrier_and(2, 256, tc::mbar_wait_bounded(sfull, j & 1, limit)))
+                if (!barrier_and(2, 128, tc::mbar_wait_bounded(sfull, j & 1, limit)))
                 {
                     atomicExch(&g_split_error, 8);
                     break;
                 }
                 consumed = j + 1;
-                mx = load_row(p, reinterpret_cast<const double *>(stage) + (is_b ? 64 * kStageLd : 0), kStageLd,
-                              is_b, row, half, r);
-                // all eight warps have read the stage: refill it with the next problem
-                named_barrier(2, 256);
-                if (prob + gridDim.x < nprob)
-                {
-                    if (t < 128)
-                        stage_problem(p, prob + gridDim.x, t, stage, sfull);
-                    issued = j + 2;
-                }
             }
-            else
-                mx = load_row(p, is_b ? p.B + prob * p.sB : p.A + prob * p.sA, is_b ? p.ldb : p.lda, is_b, row,
-                              half, r);
             const int b = j % sp.nbuf;
-            if (!barrier_and(2, 256,
-                             j < sp.nbuf || tc::mbar_wait_bounded(&dempty[b], ((j / sp.nbuf) - 1) & 1, limit)))
+            uint8_t *buf = smem + (size_t)b * sp.buf_bytes;
+            int *ex = exps + (j % kExpRing) * 128;
+            bool ok = true;
+#pragma unroll 1
+            for (int pass = 0; pass < 2; ++pass) // row-half of A, then of B
+            {
+                const bool is_b = pass == 1;
+                double r[32];
+                const bool strided = is_b && strided_b;
+                const double mx =
+                    sp.staged ? load_row_tiled(stage + (is_b ? 4 * kBoxBytes : 0), strided, row, half, r)
+                              : load_row(p, is_b ? p.B + prob * p.sB : p.A + prob * p.sA, is_b ? p.ldb : p.lda, is_b,
+                                         row, half, r);
+                if (is_b && sp.staged)
+                {
+                    // all four warps have read the stage: refill it with the next problem
+                    named_barrier(2, 128);
+                    if (prob + gridDim.x < nprob)
+                    {
+                        if (t == 0)
+                            stage_problem(&tmA, &tmB, prob + gridDim.x, stage, sfull);
+                        issued = j + 2;
+                    }
+                }
+                // the digit buffer is free once the MMAs of its last problem completed
+                if (pass == 0 &&
+                    !barrier_and(2, 128,
+                                 j < sp.nbuf || tc::mbar_wait_bounded(&dempty[b], ((j / sp.nbuf) - 1) & 1, limit)))
+                {
+                    ok = false;
+                    break;
+                }
+                split_loaded<SK, S>(r, mx, row, half, is_b ? buf + nstack * kStackBytes : buf, is_b ? ex + 64 : ex,
+                                    sp.staged && !strided ? half : 0);
+            }
+            if (!ok)
             {
                 atomicExch(&g_split_error, 5);
                 break;
             }
-            uint8_t *buf = smem + (size_t)b * sp.buf_bytes;
-            int *ex = exps + (j % kExpRing) * 128;
-            split_loaded<SK, S>(r, mx, row, half, is_b ? buf + nstack * kStackBytes : buf, is_b ? ex + 64 : ex);
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
             if (lane == 0)
@@ -828,14 +970,15 @@ __global__ void __launch_bounds__(384, 1) split_f64_persistent(const SplitStream
     }
     else
     {
-        // ---- recombination role: warps 8..11 = TMEM lane quadrants 0..3
-        //      (named barrier 1 over its 128 threads); lane 0 of warp 8 also
-        //      issues the MMAs ----
-        const int quad = warp & 3;
+        // ---- recombination role: warps 4..11, lane quadrant warp % 4, column
+        //      group (warp - 4) / 4; lane 0 of warp 4 also issues the MMAs ----
+        const int quad = warp & 3, grp = (warp - kSplitWarps) >> 2;
         const int L = quad * 32 + lane;
         const bool top = L < 64;
-        const bool issuer = warp == 8 && lane == 0;
+        const bool issuer = warp == kSplitWarps && lane == 0;
         const uint32_t lane_addr = (uint32_t)(quad * 32) << 16;
+        double *xg = xfer + grp * (64 * xfer_ld<W>());
+        const int gbar = 1 + 2 * grp;
         constexpr int bmax = (S - 1) / 2;
         if (issuer && blockIdx.x < nprob)
         {
@@ -851,7 +994,7 @@ __global__ void __launch_bounds__(384, 1) split_f64_persistent(const SplitStream
         int j = 0;
         for (int64_t prob = blockIdx.x; prob < nprob; prob += gridDim.x, ++j)
         {
-            if (!barrier_and(1, 128, tc::mbar_wait_bounded(tfull, j & 1, limit)))
+            if (!barrier_and(4, 256, tc::mbar_wait_bounded(tfull, j & 1, limit)))
             {
                 atomicExch(&g_split_error, 7);
                 break;
@@ -860,15 +1003,16 @@ __global__ void __launch_bounds__(384, 1) split_f64_persistent(const SplitStream
             const int *eA = exps + (j % kExpRing) * 128;
             const int *eB = eA + 64;
             double *Cp = p.C + prob * p.sC;
-            for (int j0 = 0; j0 < 64; j0 += W)
+            for (int jc = 0; jc < 32; jc += W)
             {
+                const int j0 = grp * 32 + jc;
                 double acc[W];
                 gather_chunk<bmax, W, SK>(tmem + lane_addr + j0, top, p.beta, acc);
-                if (j0 == 64 - W)
+                if (jc == 32 - W)
                 {
                     // every TMEM read of problem j is done: start problem j+1
                     tc::tc_fence_before();
-                    named_barrier(1, 128);
+                    named_barrier(4, 256);
                     if (issuer && prob + gridDim.x < nprob)
                     {
                         const int jn = j + 1, bn = jn % sp.nbuf;
@@ -882,13 +1026,13 @@ __global__ void __launch_bounds__(384, 1) split_f64_persistent(const SplitStream
                     }
                     __syncwarp();
                 }
-                recombine_store<W>(p, Cp, eA, eB, xfer, acc, L, j0, true);
+                finish_half_chunk<W>(p, Cp, eA, eB, xg, acc, L, j0, gbar);
             }
         }
     }
     tc::tc_fence_before();
     __syncthreads();
-    if (warp == 8)
+    if (warp == kSplitWarps)
     {
         __syncwarp();
         tc::tc_fence_after();
@@ -969,6 +1113,44 @@ cudaError_t allow_smem(const void *fn, int sk, int s, int which)
 }
 
 size_t split_smem(int s) { return (size_t)((s + 1) / 2) * 2 * kStackBytes + 1024 + 1024; }
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn split_encode_fn()
+{
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(f);
+    });
+    return fn;
+}
+
+// FP64 map {inner, rows, batch} with boxes of 16 x 64 x 1, 128-byte swizzle
+// and zero fill outside the tensor (the stage layout of the persistent form).
+// Needs a 16-byte aligned base and row / problem strides that are multiples
+// of 16 bytes; false when the driver refuses the map.
+bool make_stage_map(CUtensorMap *map, const double *base, int inner, int rows, int64_t batch, int64_t ld,
+                    int64_t stride)
+{
+    EncodeTiledFn fn = split_encode_fn();
+    if (!fn)
+        return false;
+    cuuint64_t dims[3] = {(cuuint64_t)inner, (cuuint64_t)rows, (cuuint64_t)batch};
+    const int64_t s2 = batch > 1 ? stride : (int64_t)rows * ld;
+    cuuint64_t strides[2] = {(cuuint64_t)(ld * 8), (cuuint64_t)((s2 > 0 ? s2 : ld * rows) * 8)};
+    cuuint32_t box[3] = {16, 64, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double *>(base), dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
 
 } // namespace
 } // namespace kami
@@ -1051,14 +1233,19 @@ extern "C" int kami_split_f64_gemm_batched(int nslices, kami_dtype_t slice_type,
         sp.p = p;
         const int nstack = (nslices + 1) / 2;
         sp.buf_bytes = 2 * nstack * kStackBytes;
-        // bulk copies need 16-byte aligned rows whose length is a multiple of 16 bytes
-        const bool a_ok = !(reinterpret_cast<uintptr_t>(A) & 15) && !(lda & 1) && !(strideA & 1) && !(K & 1);
-        const bool b_ok = !(reinterpret_cast<uintptr_t>(B) & 15) && !(ldb & 1) && !(strideB & 1) &&
-                          !((b_layout == KAMI_B_REF_NK ? K : N) & 1);
-        sp.staged = a_ok && b_ok ? 1 : 0;
-        const int xld = (nslices <= 6 ? 32 : 16) + 2; // xfer_ld<persistent_chunk<S>()>()
-        const size_t fixed = (size_t)2 * 64 * xld * 8 + kExpRing * 128 * 4 + 128 + 1024 +
-                             (sp.staged ? kStageBytes : 0);
+        // tensor copies need 16-byte aligned bases and row / problem strides
+        // that are multiples of 16 bytes
+        const bool a_ok = !(reinterpret_cast<uintptr_t>(A) & 15) && !(lda & 1) && (batch == 1 || !(strideA & 1));
+        const bool b_ok = !(reinterpret_cast<uintptr_t>(B) & 15) && !(ldb & 1) && (batch == 1 || !(strideB & 1));
+        CUtensorMap mapA, mapB;
+        memset(&mapA, 0, sizeof(mapA));
+        memset(&mapB, 0, sizeof(mapB));
+        sp.staged = a_ok && b_ok && make_stage_map(&mapA, A, K, M, batch, lda, strideA) &&
+                            (b_layout == KAMI_B_REF_NK ? make_stage_map(&mapB, B, K, N, batch, ldb, strideB)
+                                                       : make_stage_map(&mapB, B, N, K, batch, ldb, strideB))
+                        ? 1
+                        : 0;
+        const size_t fixed = (size_t)kXferBytes + kExpRing * 128 * 4 + 128 + 1024 + (sp.staged ? kStageBytes : 0);
         sp.nbuf = (size_t)2 * sp.buf_bytes + fixed <= 227 * 1024 ? 2 : 1;
         const size_t smem = (size_t)sp.nbuf * sp.buf_bytes + fixed;
         int dev = 0, sms = 148;
@@ -1069,7 +1256,7 @@ extern "C" int kami_split_f64_gemm_batched(int nslices, kami_dtype_t slice_type,
         if (e2 != cudaSuccess)
             return cuda_fail(e2, "cudaFuncSetAttribute(split_f64_persistent)");
         const int64_t grid = batch < sms ? batch : sms;
-        void *args2[] = {&sp};
+        void *args2[] = {&sp, &mapA, &mapB};
         e2 = cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(384), args2, smem, st);
         if (e2 != cudaSuccess)
             return cuda_fail(e2, "cudaLaunchKernel(split_f64_persistent)");
