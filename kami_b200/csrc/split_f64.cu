@@ -687,26 +687,28 @@ __global__ void __launch_bounds__(128) split_f64_kernel(const SplitParams p)
 
 // ---------------------------------------------------------------------------
 // Persistent form for the streamed regime (one launch over all problems, one
-// CTA per SM, 12 warps), so the phases of consecutive problems overlap:
-//   warps 0-3   split: 128 threads, one row-half of A and then the same
-//               row-half of B each.  With 16-byte aligned rows the inputs of
-//               problem j are staged in shared memory by eight tensor copies
-//               (TMA engine) that thread 0 issued once the four warps had
-//               read problem j-1 out of the stage; they write the digits of
-//               problem j into buffer j % nbuf once the MMAs of the problem
-//               that last used it have completed;
-//   warps 4-11  recombination of problem j from TMEM: warp w reads lane
-//               quadrant w % 4; warps 4-7 finish output columns 0-31 and
-//               warps 8-11 columns 32-63 (two groups of 128 threads, so two
-//               warps per scheduler hide each other's TMEM and FP64
-//               latencies).  After the last TMEM read of problem j by both
-//               groups, lane 0 of warp 4 issues the MMAs of problem j+1 (its
-//               digits complete), then the groups store their last columns
-//               of problem j.
+// CTA per SM), so the phases of consecutive problems overlap.  With P split
+// warps (P = 8 or 4, split_warps below):
+//   warps 0..P-1     split: one row-half of A or of B per thread (P = 8), or
+//                    a row-half of A and then the same row-half of B (P = 4).
+//                    With 16-byte aligned rows the inputs of problem j are
+//                    staged in shared memory by eight tensor copies (TMA
+//                    engine) that thread 0 issued once the split warps had
+//                    read problem j-1 out of the stage; they write the digits
+//                    of problem j into buffer j % nbuf once the MMAs of the
+//                    problem that last used it have completed;
+//   warps P..P+7     recombination of problem j from TMEM: warp w reads lane
+//                    quadrant w % 4; warps P..P+3 finish output columns 0-31
+//                    and warps P+4..P+7 columns 32-63 (two groups of 128
+//                    threads, so two warps per scheduler hide each other's
+//                    TMEM and FP64 latencies).  After the last TMEM read of
+//                    problem j by both groups, lane 0 of warp P issues the
+//                    MMAs of problem j+1 (its digits complete), then the
+//                    groups store their last columns of problem j.
 // Row and column exponents live in a ring of four entries apart from the
-// digit buffers.  mbarriers: sfull (bulk copies, by bytes), dfull[b] (4 split
-// warps), dempty[b] and tfull (MMA commits).  Named barriers: 2 (split
-// warps), 1 and 3 (one recombination group each), 4 (both groups).
+// digit buffers.  mbarriers: sfull (tensor copies, by bytes), dfull[b] (the
+// P split warps), dempty[b] and tfull (MMA commits).  Named barriers: 2
+// (split warps), 1 and 3 (one recombination group each), 4 (both groups).
 // Every mbarrier wait is bounded; each warp group agrees on the outcome of
 // its waits with a barrier reduction before acting on it, so a timeout
 // ends the whole group together.
@@ -714,7 +716,23 @@ __global__ void __launch_bounds__(128) split_f64_kernel(const SplitParams p)
 constexpr int kBoxBytes = 64 * 128;                     // one tensor-copy box: 16 doubles x 64 rows
 constexpr int kStageBytes = 8 * kBoxBytes;              // A's four boxes, then B's
 constexpr int kExpRing = 4;
-constexpr int kSplitWarps = 4;
+// Split warps of the persistent form: eight (one row-half each, 16 warps of
+// at most 128 registers) where the split's registers allow it -- int8 digits
+// and up to four 16-bit digits; four (a row-half of A, then one of B; 12
+// warps of up to 168 registers) for five to eight 16-bit digits, whose split
+// would spill under the lower limit (measured at 64^3 x 8192: 7 int8 digits
+// 0.263 vs 0.289 ms, 7 FP16 digits 0.420 vs 0.404 ms).
+template <int SK, int S>
+constexpr int split_warps()
+{
+    return SK == kSliceI8 || S <= 4 ? 8 : 4;
+}
+
+template <int SK, int S>
+constexpr int persistent_threads()
+{
+    return split_warps<SK, S>() * 32 + 256; // + two recombination groups
+}
 constexpr int kPersistentW = 16;                        // output columns per recombination chunk
 constexpr int kXferBytes = 2 * 64 * (kPersistentW + 2) * 8; // two groups x 64 rows x xfer_ld<16>()
 
@@ -848,7 +866,7 @@ __device__ __forceinline__ void finish_half_chunk(const SplitParams &p, double *
 }
 
 template <int SK, int S>
-__global__ void __launch_bounds__(384, 1) split_f64_persistent(const SplitStreamParams sp,
+__global__ void __launch_bounds__(persistent_threads<SK, S>(), 1) split_f64_persistent(const SplitStreamParams sp,
                                                                const __grid_constant__ CUtensorMap tmA,
                                                                const __grid_constant__ CUtensorMap tmB)
 {
@@ -859,6 +877,9 @@ __global__ void __launch_bounds__(384, 1) split_f64_persistent(const SplitStream
     uint8_t *smem = smem_raw + ((1024u - (uint32_t)(reinterpret_cast<uintptr_t>(smem_raw) & 1023u)) & 1023u);
     constexpr int nstack = (S + 1) / 2;
     constexpr int W = kPersistentW;
+    constexpr int kSplitWarps = split_warps<SK, S>();
+    constexpr int kSplitThreads = kSplitWarps * 32;
+    constexpr int kSplitPasses = 256 / kSplitThreads; // row-halves of A and B per split thread
     uint8_t *stage = smem + (size_t)sp.nbuf * sp.buf_bytes;
     double *xfer = reinterpret_cast<double *>(stage + (sp.staged ? kStageBytes : 0)); // kXferBytes
     int *exps = reinterpret_cast<int *>(xfer + kXferBytes / 8);                        // kExpRing x 128
@@ -895,8 +916,8 @@ __global__ void __launch_bounds__(384, 1) split_f64_persistent(const SplitStream
 
     if (warp < kSplitWarps)
     {
-        // ---- split role (named barrier 2 over its 128 threads) ----
-        const int row = t >> 1, half = t & 1;
+        // ---- split role (named barrier 2 over its kSplitThreads threads) ----
+        const int row = (t & 127) >> 1, half = t & 1;
         const bool strided_b = p.b_layout != KAMI_B_REF_NK;
         int issued = 0, consumed = 0; // stage phases started / completed and read
         if (sp.staged && blockIdx.x < nprob)
@@ -910,7 +931,7 @@ __global__ void __launch_bounds__(384, 1) split_f64_persistent(const SplitStream
         {
             if (sp.staged)
             {
-                if (!barrier_and(2, 128, tc::mbar_wait_bounded(sfull, j & 1, limit)))
+                if (!barrier_and(2, kSplitThreads, tc::mbar_wait_bounded(sfull, j & 1, limit)))
                 {
                     atomicExch(&g_split_error, 8);
                     break;
@@ -922,19 +943,19 @@ __global__ void __launch_bounds__(384, 1) split_f64_persistent(const SplitStream
             int *ex = exps + (j % kExpRing) * 128;
             bool ok = true;
 #pragma unroll 1
-            for (int pass = 0; pass < 2; ++pass) // row-half of A, then of B
+            for (int pass = 0; pass < kSplitPasses; ++pass) // row-half of A, then of B
             {
-                const bool is_b = pass == 1;
+                const bool is_b = kSplitPasses == 2 ? pass == 1 : t >= 128;
                 double r[32];
                 const bool strided = is_b && strided_b;
                 const double mx =
                     sp.staged ? load_row_tiled(stage + (is_b ? 4 * kBoxBytes : 0), strided, row, half, r)
                               : load_row(p, is_b ? p.B + prob * p.sB : p.A + prob * p.sA, is_b ? p.ldb : p.lda, is_b,
                                          row, half, r);
-                if (is_b && sp.staged)
+                if (pass == kSplitPasses - 1 && sp.staged)
                 {
-                    // all four warps have read the stage: refill it with the next problem
-                    named_barrier(2, 128);
+                    // all split warps have read the stage: refill it with the next problem
+                    named_barrier(2, kSplitThreads);
                     if (prob + gridDim.x < nprob)
                     {
                         if (t == 0)
@@ -944,7 +965,7 @@ __global__ void __launch_bounds__(384, 1) split_f64_persistent(const SplitStream
                 }
                 // the digit buffer is free once the MMAs of its last problem completed
                 if (pass == 0 &&
-                    !barrier_and(2, 128,
+                    !barrier_and(2, kSplitThreads,
                                  j < sp.nbuf || tc::mbar_wait_bounded(&dempty[b], ((j / sp.nbuf) - 1) & 1, limit)))
                 {
                     ok = false;
@@ -1060,12 +1081,14 @@ struct SplitFns
 {
     const void *per_problem;
     const void *persistent;
+    int persistent_threads;
 };
 
 template <int SK, int S>
 SplitFns split_fns()
 {
-    return {(const void *)&split_f64_kernel<SK, S>, (const void *)&split_f64_persistent<SK, S>};
+    return {(const void *)&split_f64_kernel<SK, S>, (const void *)&split_f64_persistent<SK, S>,
+            persistent_threads<SK, S>()};
 }
 
 // kernels per (digit kind, digit count): FP16 digits 2..7, BF16 and int8
@@ -1098,7 +1121,7 @@ SplitFns split_lookup(int sk, int s)
         default: break;
         }
 #undef KAMI_SPLIT_CASE
-    return {nullptr, nullptr};
+    return {nullptr, nullptr, 0};
 }
 
 // raise the dynamic shared memory limit of one kernel, once per process
@@ -1257,7 +1280,7 @@ extern "C" int kami_split_f64_gemm_batched(int nslices, kami_dtype_t slice_type,
             return cuda_fail(e2, "cudaFuncSetAttribute(split_f64_persistent)");
         const int64_t grid = batch < sms ? batch : sms;
         void *args2[] = {&sp, &mapA, &mapB};
-        e2 = cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(384), args2, smem, st);
+        e2 = cudaLaunchKernel(fn, dim3((unsigned)grid), dim3((unsigned)fns.persistent_threads), args2, smem, st);
         if (e2 != cudaSuccess)
             return cuda_fail(e2, "cudaLaunchKernel(split_f64_persistent)");
         return KAMI_OK;
