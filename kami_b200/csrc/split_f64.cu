@@ -734,7 +734,7 @@ constexpr int persistent_threads()
     return split_warps<SK, S>() * 32 + 256; // + two recombination groups
 }
 constexpr int kPersistentW = 16;                        // output columns per recombination chunk
-constexpr int kXferBytes = 2 * 64 * (kPersistentW + 2) * 8; // two groups x 64 rows x xfer_ld<16>()
+constexpr int kXferBytes = 2 * 64 * kPersistentW * 8;   // two groups' 64 x 16 FP64 tiles
 
 struct SplitStreamParams
 {
@@ -793,75 +793,96 @@ __device__ __forceinline__ void issue_products(const SplitParams &p, uint32_t tm
     tc::mma_commit(tfull);
 }
 
-// Finish the 64 x W chunk j0..j0+W-1 of C from the partial sums of one TMEM
+// 16-byte chunk c (columns 2c, 2c+1) of row r of a recombination group's
+// 64 x 16 FP64 tile: 128-byte rows, chunk index XOR r % 8, so eight
+// consecutive rows, or the eight chunks of one row, fall in distinct banks.
+__device__ __forceinline__ double *tile_chunk(double *tile, int r, int c)
+{
+    return tile + r * 16 + ((c ^ (r & 7)) << 1);
+}
+
+// Finish the 64 x 16 chunk j0..j0+15 of C from the partial sums of one TMEM
 // lane L (L < 64: the top partial of row L, L >= 64: the bottom partial of
-// row L - 64).  The top thread of row r finishes columns j0..j0+W/2-1 and the
-// bottom thread columns j0+W/2..j0+W-1: each first leaves the half that it
-// does not finish in xfer (64 rows x xfer_ld<W>() doubles), then adds the
-// other thread's half to its own, scales by 2^(eA[r] + eB[col]), applies
-// alpha and beta and stores W/2 consecutive doubles of row r.  Named barrier
-// `bar` over the 128 threads of the group orders xfer.
+// row L - 64).  The top thread of row r finishes columns j0..j0+7 and the
+// bottom thread columns j0+8..j0+15: each leaves the half that it does not
+// finish in the group's tile, adds the other thread's half to its own, scales
+// by 2^(eA[r] + eB[col]) and alpha, and puts its eight results back into the
+// tile; then the 128 threads copy the tile out row by row (8 threads per
+// 128-byte row, beta applied there), so every warp store covers four whole
+// row segments of C.  Named barrier `bar` over the group's 128 threads orders
+// the tile.
 template <int W>
 __device__ __forceinline__ void finish_half_chunk(const SplitParams &p, double *Cp, const int *eA, const int *eB,
-                                                  double *xfer, const double (&part)[W], int L, int j0, int bar)
+                                                  double *tile, const double (&part)[W], int L, int j0, int bar)
 {
-    constexpr int LD = xfer_ld<W>(), HW = W / 2;
+    static_assert(W == 16, "one 128-byte tile row per output row");
+    constexpr int HW = W / 2;
     const bool top = L < 64;
     const int r = L & 63;
-    double *xr = xfer + r * LD;
-    named_barrier(bar, 128); // the previous chunk's reads of xfer are done
+    const int mine = top ? 0 : 4; // first chunk this thread finishes
+    named_barrier(bar, 128);      // the previous chunk's copy-out is done with the tile
 #pragma unroll
-    for (int e = 0; e < HW; e += 2)
-    {
-        const double2 v = top ? make_double2(part[HW + e], part[HW + e + 1]) : make_double2(part[e], part[e + 1]);
-        *reinterpret_cast<double2 *>(xr + (top ? HW : 0) + e) = v;
-    }
+    for (int c = 0; c < 4; ++c)
+        *reinterpret_cast<double2 *>(tile_chunk(tile, r, 4 - mine + c)) =
+            top ? make_double2(part[HW + 2 * c], part[HW + 2 * c + 1]) : make_double2(part[2 * c], part[2 * c + 1]);
     named_barrier(bar, 128);
-    if (r >= p.M)
-        return;
-    const int jb = j0 + (top ? 0 : HW); // first output column this thread finishes
+    const int jb = j0 + 2 * mine; // first output column this thread finishes
     const int ea = eA[r];
-    // all shared-memory reads first: HW exponents (16-byte aligned, jb is a
-    // multiple of 8) and the other thread's HW partials
+    // HW exponents (16-byte aligned: jb is a multiple of 8) and the other
+    // thread's HW partials
     int eb[HW];
 #pragma unroll
     for (int e = 0; e < HW; e += 4)
         *reinterpret_cast<int4 *>(&eb[e]) = *reinterpret_cast<const int4 *>(eB + jb + e);
     double o[HW];
 #pragma unroll
-    for (int e = 0; e < HW; e += 2)
-        *reinterpret_cast<double2 *>(&o[e]) = *reinterpret_cast<const double2 *>(xr + (top ? 0 : HW) + e);
+    for (int c = 0; c < 4; ++c)
+        *reinterpret_cast<double2 *>(&o[2 * c]) = *reinterpret_cast<const double2 *>(tile_chunk(tile, r, mine + c));
     double v[HW];
 #pragma unroll
     for (int e = 0; e < HW; ++e)
         v[e] = p.alpha * scale2((top ? part[e] : part[HW + e]) + o[e], ea + eb[e]);
-    double *dst = Cp + (int64_t)r * p.ldc + jb;
-    if (p.c_vec && jb + HW <= p.N)
+    named_barrier(bar, 128); // every exchange read is done: the tile takes the results
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+        *reinterpret_cast<double2 *>(tile_chunk(tile, r, mine + c)) = make_double2(v[2 * c], v[2 * c + 1]);
+    named_barrier(bar, 128);
+    // copy-out: thread L takes chunk L % 8 of rows L / 8, L / 8 + 16, ...
+    const int cc = L & 7, col = j0 + 2 * cc;
+    if (col >= p.N)
+        return;
+    const bool two = col + 1 < p.N;
+#pragma unroll
+    for (int pass = 0; pass < 4; ++pass)
     {
-        if (p.beta_c != 0.0)
+        const int row = (L >> 3) + 16 * pass;
+        if (row >= p.M)
+            break;
+        const double2 val = *reinterpret_cast<const double2 *>(tile_chunk(tile, row, cc));
+        double *dst = Cp + (int64_t)row * p.ldc + col;
+        double v0 = val.x, v1 = val.y;
+        if (two && p.c_vec)
         {
-#pragma unroll
-            for (int e = 0; e < HW; e += 2)
+            if (p.beta_c != 0.0)
             {
-                const double2 old = *reinterpret_cast<const double2 *>(dst + e);
-                v[e] += p.beta_c * old.x;
-                v[e + 1] += p.beta_c * old.y;
+                const double2 old = *reinterpret_cast<const double2 *>(dst);
+                v0 += p.beta_c * old.x;
+                v1 += p.beta_c * old.y;
             }
+            *reinterpret_cast<double2 *>(dst) = make_double2(v0, v1);
         }
-#pragma unroll
-        for (int e = 0; e < HW; e += 2)
-            *reinterpret_cast<double2 *>(dst + e) = make_double2(v[e], v[e + 1]);
-    }
-    else
-    {
-#pragma unroll
-        for (int e = 0; e < HW; ++e)
-            if (jb + e < p.N)
+        else
+        {
+            if (p.beta_c != 0.0)
+                v0 += p.beta_c * dst[0];
+            dst[0] = v0;
+            if (two)
             {
                 if (p.beta_c != 0.0)
-                    v[e] += p.beta_c * dst[e];
-                dst[e] = v[e];
+                    v1 += p.beta_c * dst[1];
+                dst[1] = v1;
             }
+        }
     }
 }
 
@@ -998,7 +1019,7 @@ __global__ void __launch_bounds__(persistent_threads<SK, S>(), 1) split_f64_pers
         const bool top = L < 64;
         const bool issuer = warp == kSplitWarps && lane == 0;
         const uint32_t lane_addr = (uint32_t)(quad * 32) << 16;
-        double *xg = xfer + grp * (64 * xfer_ld<W>());
+        double *xg = xfer + grp * (64 * W);
         const int gbar = 1 + 2 * grp;
         constexpr int bmax = (S - 1) / 2;
         if (issuer && blockIdx.x < nprob)
