@@ -69,7 +69,8 @@ def parse():
                     help="block (default, the headline line) or one of the other configurations; "
                          "non-default workloads print one JSON line per measured case")
     ap.add_argument("--case", default="block128",
-                    choices=["block128", "stream128", "fp64-64", "split-int8x7", "spgemm-numeric", "spgemm-symbolic",
+                    choices=["block128", "stream128", "fp64-64", "split-int8x7", "split-fp16x6", "spgemm-numeric",
+                             "spgemm-symbolic",
                              "uneven-f16", "bmm-bf16"],
                     help="--workload case: run one benchmark case three times, untimed (for profiler captures)")
     return ap.parse_args()
@@ -381,15 +382,16 @@ def run_case(args):
         B = (torch.rand((8192, 64, 64), generator=g, dtype=torch.float64) * 2 - 1).to(dev)
         C = torch.empty((8192, 64, 64), dtype=torch.float64, device=dev)
         fn = lambda: api.gemm_batched(A, B, C)
-    elif c == "split-int8x7":
-        # the split-FP64 streamed workload: 8192 x 64^3, sign * 10^u, 7 int8 digits
+    elif c in ("split-int8x7", "split-fp16x6"):
+        # the split-FP64 streamed workload: 8192 x 64^3, sign * 10^u, 7 int8 or 6 FP16 digits
         rng = np.random.default_rng(0)
         A = torch.tensor(rng.choice([-1.0, 1.0], (8192, 64, 64)) * 10.0 ** rng.uniform(-3, 3, (8192, 64, 64)),
                          device=dev)
         B = torch.tensor(rng.choice([-1.0, 1.0], (8192, 64, 64)) * 10.0 ** rng.uniform(-3, 3, (8192, 64, 64)),
                          device=dev)
         C = torch.empty((8192, 64, 64), dtype=torch.float64, device=dev)
-        fn = lambda: api.split_f64_gemm(A, B, C, nslices=7, slice_dtype=torch.int8)
+        ns, sdt = (7, torch.int8) if c == "split-int8x7" else (6, torch.float16)
+        fn = lambda: api.split_f64_gemm(A, B, C, nslices=ns, slice_dtype=sdt)
     elif c in ("spgemm-numeric", "spgemm-symbolic"):
         nb = 1024
         rpa, cia = oracle.bsr_pattern(nb, nb, 0.01, 1)
