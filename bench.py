@@ -752,13 +752,19 @@ def run_secondary(args):
                         raise RuntimeError(f"CUTLASS comparator returned {st}")
 
                 name = f"{str(idt).split('.')[-1]} {n}^3 x {b} streamed, {str(odt).split('.')[-1]} out, B as N x K"
-                for impl, fn in (("kami_b200", lambda: api.gemm_batched(A, B, C1)), ("cutlass_sm100", cutlass_run)):
+                # cuBLAS (torch.bmm on B's transposed view) writes C in the input type
+                C3 = torch.empty((b, n, n), dtype=idt, device=dev)
+                Bt_ = B.transpose(1, 2)
+                for impl, fn, cout in (("kami_b200", lambda: api.gemm_batched(A, B, C1), C1),
+                                       ("cutlass_sm100", cutlass_run, C2),
+                                       ("cublas", lambda: torch.bmm(A, Bt_, out=C3), C3)):
                     ms = _time_ms(fn, W, K_, flush)
                     t = min(ms)
-                    by = b * n * n * (2 + 2 + C1.element_size())
+                    by = b * n * n * (2 + 2 + cout.element_size())
                     _emit({"workload": "comparators", "case": name, "impl": impl, "ms": t,
                            "ms_mean": statistics.fmean(ms), "tflops": 2.0 * n ** 3 * b / t / 1e9,
-                           "hbm_gbs": by / t / 1e6, "frac_hbm": by / t / 1e6 / peak_bw})
+                           "hbm_gbs": by / t / 1e6, "frac_hbm": by / t / 1e6 / peak_bw,
+                           "c_dtype": str(cout.dtype).split('.')[-1]})
                 diff = float((C1.float() - C2.float()).abs().max())
                 _emit({"workload": "comparators", "case": name, "max_abs_diff_kami_vs_cutlass": diff})
         else:
