@@ -600,8 +600,16 @@ static int build_plan(int in_type, int out_type, int count, const int *M, const 
     if (tc && (e = cudaFuncSetAttribute(grouped_tc05_fn(in_type == KAMI_BF16, true),
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
         return cuda_fail(e, "cudaFuncSetAttribute(grouped kernel)");
+    // all of the SM's unified L1 / shared memory as shared memory, so the
+    // occupancy below counts every CTA that fits
+    for (int pk = 0; tc && pk < 2; ++pk)
+        if ((e = cudaFuncSetAttribute(grouped_tc05_fn(in_type == KAMI_BF16, pk == 1),
+                                      cudaFuncAttributePreferredSharedMemoryCarveout, 100)) != cudaSuccess)
+            return cuda_fail(e, "cudaFuncSetAttribute(grouped kernel carveout)");
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, smem)) != cudaSuccess)
         return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    if (tc)
+        occ = grouped_tc05_ctas_per_sm(); // sized for two per SM; the query reports one
     occ = std::max(occ, 1);
     const int ctas = std::max(1, std::min(count, sms * occ));
     const int esz = in_type == KAMI_F64 ? 8 : 2;

@@ -35,6 +35,7 @@ struct GroupedParams
 const void *grouped_tc05_fn(bool bf16, bool packed);
 int grouped_tc05_threads();
 int grouped_tc05_smem();
+int grouped_tc05_ctas_per_sm();
 int grouped_tc05_launch(const GroupedParams &p, bool bf16, bool packed, int ctas, cudaStream_t s);
 int grouped_tc05_read_error(int *flag);
 

@@ -230,7 +230,7 @@ def test_grouped_tcgen05_more_problems_than_cached(cuda):
     shapes = np.stack([rng.choice([8, 16, 24], count), rng.choice([8, 16], count), rng.choice([8, 16], count)], 1)
     As, Bs, A, B = make_inputs(shapes, torch.float16, 16)
     plan = api.GroupedPlan(shapes, torch.float16, kernel="tcgen05")
-    assert plan.info()["problems"] // plan.info()["ctas"] > 512
+    assert plan.info()["problems"] // plan.info()["ctas"] > 224  # the cache holds at most 224
     C = torch.empty(plan.sizes[2], dtype=torch.float32, device="cuda")
     plan.run(A, B, C)
     Ch = C.double().cpu().numpy()
