@@ -16,9 +16,14 @@
 // writes 32 consecutive columns of one C row -- coalesced with no transpose.
 //
 // Four CTAs per SM walk the block-rows i = blockIdx.x, + gridDim.x, ...:
-//   warp 0      loads each tile's B slice (TMA, lane 0) and the tile itself
+//   warps 0, 6  load the tiles alternately (tile j by warp 0 when j is even):
+//               each tile's B slice (TMA, lane 0) and the tile itself
 //               (cp.async, all lanes, each arriving on the slot's barrier
-//               when its copy lands) into a ring of slots;
+//               when its copy lands) into a ring of at least two slots.  A
+//               loader at tile j waited, at its previous tile j - 2, for the
+//               commit of tile j - 2 - S, so the MMAs (consumed in order)
+//               have already freed its own previous fill of the slot: no
+//               parity wait runs more than one phase ahead;
 //   warp 1      lane 0 issues the MMAs (ceil(N / 128) per tile and repeat)
 //               into a ring of four TMEM accumulators, and owns the TMEM
 //               allocation;
@@ -47,16 +52,18 @@ __device__ int g_spmm_tc_error = 0;
 
 namespace {
 
-// Four CTAs per SM: the per-tile work is two tiny MMAs, so one CTA's single
-// loading lane and single MMA-issuing lane (~850 and ~430 cycles a tile) set
-// the pace; four CTAs run four such pipelines side by side (one CTA per SM:
-// 55 us for the n = 16384, 1 % case; two: 37 us; four: 27.6 us).  72
-// registers x 192 threads x 4 and 4 x 128 TMEM columns fill the SM.
+// Four CTAs per SM: the per-tile work is two tiny MMAs, so a CTA's loading
+// lanes and single MMA-issuing lane set the pace (one loader: ~850 and ~430
+// cycles a tile); four CTAs run four such pipelines side by side (one CTA
+// per SM: 55 us for the n = 16384, 1 % case; two: 37 us; four: 27.6 us), and
+// two loader warps per CTA bring it to 25.7 us.  60 registers x 224 threads
+// x 4 and 4 x 128 TMEM columns fit the SM.
 constexpr int kCtasPerSm = 4;                 // resident CTAs per SM (the grid is this many per SM)
 constexpr int kEpiGroups = 1;                 // epilogue groups of four warps
 constexpr int kAccs = 4;                      // TMEM accumulators (block-rows in flight) per CTA
 constexpr int kMaxSlots = 16;
-constexpr int kThreads = (2 + 4 * kEpiGroups) * 32;
+constexpr int kLoadWarp2 = 2 + 4 * kEpiGroups; // the second loader warp, after the epilogue
+constexpr int kThreads = (kLoadWarp2 + 1) * 32;
 
 struct SpTcParams
 {
@@ -149,9 +156,11 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) spmm_tc05_kernel(const _
     tc::tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
-    if (warp == 0)
+    if (warp == 0 || warp == kLoadWarp2)
     {
-        // ---- loads: the B slice by TMA (lane 0), the tile by cp.async ----
+        // ---- loads: the B slice by TMA (lane 0), the tile by cp.async; this
+        //      warp takes the tiles j with j % 2 == lid ----
+        const int lid = warp == 0 ? 0 : 1;
         if (lane == 0)
             tc::prefetch_tmap(&tmB);
         const uint32_t base = tc::smem_u32(smem);
@@ -176,6 +185,8 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) spmm_tc05_kernel(const _
             const int ee = e1 - eb < 32 ? e1 - eb : 32;
             for (int t = 0; t < ee; ++t, ++j)
             {
+                if ((j & 1) != lid)
+                    continue; // the other loader's tile
                 const int e = eb + t;
                 const int s = j % S;
                 bool w = true;
@@ -388,6 +399,8 @@ int spmm_tc05_launch(bool bf16, int out_type, int mb, int kb, int N, const int *
     p.slot_bytes = (p.npad * 32 + 512 + 1023) / 1024 * 1024;
     const int budget = 228 * 1024 / kCtasPerSm - 1024 - 1024 - 512;
     p.slots = budget / p.slot_bytes < kMaxSlots ? budget / p.slot_bytes : kMaxSlots;
+    if (p.slots < 2) // the two loaders need two slots (see the kernel)
+        return KAMI_ERR_UNSUPPORTED;
     p.acc_cols = (p.npad / 128) * 16;
     uint32_t cols = 32;
     while ((int)cols < kAccs * p.acc_cols)

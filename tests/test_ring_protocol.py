@@ -305,16 +305,94 @@ def simulate_grouped(S, NA, G, chunks, rng, acc_wait=True):
     return bad
 
 
-def test_grouped_kernel_protocol():
-    """The grouped kernel's constants (6 slots, 4 accumulators, 2 epilogue
+@pytest.mark.parametrize("S,NA,G", [(2, 2, 2),   # the kernel's constants (two CTAs per SM)
+                                    (6, 4, 2)])  # its earlier one-CTA-per-SM form
+def test_grouped_kernel_protocol(S, NA, G):
+    """The grouped kernel's constants (S slots, NA accumulators, G epilogue
     groups, one issuer) never pass a wait early over random chunk mixes."""
-    rng = random.Random(11)
+    rng = random.Random(11 + S)
     for _ in range(60):
         chunks = [rng.choice((1, 1, 1, 2)) for _ in range(rng.randint(1, 50))]
-        assert simulate_grouped(6, 4, 2, chunks, rng) == []
+        assert simulate_grouped(S, NA, G, chunks, rng) == []
 
 
 def test_grouped_kernel_needs_its_accumulator_wait():
     rng = random.Random(3)
     chunks = [1] * 40
     assert any(simulate_grouped(6, 4, 2, chunks, rng, acc_wait=False) for _ in range(30))
+
+
+def simulate_two_loaders(S, ntiles, rng):
+    """spmm_tc05_kernel (kami_b200/csrc/spmm_tc05.cu): two loader warps take
+    the tiles alternately (tile j by loader j % 2) and fill slot j % S, each
+    first waiting for the slot's previous use to be committed; one issuer
+    consumes the tiles in order and frees each slot with a commit.  Returns
+    the violations (a wait passing before the phase it needs completed)."""
+    full = [Barrier(1) for _ in range(S)]
+    empty = [Barrier(1) for _ in range(S)]
+    bad, events = [], []
+    now, ic, iss_done = 0, 0, 0
+    lj = [0, 1]  # next tile of each loader
+    filled = [None] * S
+    for _ in range(200000):
+        progressed = False
+        order = [("load", 0), ("load", 1), ("iss", 0)]
+        rng.shuffle(order)
+        for kind, w in order:
+            if kind == "load" and lj[w] < ntiles:
+                j = lj[w]
+                s = j % S
+                if j >= S:
+                    if not empty[s].passes(((j // S) - 1) & 1):
+                        continue
+                    if j // S - 1 >= empty[s].phase:
+                        bad.append(("loader", w, j))
+                events.append((now + rng.randint(1, 40), "load", (s, j)))
+                lj[w] += 2
+                progressed = True
+            elif kind == "iss" and ic < ntiles:
+                s = ic % S
+                if not full[s].passes((ic // S) & 1):
+                    continue
+                if ic // S >= full[s].phase:
+                    bad.append(("issuer", ic))
+                if filled[s] != ic:
+                    bad.append(("issuer reads a slot holding another tile", ic, filled[s]))
+                iss_done = max(now, iss_done) + rng.randint(1, 30)
+                events.append((iss_done, "mma", s))
+                ic += 1
+                progressed = True
+        if not progressed:
+            if not events:
+                break
+            events.sort(key=lambda e: e[0])
+            t0, kind, x = events.pop(0)
+            now = max(now, t0)
+            if kind == "load":
+                s, j = x
+                filled[s] = j
+                full[s].arrive()
+            else:
+                empty[x].arrive()
+    if not bad and ic < ntiles:
+        bad.append(("stalled", ic, lj))
+    return bad
+
+
+@pytest.mark.parametrize("S", [2, 3, 4, 5, 6])
+def test_two_loaders_never_pass_a_wait_early(S):
+    """Loader w at tile j already waited, at its previous tile j - 2, for the
+    commit of tile j - 2 - S; the issuer consumes in order, so every tile up
+    to j - 2 - S -- among them j - 2S, the previous fill of slot j % S that
+    this loader made -- is consumed.  So with S >= 2 slots no loader waits
+    more than one phase ahead of a slot, odd or even S alike."""
+    rng = random.Random(S)
+    for _ in range(40):
+        assert simulate_two_loaders(S, rng.randint(1, 80), rng) == []
+
+
+def test_two_loaders_one_slot_does_pass_a_wait_early():
+    """With a single slot the argument fails (j - 2 - S < j - 2S), and the
+    loaders do overtake: the launcher never runs two loaders on one slot."""
+    rng = random.Random(5)
+    assert any(simulate_two_loaders(1, 60, rng) for _ in range(60))
