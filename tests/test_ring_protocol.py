@@ -44,6 +44,8 @@ def launcher_config(stage_bytes, bn, bulk_store):
             groups = 2
             budget = SMEM - 1024 - 512 - 4 * groups * EPI_TILE
     stages = min(6, budget // stage_bytes)
+    if bulk_store and 65536 <= stage_bytes <= 90 * 1024:
+        return 1, 2, 1, 1  # two CTAs per SM: one slot, two accumulators, one group each
     if stages < 2:
         return None
     issuers = 2 if stage_bytes < 32768 and stages % 2 == 0 and naccs % 2 == 0 else 1
