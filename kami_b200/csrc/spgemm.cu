@@ -46,6 +46,14 @@ __device__ unsigned int g_spg_bar[kFuseSlots][2];
 // device status of the fused pass's bounded barrier waits (read and cleared
 // by kami_device_status)
 __device__ int g_spg_error = 0;
+// Look-back flags of the single-pass symbolic kernel: one 64-bit word per
+// chunk of block-rows, [epoch (31 bits) | inclusive (1 bit) | value (32
+// bits)].  Each launch takes the next slot and a new epoch, so a word left by
+// an earlier launch never reads as ready and nothing is reset between
+// launches.
+constexpr int kLbSlots = 16;
+constexpr int kLbMaxChunks = 16384;
+__device__ unsigned long long g_spg_flags[kLbSlots][kLbMaxChunks];
 
 namespace {
 
@@ -374,6 +382,195 @@ __global__ void spgemm_symbolic_fused_kernel(int mb, int nb, const int *__restri
             out += __shfl_sync(0xffffffffu, pre, 31);
         }
         __syncwarp();
+    }
+}
+
+
+// ---------------------------------------------------------------------------
+// The symbolic pass in one launch and one pass: chunk c of block-rows (R
+// consecutive rows, c = blockIdx.x, + gridDim.x, ...) is counted by its CTA,
+// which publishes the chunk's total, finds the exclusive prefix of the
+// chunks before it by a decoupled look-back over their flags (a chunk's flag
+// carries its own total, or the inclusive prefix once its CTA found it), writes
+// RowPtrC for its rows and fills their ColIdxC.  No grid barrier: a chunk's
+// fill starts as soon as its prefix is known.  The launch is cooperative, so
+// every chunk's CTA is resident and a look-back never waits for a CTA that
+// does not run; the waits are bounded all the same (a timeout sets
+// g_spg_error).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long lb_word(unsigned epoch, bool incl, int value)
+{
+    return ((unsigned long long)epoch << 33) | ((unsigned long long)incl << 32) | (uint32_t)value;
+}
+
+// Exclusive prefix of chunk c (c > 0), by warp 0 of its CTA: lane l reads the
+// flag of chunk p - l for a window of 32 predecessors; the window's sum up to
+// and including the nearest inclusive flag ends the walk.  Returns false on
+// a timeout.
+__device__ __forceinline__ bool lb_prefix(const unsigned long long *flags, int c, unsigned epoch, uint64_t limit_ns,
+                                          int lane, int *prefix)
+{
+    int acc = 0;
+    int p = c - 1;
+    const uint64_t t0 = spg_globaltimer();
+    while (p >= 0)
+    {
+        const int q = p - lane;
+        unsigned long long w = 0;
+        bool ready = true;
+        if (q >= 0)
+        {
+            w = *reinterpret_cast<const volatile unsigned long long *>(&flags[q]);
+            ready = (unsigned)(w >> 33) == epoch;
+        }
+        const bool incl = q >= 0 && ready && ((w >> 32) & 1ull);
+        const unsigned incl_mask = __ballot_sync(0xffffffffu, incl);
+        // lanes up to the nearest inclusive flag (or all 32 / down to chunk 0)
+        const int last = incl_mask ? __ffs(incl_mask) - 1 : 31;
+        const bool need = lane <= last && q >= 0;
+        if (!__all_sync(0xffffffffu, !need || ready))
+        {
+            if (spg_globaltimer() - t0 > limit_ns)
+                return false;
+            __nanosleep(32);
+            continue; // a predecessor has not published yet: read the window again
+        }
+        int v = need ? (int)(uint32_t)w : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+            v += __shfl_xor_sync(0xffffffffu, v, o);
+        acc += v;
+        if (incl_mask)
+            break;
+        p -= 32;
+    }
+    *prefix = acc;
+    return true;
+}
+
+// rows_per_warp (k): each warp takes rows r0 + w + wpc t of its chunk (R =
+// wpc k rows); with k = 1 the row's bitmap stays in shared memory from the
+// count to the fill, otherwise it is rebuilt for the fill.
+__global__ void spgemm_symbolic_lookback_kernel(int mb, int nb, const int *__restrict__ rpa,
+                                                const int *__restrict__ cia, const int *__restrict__ rpb,
+                                                const int *__restrict__ cib, int *__restrict__ rpc,
+                                                int *__restrict__ cic, int64_t cap, unsigned long long *flags,
+                                                unsigned epoch, int rows_per_warp, uint64_t limit_ns)
+{
+    extern __shared__ uint32_t bm_all[];
+    __shared__ int s_cnt[1024]; // row counts of the chunk, then their exclusive offsets
+    __shared__ int s_prefix, s_ok;
+    const int words = (nb + 31) >> 5;
+    const int wpc = blockDim.x >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int k = rows_per_warp, R = wpc * k;
+    uint32_t *bm = bm_all + (size_t)warp * words;
+    const int nchunks = (mb + R - 1) / R;
+    for (int c = blockIdx.x; c < nchunks; c += gridDim.x)
+    {
+        const int r0 = c * R;
+        // ---- count: row r0 + w + wpc t of the chunk ----
+        for (int t = 0; t < k; ++t)
+        {
+            const int lr = warp + wpc * t, row = r0 + lr;
+            int cnt = 0;
+            if (row < mb)
+            {
+                build_row_bitmap(bm, words, row, rpa, cia, rpb, cib, lane);
+                for (int w = lane; w < words; w += 32)
+                    cnt += __popc(bm[w]);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1)
+                    cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+            }
+            if (lane == 0)
+                s_cnt[lr] = cnt;
+            __syncwarp();
+        }
+        __syncthreads();
+        // ---- warp 0: the chunk's exclusive row offsets and total, publish,
+        //      look back, publish the inclusive prefix ----
+        if (warp == 0)
+        {
+            int carry = 0;
+            for (int b = 0; b < R; b += 32)
+            {
+                const int v = b + lane < R ? s_cnt[b + lane] : 0;
+                int x = v;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1)
+                {
+                    const int y = __shfl_up_sync(0xffffffffu, x, o);
+                    if (lane >= o)
+                        x += y;
+                }
+                if (b + lane < R)
+                    s_cnt[b + lane] = carry + x - v;
+                carry += __shfl_sync(0xffffffffu, x, 31);
+            }
+            const int total = carry;
+            if (lane == 0)
+                atomicExch(&flags[c], lb_word(epoch, c == 0, total));
+            int prefix = 0;
+            bool ok = true;
+            if (c > 0)
+                ok = lb_prefix(flags, c, epoch, limit_ns, lane, &prefix);
+            if (lane == 0)
+            {
+                if (ok && c > 0)
+                    atomicExch(&flags[c], lb_word(epoch, true, prefix + total));
+                if (!ok)
+                    atomicExch(&g_spg_error, 3);
+                s_prefix = prefix;
+                s_ok = ok;
+                if (r0 + R >= mb) // the last chunk: the total of all rows
+                    rpc[mb] = prefix + total;
+            }
+        }
+        __syncthreads();
+        if (!s_ok)
+            return;
+        const int prefix = s_prefix;
+        for (int lr = threadIdx.x; lr < R; lr += blockDim.x)
+            if (r0 + lr < mb)
+                rpc[r0 + lr] = prefix + s_cnt[lr];
+        // ---- fill: ColIdxC ascending per row, up to the capacity ----
+        if (cap > 0)
+            for (int t = 0; t < k; ++t)
+            {
+                const int lr = warp + wpc * t, row = r0 + lr;
+                if (row >= mb)
+                    break;
+                if (k > 1)
+                    build_row_bitmap(bm, words, row, rpa, cia, rpb, cib, lane);
+                int out = prefix + s_cnt[lr];
+                for (int w0 = 0; w0 < words; w0 += 32)
+                {
+                    const int w = w0 + lane;
+                    uint32_t bits = w < words ? bm[w] : 0u;
+                    const int cb = __popc(bits);
+                    int pre = cb;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1)
+                    {
+                        const int y = __shfl_up_sync(0xffffffffu, pre, o);
+                        if (lane >= o)
+                            pre += y;
+                    }
+                    int pos = out + pre - cb;
+                    while (bits)
+                    {
+                        const int b = __ffs(bits) - 1;
+                        if (pos < cap)
+                            cic[pos] = w * 32 + b;
+                        ++pos;
+                        bits &= bits - 1;
+                    }
+                    out += __shfl_sync(0xffffffffu, pre, 31);
+                }
+                __syncwarp();
+            }
+        __syncthreads(); // s_cnt and the bitmaps are reused by the next chunk
     }
 }
 
@@ -1035,6 +1232,64 @@ int symbolic_fused(int mb, int nb, const int *rpa, const int *cia, const int *rp
     return KAMI_OK;
 }
 
+
+// The single-pass symbolic launch; KAMI_ERR_UNSUPPORTED (nothing launched)
+// when the device has no cooperative launch or the rows need more chunks
+// than the flag array holds.
+int symbolic_lookback(int mb, int nb, const int *rpa, const int *cia, const int *rpb, const int *cib, int *rpc,
+                      int *cic, int64_t cap, cudaStream_t s)
+{
+    int dev = 0, sms = 0, coop = 0, occ = 0;
+    cudaError_t e;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess)
+        return cuda_fail(e, "cudaGetDevice");
+    if (dev < 0 || dev >= 64)
+        return KAMI_ERR_UNSUPPORTED;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    if (!coop || mb < 1)
+        return KAMI_ERR_UNSUPPORTED;
+    static std::once_flag once[64];
+    static unsigned long long *flag_base[64];
+    static cudaError_t flag_err[64];
+    std::call_once(once[dev], [&] {
+        void *ptr = nullptr;
+        flag_err[dev] = cudaGetSymbolAddress(&ptr, g_spg_flags);
+        flag_base[dev] = reinterpret_cast<unsigned long long *>(ptr);
+    });
+    if (flag_err[dev] != cudaSuccess)
+        return cuda_fail(flag_err[dev], "cudaGetSymbolAddress(spgemm look-back flags)");
+    int wpc;
+    size_t smem;
+    int st = bitmap_launch(nb, &wpc, &smem);
+    if (st)
+        return st;
+    // rows per warp per chunk: the chunks must fit the flag array and R = wpc k
+    // rows the kernel's offset array
+    const int64_t k64 = ((int64_t)mb + (int64_t)wpc * kLbMaxChunks - 1) / ((int64_t)wpc * kLbMaxChunks);
+    if (k64 < 1 || wpc * k64 > 1024)
+        return KAMI_ERR_UNSUPPORTED;
+    const int k = (int)k64, R = wpc * k;
+    const int nchunks = (mb + R - 1) / R;
+    const void *fn = (const void *)spgemm_symbolic_lookback_kernel;
+    if ((st = prep_bitmap_fn(fn, smem)))
+        return st;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, wpc * 32, smem)) != cudaSuccess)
+        return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor(spgemm look-back)");
+    if (occ < 1)
+        return KAMI_ERR_UNSUPPORTED;
+    const int grid = nchunks < sms * occ ? nchunks : sms * occ;
+    static std::atomic<unsigned int> next_launch{0};
+    const unsigned int n = next_launch.fetch_add(1);
+    unsigned long long *flags = flag_base[dev] + (size_t)(n % kLbSlots) * kLbMaxChunks;
+    unsigned epoch = (n % 0x7fffffffu) + 1; // never 0, the value of untouched flags
+    uint64_t limit = (uint64_t)2e9 + (uint64_t)mb * 20000ull;
+    void *args[] = {&mb, &nb, &rpa, &cia, &rpb, &cib, &rpc, &cic, &cap, &flags, &epoch, (void *)&k, &limit};
+    if ((e = cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(wpc * 32), args, smem, s)) != cudaSuccess)
+        return cuda_fail(e, "cudaLaunchCooperativeKernel(spgemm_symbolic_lookback_kernel)");
+    return KAMI_OK;
+}
+
 } // namespace
 
 int spgemm_tc05_launch(bool bf16, int mb, int64_t nnzc, const int *rpa, const int *cia, const int *rpb, const int *cib,
@@ -1145,6 +1400,12 @@ int kami_spgemm_bsr_symbolic_device(int bsr, int mb, int kb, int nb, const int *
             return st0;
         if (!row_ptr_c)
             return fail(KAMI_ERR_INVALID_VALUE, "spgemm: row_ptr_c is NULL");
+        // one pass with a decoupled look-back; past the flag array's capacity
+        // the three-phase form with grid barriers
+        const int stl = symbolic_lookback(mb, nb, row_ptr_a, col_idx_a, row_ptr_b, col_idx_b, row_ptr_c, col_idx_c,
+                                          capacity, reinterpret_cast<cudaStream_t>(stream));
+        if (stl != KAMI_ERR_UNSUPPORTED)
+            return stl;
         const int st1 = symbolic_fused(mb, nb, row_ptr_a, col_idx_a, row_ptr_b, col_idx_b, row_ptr_c, col_idx_c,
                                        capacity, reinterpret_cast<cudaStream_t>(stream));
         if (st1 != KAMI_ERR_UNSUPPORTED)
