@@ -143,12 +143,13 @@ def test_symbolic_device_matches_host_and_numeric_bound(cuda, mb, kb, nb, densit
 
 
 @pytest.mark.parametrize("mb,kb,nb,density", [(20000, 64, 3000, 0.01), (1, 5, 7, 1.0), (3000, 3000, 40, 0.002),
-                                              (50000, 16, 100, 0.05)])
+                                              (50000, 16, 100, 0.05), (140000, 16, 40, 0.02)])
 def test_symbolic_device_one_launch_large(cuda, mb, kb, nb, density):
-    """The one-launch symbolic pass (count, scan, column fill as phases of a
-    cooperative kernel) with many block-rows per CTA, a single row, and rows
-    without entries, against the oracle's structure and the separate
-    count / fill kernels."""
+    """The one-launch symbolic pass (count, look-back scan and column fill in
+    one cooperative kernel) with many chunks per CTA, a single row, rows
+    without entries and -- at 140000 block-rows, past one row per warp in
+    16384 chunks -- two rows per warp and chunk, against the oracle's
+    structure and the separate count / fill kernels."""
     A = random_bsr(mb, kb, density, 21, integer=True)
     B = random_bsr(kb, nb, min(1.0, density * 10), 22, integer=True)
     dA, dB = to_dev(A, kb), to_dev(B, nb)
