@@ -52,7 +52,7 @@ def _worker(rank, world, port, out):
 def test_two_gloo_ranks_shard_and_reduce():
     world = 2
     port = _free_port()
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()  # no fork of this multi-threaded process
     out = mgr.dict()
     mp.spawn(_worker, args=(world, port, out), nprocs=world, join=True)
     for rank in range(world):
