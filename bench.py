@@ -13,8 +13,8 @@ One JSON line on rank 0.  `value` is device time of the GEMM launches only
 (inputs resident in HBM; the 256 MiB L2 flush between steps is outside the
 timed events); `e2e` is the same metric through the public C-ABI call on
 host buffers (kami_gemm_batched_host: the inputs copied from pinned host
-memory and C copied back inside the timed region, the copies of one chunk of
-the batch overlapping the product of the next).  With --gpus N > 1 every rank runs its own replica (weak scaling);
+memory and C copied back inside the timed region; the batch in chunks whose
+products start as their inputs land, so copies and products overlap).  With --gpus N > 1 every rank runs its own replica (weak scaling);
 the time is the max over ranks.
 """
 from __future__ import annotations
@@ -270,8 +270,8 @@ def run_ours(args, rank, world):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        # the public host-buffer call: copies in, product, copy out, the
-        # copies of one chunk overlapping the product of the next
+        # the public host-buffer call: copies in, products, copies out,
+        # overlapped chunk by chunk
         api.gemm_batched_host(A_pin, B_pin, C_pin, variant=args.variant, partition=args.partition,
                               num_iter=num_iter, stream=stream)
         e1.record(stream)

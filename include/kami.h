@@ -142,9 +142,11 @@ int kami_gemm_batched(kami_dtype_t in_type, kami_dtype_t out_type,
  * packed M x K row-major, B the reference's N x K row-major, C M x N; alpha 1,
  * beta 0): the reference's host sequence -- copy in, launch, copy out
  * (e.g. batched_gemm_2d_double_mma.cu) -- as one call, with the batch cut
- * into chunks of whole SM waves so that the input copies of chunk c + 1 and
- * the result copy of chunk c - 1 overlap the product of chunk c (two extra
- * streams, double-buffered device workspace).  Host buffers should be pinned
+ * into chunks of about one problem per four SMs (16 at most): the input
+ * copies run back to back on one stream, the result copies on another, and
+ * each chunk's product starts on one of the library's compute streams as
+ * soon as its inputs have landed (one device buffer per chunk, a ring of
+ * buffers above 1 GiB in all).  Host buffers should be pinned
  * (pageable memory works, without overlap) and stay valid until the work on
  * `stream` completes; `stream` waits for the last result copy.  workspace:
  * device memory of kami_gemm_batched_host_workspace_size bytes, or NULL for a

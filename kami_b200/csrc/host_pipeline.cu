@@ -3,26 +3,36 @@
 //
 // The reference's programs copy A and B to the device, launch, and copy C
 // back, one after the other (e.g. batched_gemm_2d_double_mma.cu: cudaMemcpy,
-// kernel, cudaMemcpy).  Here the batch is cut into chunks of two SM waves
-// and pipelined over three streams: while chunk c is multiplied on the
-// caller's stream, chunk c + 1's A and B travel host -> device and chunk
-// c - 1's C device -> host, each copy direction on its own stream (and copy
-// engine), through a double-buffered device workspace.  The caller's stream
-// waits for the last copy, so work queued after the call sees C complete.
+// kernel, cudaMemcpy).  Here the batch is cut into chunks of about one
+// problem per four SMs.  The input copies run back to back on one stream, the
+// result copies on another (each direction on its own copy engine), and each
+// chunk's product is launched on one of several compute streams as soon as
+// its inputs have landed, so it takes the SMs the earlier chunks leave free.
+// The repeated-products kernel runs one CTA per SM here: SMs then free up in
+// the order they started, each runs its problems back to back, and the last
+// results arrive spread over time as the first inputs did, so that little
+// but the first chunk's input copy and the last chunk's result copy is left
+// outside the overlap.  (FP16 128^3 x 592, 1000 repeats: copy in 0.71 ms,
+// products 1.30 ms, copy out 0.68 ms; two chunks of two waves 1.99 ms, 4
+// chunks of 148 on two CTAs per SM 1.64-1.67 ms, 16 chunks of 37 at one CTA
+// per SM 1.555 ms.)  Each chunk has its own device buffers (a ring of
+// buffers once the whole batch would need more than 1 GiB).  The caller's
+// stream waits for the last copy, so work queued after the call sees C
+// complete.
 #include <algorithm>
 #include <map>
 #include <mutex>
 
 #include "kami_common.cuh"
 
-extern "C" int kami_gemm_batched(kami_dtype_t in_type, kami_dtype_t out_type, kami_partition_t partition,
-                                 kami_variant_t variant, int M, int N, int K, int P, int alloc_warps, int64_t batch,
-                                 const void *A, int64_t lda, int64_t strideA, kami_a_layout_t a_layout, const void *B,
-                                 int64_t ldb, int64_t strideB, kami_b_layout_t b_layout, void *C, int64_t ldc,
-                                 int64_t strideC, double alpha, double beta, int num_iter, void *workspace,
-                                 size_t ws_bytes, void *stream);
-
 namespace kami {
+
+int gemm_batched_hinted(kami_dtype_t in_type, kami_dtype_t out_type, kami_partition_t partition,
+                        kami_variant_t variant, int M, int N, int K, int P, int alloc_warps, int64_t batch,
+                        const void *A, int64_t lda, int64_t strideA, kami_a_layout_t a_layout, const void *B,
+                        int64_t ldb, int64_t strideB, kami_b_layout_t b_layout, void *C, int64_t ldc,
+                        int64_t strideC, double alpha, double beta, int num_iter, void *workspace, size_t ws_bytes,
+                        void *stream, int one_per_sm);
 
 int fail(int code, const char *fmt, ...);
 int cuda_fail(cudaError_t e, const char *what);
@@ -32,34 +42,45 @@ namespace {
 int esize(int t) { return t == KAMI_F64 ? 8 : t == KAMI_F32 ? 4 : 2; }
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+constexpr int kMaxChunks = 16;               // chunks (and device buffers) per call
+constexpr int kStreams = 8;                  // compute streams the chunks' products spread over
+constexpr size_t kBufCap = (size_t)1 << 30;  // one buffer per chunk up to this many bytes in all
+
 struct Chunking
 {
     int64_t chunk;  // problems per chunk
     int64_t chunks; // number of chunks
+    int bufs;       // device buffers; chunk c uses buffer c % bufs
     size_t a, b, c; // bytes of one chunk's A, B, C buffers (256-byte multiples)
 };
 
 Chunking chunking(int in_type, int out_type, int M, int N, int K, int64_t batch, int sms)
 {
     Chunking ch{};
-    // up to 8 chunks, each at least two problems per SM: with one, the MMA
-    // issue of a single CTA per SM leaves the tensor pipe half idle (FP16
-    // 128^3 x 148 problems, 1000 repeats: 0.71 ms, x 592: 1.44 ms)
-    const int64_t waves = std::max<int64_t>(1, batch / (2 * (int64_t)std::max(sms, 1)));
-    ch.chunks = std::min<int64_t>(8, waves);
+    // about one problem per four SMs per chunk (FP16 128^3 x 592 with 1000
+    // repeats: 16 chunks of 37), the products at most one CTA per SM
+    const int64_t target = std::max(1, sms / 4);
+    ch.chunks = std::min<int64_t>(kMaxChunks, std::max<int64_t>(1, (batch + target - 1) / target));
     ch.chunk = (batch + ch.chunks - 1) / ch.chunks;
+    ch.chunks = (batch + ch.chunk - 1) / ch.chunk;
     ch.a = align256((size_t)ch.chunk * M * K * esize(in_type));
     ch.b = align256((size_t)ch.chunk * N * K * esize(in_type));
     ch.c = align256((size_t)ch.chunk * M * N * esize(out_type));
+    const size_t per = ch.a + ch.b + ch.c;
+    int64_t bufs = ch.chunks;
+    if (bufs > 2 && (size_t)bufs * per > kBufCap)
+        bufs = std::max<int64_t>(2, (int64_t)(kBufCap / per));
+    ch.bufs = (int)bufs;
     return ch;
 }
 
-// per device: the two copy streams, the events that chain the chunks, and a
-// library-owned workspace for callers that pass none
+// per device: the copy and compute streams, the events that chain the
+// chunks, and a library-owned workspace for callers that pass none
 struct DeviceCtx
 {
-    cudaStream_t h2d = nullptr, d2h = nullptr;
-    cudaEvent_t h2d_done[2], comp_done[2], d2h_done[2];
+    cudaStream_t h2d = nullptr, d2h = nullptr, comp[kStreams] = {};
+    cudaEvent_t entry = nullptr, call_done = nullptr;
+    cudaEvent_t h2d_done[kMaxChunks], comp_done[kMaxChunks], d2h_done[kMaxChunks];
     void *ws = nullptr;
     size_t ws_bytes = 0;
     bool ready = false;
@@ -76,7 +97,13 @@ int get_ctx(int dev, DeviceCtx **out)
         if ((e = cudaStreamCreateWithFlags(&c.h2d, cudaStreamNonBlocking)) != cudaSuccess ||
             (e = cudaStreamCreateWithFlags(&c.d2h, cudaStreamNonBlocking)) != cudaSuccess)
             return cuda_fail(e, "cudaStreamCreate(host pipeline)");
-        for (int i = 0; i < 2; ++i)
+        for (int i = 0; i < kStreams; ++i)
+            if ((e = cudaStreamCreateWithFlags(&c.comp[i], cudaStreamNonBlocking)) != cudaSuccess)
+                return cuda_fail(e, "cudaStreamCreate(host pipeline)");
+        if ((e = cudaEventCreateWithFlags(&c.entry, cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&c.call_done, cudaEventDisableTiming)) != cudaSuccess)
+            return cuda_fail(e, "cudaEventCreate(host pipeline)");
+        for (int i = 0; i < kMaxChunks; ++i)
             if ((e = cudaEventCreateWithFlags(&c.h2d_done[i], cudaEventDisableTiming)) != cudaSuccess ||
                 (e = cudaEventCreateWithFlags(&c.comp_done[i], cudaEventDisableTiming)) != cudaSuccess ||
                 (e = cudaEventCreateWithFlags(&c.d2h_done[i], cudaEventDisableTiming)) != cudaSuccess)
@@ -103,7 +130,7 @@ int kami_gemm_batched_host_workspace_size(kami_dtype_t in_type, kami_dtype_t out
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const Chunking ch = chunking(in_type, out_type, M, N, K, std::max<int64_t>(batch, 1), sms);
-    *bytes = 2 * (ch.a + ch.b + ch.c);
+    *bytes = (size_t)ch.bufs * (ch.a + ch.b + ch.c);
     return KAMI_OK;
 }
 
@@ -123,7 +150,7 @@ int kami_gemm_batched_host(kami_dtype_t in_type, kami_dtype_t out_type, kami_par
         return cuda_fail(e, "cudaGetDevice");
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const Chunking ch = chunking(in_type, out_type, M, N, K, batch, sms);
-    const size_t need = 2 * (ch.a + ch.b + ch.c);
+    const size_t need = (size_t)ch.bufs * (ch.a + ch.b + ch.c);
     std::lock_guard<std::mutex> lk(g_mu);
     DeviceCtx *ctx = nullptr;
     int st = get_ctx(dev, &ctx);
@@ -156,23 +183,22 @@ int kami_gemm_batched_host(kami_dtype_t in_type, kami_dtype_t out_type, kami_par
     const int isz = esize(in_type), osz = esize(out_type);
     const uint8_t *Ah = reinterpret_cast<const uint8_t *>(A), *Bh = reinterpret_cast<const uint8_t *>(B);
     uint8_t *Ch = reinterpret_cast<uint8_t *>(C);
-    // the copies start after work already queued on the caller's stream and
-    // after the previous call's result copies (whose products precede them)
-    // have left the shared workspace
-    if ((e = cudaStreamWaitEvent(ctx->h2d, ctx->d2h_done[0], 0)) != cudaSuccess ||
-        (e = cudaStreamWaitEvent(ctx->h2d, ctx->d2h_done[1], 0)) != cudaSuccess ||
-        (e = cudaEventRecord(ctx->comp_done[1], s0)) != cudaSuccess ||
-        (e = cudaStreamWaitEvent(ctx->h2d, ctx->comp_done[1], 0)) != cudaSuccess)
+    // the copies start after the work already queued on the caller's stream
+    // and after the previous call's last result copy (whose products precede
+    // it) has left the shared workspace
+    if ((e = cudaEventRecord(ctx->entry, s0)) != cudaSuccess ||
+        (e = cudaStreamWaitEvent(ctx->h2d, ctx->entry, 0)) != cudaSuccess ||
+        (e = cudaStreamWaitEvent(ctx->h2d, ctx->call_done, 0)) != cudaSuccess)
         return cuda_fail(e, "host gemm: stream ordering");
+    const size_t per = ch.a + ch.b + ch.c;
     for (int64_t c = 0; c < ch.chunks; ++c)
     {
-        const int buf = (int)(c & 1);
+        const int buf = (int)(c % ch.bufs);
         const int64_t p0 = c * ch.chunk, n = std::min(ch.chunk, batch - p0);
-        if (n <= 0)
-            break;
-        uint8_t *dA = ws + (size_t)buf * (ch.a + ch.b + ch.c), *dB = dA + ch.a, *dC = dB + ch.b;
-        // inputs in: the buffer is free once chunk c - 2's product is done
-        if (c >= 2 && (e = cudaStreamWaitEvent(ctx->h2d, ctx->comp_done[buf], 0)) != cudaSuccess)
+        uint8_t *dA = ws + (size_t)buf * per, *dB = dA + ch.a, *dC = dB + ch.b;
+        cudaStream_t cs = ctx->comp[c % kStreams];
+        // inputs in: a reused buffer is free once chunk c - bufs's product is done
+        if (c >= ch.bufs && (e = cudaStreamWaitEvent(ctx->h2d, ctx->comp_done[buf], 0)) != cudaSuccess)
             return cuda_fail(e, "host gemm: stream ordering");
         if ((e = cudaMemcpyAsync(dA, Ah + (size_t)p0 * M * K * isz, (size_t)n * M * K * isz, cudaMemcpyHostToDevice,
                                  ctx->h2d)) != cudaSuccess ||
@@ -180,16 +206,16 @@ int kami_gemm_batched_host(kami_dtype_t in_type, kami_dtype_t out_type, kami_par
                                  ctx->h2d)) != cudaSuccess ||
             (e = cudaEventRecord(ctx->h2d_done[buf], ctx->h2d)) != cudaSuccess)
             return cuda_fail(e, "host gemm: input copy");
-        // the product: after its inputs, and after chunk c - 2's C left the buffer
-        if ((e = cudaStreamWaitEvent(s0, ctx->h2d_done[buf], 0)) != cudaSuccess ||
-            (c >= 2 && (e = cudaStreamWaitEvent(s0, ctx->d2h_done[buf], 0)) != cudaSuccess))
+        // the product: after its inputs, and after chunk c - bufs's C left a reused buffer
+        if ((e = cudaStreamWaitEvent(cs, ctx->h2d_done[buf], 0)) != cudaSuccess ||
+            (c >= ch.bufs && (e = cudaStreamWaitEvent(cs, ctx->d2h_done[buf], 0)) != cudaSuccess))
             return cuda_fail(e, "host gemm: stream ordering");
-        st = kami_gemm_batched(in_type, out_type, partition, variant, M, N, K, 0, 0, n, dA, K, (int64_t)M * K,
-                               KAMI_A_ROW_MK, dB, K, (int64_t)N * K, KAMI_B_REF_NK, dC, N, (int64_t)M * N, 1.0, 0.0,
-                               num_iter, nullptr, 0, stream);
+        st = gemm_batched_hinted(in_type, out_type, partition, variant, M, N, K, 0, 0, n, dA, K, (int64_t)M * K,
+                                 KAMI_A_ROW_MK, dB, K, (int64_t)N * K, KAMI_B_REF_NK, dC, N, (int64_t)M * N, 1.0, 0.0,
+                                 num_iter, nullptr, 0, cs, 1);
         if (st)
             return st;
-        if ((e = cudaEventRecord(ctx->comp_done[buf], s0)) != cudaSuccess)
+        if ((e = cudaEventRecord(ctx->comp_done[buf], cs)) != cudaSuccess)
             return cuda_fail(e, "host gemm: stream ordering");
         // result out
         if ((e = cudaStreamWaitEvent(ctx->d2h, ctx->comp_done[buf], 0)) != cudaSuccess ||
@@ -198,10 +224,11 @@ int kami_gemm_batched_host(kami_dtype_t in_type, kami_dtype_t out_type, kami_par
             (e = cudaEventRecord(ctx->d2h_done[buf], ctx->d2h)) != cudaSuccess)
             return cuda_fail(e, "host gemm: result copy");
     }
-    // the caller's stream continues once every result copy is done
-    for (int buf = 0; buf < 2; ++buf)
-        if ((e = cudaStreamWaitEvent(s0, ctx->d2h_done[buf], 0)) != cudaSuccess)
-            return cuda_fail(e, "host gemm: stream ordering");
+    // the result copies run in order on one stream: the caller's stream
+    // continues once the last one is done
+    if ((e = cudaEventRecord(ctx->call_done, ctx->d2h)) != cudaSuccess ||
+        (e = cudaStreamWaitEvent(s0, ctx->call_done, 0)) != cudaSuccess)
+        return cuda_fail(e, "host gemm: stream ordering");
     return KAMI_OK;
 }
 

@@ -363,12 +363,22 @@ int kami_gemm_describe(kami_dtype_t in_type, kami_dtype_t out_type, kami_partiti
     return KAMI_OK;
 }
 
-int kami_gemm_batched(kami_dtype_t in_type, kami_dtype_t out_type, kami_partition_t partition,
-                      kami_variant_t variant, int M, int N, int K, int P, int alloc_warps, int64_t batch,
-                      const void *A, int64_t lda, int64_t strideA, kami_a_layout_t a_layout, const void *B,
-                      int64_t ldb, int64_t strideB, kami_b_layout_t b_layout, void *C, int64_t ldc,
-                      int64_t strideC, double alpha, double beta, int num_iter, void *workspace, size_t ws_bytes,
-                      void *stream)
+} // extern "C"
+
+namespace kami {
+
+// kami_gemm_batched with launch hints for callers inside the library.
+// one_per_sm: at most one CTA of the repeated-products kernel per SM -- for
+// the host pipeline, whose chunks run as concurrent launches: with one CTA
+// per SM the SMs free up in the order they started, so each SM runs its
+// problems back to back and the last results are spread over time like the
+// first inputs were.
+int gemm_batched_hinted(kami_dtype_t in_type, kami_dtype_t out_type, kami_partition_t partition,
+                        kami_variant_t variant, int M, int N, int K, int P, int alloc_warps, int64_t batch,
+                        const void *A, int64_t lda, int64_t strideA, kami_a_layout_t a_layout, const void *B,
+                        int64_t ldb, int64_t strideB, kami_b_layout_t b_layout, void *C, int64_t ldc,
+                        int64_t strideC, double alpha, double beta, int num_iter, void *workspace, size_t ws_bytes,
+                        void *stream, int one_per_sm)
 {
     int st = check_request(in_type, out_type, M, N, K, batch, a_layout, b_layout, num_iter);
     if (st)
@@ -423,6 +433,7 @@ int kami_gemm_batched(kami_dtype_t in_type, kami_dtype_t out_type, kami_partitio
     g.alpha = alpha;
     g.beta = beta;
     g.num_iter = num_iter;
+    g.one_per_sm = one_per_sm;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
 
     if (variant == KAMI_VARIANT_TCGEN05 || variant == KAMI_VARIANT_TCGEN05_TS ||
@@ -484,4 +495,16 @@ int kami_gemm_batched(kami_dtype_t in_type, kami_dtype_t out_type, kami_partitio
     return KAMI_OK;
 }
 
-} // extern "C"
+} // namespace kami
+
+extern "C" int kami_gemm_batched(kami_dtype_t in_type, kami_dtype_t out_type, kami_partition_t partition,
+                                 kami_variant_t variant, int M, int N, int K, int P, int alloc_warps, int64_t batch,
+                                 const void *A, int64_t lda, int64_t strideA, kami_a_layout_t a_layout, const void *B,
+                                 int64_t ldb, int64_t strideB, kami_b_layout_t b_layout, void *C, int64_t ldc,
+                                 int64_t strideC, double alpha, double beta, int num_iter, void *workspace,
+                                 size_t ws_bytes, void *stream)
+{
+    return kami::gemm_batched_hinted(in_type, out_type, partition, variant, M, N, K, P, alloc_warps, batch, A, lda,
+                                     strideA, a_layout, B, ldb, strideB, b_layout, C, ldc, strideC, alpha, beta,
+                                     num_iter, workspace, ws_bytes, stream, 0);
+}

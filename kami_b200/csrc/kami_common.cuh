@@ -29,6 +29,7 @@ struct GemmArgs {
     int num_iter;
     int problems_per_cta;
     unsigned long long *trace; // traced instances: per-warp {communication, computation} cycles of problem 0
+    int one_per_sm;            // launch hint: at most one CTA of the repeated-products kernel per SM
 };
 
 // Host-side description of a resolved launch (kami_gemm_describe).

@@ -1220,8 +1220,22 @@ int tc05_launch(const GemmArgs &g, int in_type, int partition, int P, void *, si
     });
     if (e != cudaSuccess)
         return cuda_fail(e, "cudaFuncSetAttribute(tc05_block_kernel)");
+    // one CTA per SM on request: more than half of the SM's shared memory
+    int smem = (int)s.smem;
+    if (g.one_per_sm)
+    {
+        static int per_sm = 0;
+        if (!per_sm)
+        {
+            int dev = 0;
+            cudaGetDevice(&dev);
+            if (cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess)
+                per_sm = 228 * 1024;
+        }
+        smem = std::max(smem, std::min(per_sm / 2 + 1024, 227 * 1024));
+    }
     void *args[] = {&ma, &mb, &mc, &p};
-    e = cudaLaunchKernel(fn, dim3((unsigned)g.batch), dim3(128), args, s.smem, stream);
+    e = cudaLaunchKernel(fn, dim3((unsigned)g.batch), dim3(128), args, smem, stream);
     if (e != cudaSuccess)
         return cuda_fail(e, "cudaLaunchKernel(tc05_block_kernel)");
     return KAMI_OK;
