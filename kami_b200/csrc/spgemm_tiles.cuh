@@ -70,7 +70,13 @@ __device__ __forceinline__ void mma16816(float (&d)[4], uint32_t a0, uint32_t a1
 // Store one C tile held as m16n8k16 accumulators with alpha / beta into
 // tile `c` of vc (FP32, FP16 or BF16 tiles, row-major 16 x 16): lane (gq,
 // tq) holds rows gq, gq + 8 and columns 2tq, 2tq + 1 (acc0) and 2tq + 8,
-// 2tq + 9 (acc1).  beta == 0 never reads C.
+// 2tq + 9 (acc1).  beta == 0 never reads C.  FP32 tiles at a 16-byte
+// aligned base are written as float4: lane pairs (tq, tq ^ 1) swap one
+// column pair, so each lane holds four consecutive columns and every store
+// instruction covers eight whole 64-byte rows (512 contiguous bytes) instead
+// of eight 32-byte halves of them (n = 16384, 1 % numeric pass: best of 25
+// 36.8 against 37.7 us, medians equal).  Every caller runs this with the
+// whole warp.
 __device__ __forceinline__ void store_tile_frag(void *vc, int64_t c, int out_type, float alpha, float beta, int gq,
                                                 int tq, const float (&acc0)[4], const float (&acc1)[4])
 {
@@ -78,6 +84,35 @@ __device__ __forceinline__ void store_tile_frag(void *vc, int64_t c, int out_typ
     if (out_type == KAMI_F32)
     {
         float *out = reinterpret_cast<float *>(vc) + c * 256;
+        if ((reinterpret_cast<uintptr_t>(vc) & 15) == 0)
+        {
+            const bool odd = tq & 1;
+            const int col = (tq & 1) * 8 + (tq >> 1) * 4;
+            const float s0 = odd ? acc0[0] : acc1[0], s1 = odd ? acc0[1] : acc1[1];
+            const float s2 = odd ? acc0[2] : acc1[2], s3 = odd ? acc0[3] : acc1[3];
+            const float g0 = __shfl_xor_sync(0xffffffffu, s0, 1), g1 = __shfl_xor_sync(0xffffffffu, s1, 1);
+            const float g2 = __shfl_xor_sync(0xffffffffu, s2, 1), g3 = __shfl_xor_sync(0xffffffffu, s3, 1);
+            float4 w0 = odd ? make_float4(g0, g1, acc1[0], acc1[1]) : make_float4(acc0[0], acc0[1], g0, g1);
+            float4 w1 = odd ? make_float4(g2, g3, acc1[2], acc1[3]) : make_float4(acc0[2], acc0[3], g2, g3);
+            float4 *o0 = reinterpret_cast<float4 *>(out + r0 * 16 + col);
+            float4 *o1 = reinterpret_cast<float4 *>(out + r1 * 16 + col);
+            if (alpha != 1.f || beta != 0.f)
+            {
+                float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f), p1 = p0;
+                if (beta != 0.f)
+                {
+                    p0 = *o0;
+                    p1 = *o1;
+                }
+                w0 = make_float4(alpha * w0.x + beta * p0.x, alpha * w0.y + beta * p0.y, alpha * w0.z + beta * p0.z,
+                                 alpha * w0.w + beta * p0.w);
+                w1 = make_float4(alpha * w1.x + beta * p1.x, alpha * w1.y + beta * p1.y, alpha * w1.z + beta * p1.z,
+                                 alpha * w1.w + beta * p1.w);
+            }
+            *o0 = w0;
+            *o1 = w1;
+            return;
+        }
         float2 v00 = make_float2(acc0[0], acc0[1]), v01 = make_float2(acc1[0], acc1[1]);
         float2 v10 = make_float2(acc0[2], acc0[3]), v11 = make_float2(acc1[2], acc1[3]);
         if (alpha != 1.f || beta != 0.f)
