@@ -39,8 +39,8 @@ namespace kami {
 int fail(int code, const char *fmt, ...);
 int cuda_fail(cudaError_t e, const char *what);
 int spmm_tc05_launch(bool bf16, int out_type, int mb, int kb, int N, const int *rowptr, const int *colidx,
-                     const void *vals, const void *B, int64_t ldb, void *C, int64_t ldc, double alpha, double beta,
-                     int num_iter, cudaStream_t s);
+                     const void *vals, const void *B, int64_t ldb, bool b_nk, void *C, int64_t ldc, double alpha,
+                     double beta, int num_iter, cudaStream_t s);
 
 namespace {
 
@@ -516,11 +516,11 @@ int spmm_launch(kami_dtype_t in_type, kami_dtype_t out_type, int bsr, int mb, in
     if (grid.y > 65535)
         return fail(KAMI_ERR_UNSUPPORTED, "spmm: N above %d", 65535 * kCols);
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    // one large problem with B as K x N: the tcgen05 kernel (spmm_tc05.cu)
-    if (!panel && !p.refnk && batch == 1 && tile_rows == 1 && ntiles == 1)
+    // one large problem: the tcgen05 kernel (spmm_tc05.cu), B as K x N or N x K
+    if (!panel && batch == 1 && tile_rows == 1 && ntiles == 1)
     {
-        const int s5 = spmm_tc05_launch(p.bf16 != 0, out_type, mb, kb, N, rowptr, colidx, vals, B, ldb, C, ldc, alpha,
-                                        beta, num_iter, st);
+        const int s5 = spmm_tc05_launch(p.bf16 != 0, out_type, mb, kb, N, rowptr, colidx, vals, B, ldb, p.refnk != 0,
+                                        C, ldc, alpha, beta, num_iter, st);
         if (s5 != KAMI_ERR_UNSUPPORTED)
             return s5;
     }

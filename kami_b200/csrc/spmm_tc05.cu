@@ -1,13 +1,18 @@
 // spmm_tc05.cu -- block SpMM C = A B (A BSR with 16 x 16 tiles, B dense
-// K x N row-major, C dense M x N) on the 5th-generation tensor cores, for the
-// streamed regime of large sparse matrices (K beyond a staged panel).
+// K x N row-major or N x K row-major (the reference's layout), C dense
+// M x N) on the 5th-generation tensor cores, for the streamed regime of large
+// sparse matrices (K beyond a staged panel).
 //
 // A block-row of C is only 16 rows high, below the smallest tcgen05 MMA
 // (M = 64).  So each block-row is computed transposed:
 //   C_i^T (N x 16) = sum over the row's tiles (i, k) of  B_k^T (N x 16) A_ik^T,
 // where B_k is rows 16k .. 16k + 15 of B.  B_k^T is the MMA's A operand with
 // M = 128 columns of B per MMA, read MN-major straight from B's row-major
-// rows (TMA boxes of 64 columns x 16 rows, 128-byte swizzle); the tile A_ik
+// rows (TMA boxes of 64 columns x 16 rows, 128-byte swizzle) -- or, for B
+// as N x K, K-major: the slice's 16 K values of a column are 32 contiguous
+// bytes, loaded by TMA boxes of 16 x 128 rows with 32-byte swizzling (one
+// 32-byte request per column -- boxes of 8 values, two 16-byte requests per
+// column, measured 38.9 us, no faster than the mma.sync form); the tile A_ik
 // is the MMA's B operand with N = 16 (its rows) and K = 16 (its columns),
 // K-major without swizzle: the loaders write its 16-byte row halves into the
 // 8-row x 16-byte core matrices the descriptor describes.  The accumulator of
@@ -69,7 +74,7 @@ struct SpTcParams
 {
     int mb, kb, N;
     int npad;          // N rounded up to 128
-    int slot_bytes;    // B slice (npad x 16 x 2 bytes, MN-major boxes) + 512-byte tile, 1024-byte multiple
+    int slot_bytes;    // B slice (npad x 16 x 2 bytes) + 512-byte tile, 1024-byte multiple
     int slots;
     int acc_cols;      // TMEM columns of one accumulator: 16 per 128 columns of C
     uint32_t tmem_cols;
@@ -114,7 +119,9 @@ __device__ __forceinline__ float to_f(uint16_t b, bool bf)
     return bf ? __bfloat162float(__ushort_as_bfloat16(b)) : __half2float(__ushort_as_half(b));
 }
 
-template <bool BF16>
+// KMAJ: B is N x K and its slices are K-major (32-byte rows, 4 KB per 128
+// columns); else B is K x N and its slices MN-major (boxes of 64 columns).
+template <bool BF16, bool KMAJ>
 __global__ void __launch_bounds__(kThreads, kCtasPerSm) spmm_tc05_kernel(const __grid_constant__ CUtensorMap tmB,
                                                                 const SpTcParams p)
 {
@@ -205,8 +212,14 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) spmm_tc05_kernel(const _
                 {
                     const int krow = (k >= 0 && k < p.kb) ? k * 16 : p.kb * 16; // past the end: zeros
                     tc::mbar_expect_tx(&full[s], (uint32_t)(nbox * 2048));
-                    for (int b = 0; b < nbox; ++b)
-                        tc::tma_load_3d(smem + (size_t)s * p.slot_bytes + b * 2048, &tmB, &full[s], b * 64, krow, 0);
+                    if (KMAJ) // K values krow .. krow + 15 of 128 columns per box
+                        for (int c = 0; c < nbox / 2; ++c)
+                            tc::tma_load_3d(smem + (size_t)s * p.slot_bytes + c * 4096, &tmB, &full[s], krow, c * 128,
+                                            0);
+                    else
+                        for (int b = 0; b < nbox; ++b)
+                            tc::tma_load_3d(smem + (size_t)s * p.slot_bytes + b * 2048, &tmB, &full[s], b * 64, krow,
+                                            0);
                 }
                 cp16(slot + tile_off + tdst, p.vals + (int64_t)e * 256 + r * 16 + h * 8);
                 cp_arrive_on(&full[s]);
@@ -261,8 +274,12 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) spmm_tc05_kernel(const _
                     const uint64_t bd = desc_kmajor_noswz(slot + p.npad * 32, 128, 256);
                     for (int it = 0; it < p.num_iter; ++it)
                         for (int c = 0; c < nch; ++c)
-                            tc::mma_f16_ss(acc + (uint32_t)(c * 16), tc::desc_mnmajor_sw128(slot + c * 4096, 2048), bd,
-                                           p.idesc, (t > 0 || it > 0) ? 1u : 0u);
+                        {
+                            // columns 128c .. of the slice, 4 KB in both layouts
+                            const uint64_t ad = KMAJ ? tc::desc_kmajor_sw32(slot + c * 4096)
+                                                     : tc::desc_mnmajor_sw128(slot + c * 4096, 2048);
+                            tc::mma_f16_ss(acc + (uint32_t)(c * 16), ad, bd, p.idesc, (t > 0 || it > 0) ? 1u : 0u);
+                        }
                     tc::mma_commit(&empty[s]);
                 }
                 if (!ok)
@@ -368,12 +385,12 @@ EncodeTiledFn encode_fn()
 
 } // namespace
 
-// The tcgen05 SpMM for one problem with B K x N row-major (16-byte aligned,
-// ldb a multiple of 8), tiles 16-byte aligned, N <= 512; else
-// KAMI_ERR_UNSUPPORTED without launching anything.
+// The tcgen05 SpMM for one problem with B K x N row-major, or N x K
+// row-major when b_nk (16-byte aligned, ldb a multiple of 8), tiles 16-byte
+// aligned, N <= 512; else KAMI_ERR_UNSUPPORTED without launching anything.
 int spmm_tc05_launch(bool bf16, int out_type, int mb, int kb, int N, const int *rowptr, const int *colidx,
-                     const void *vals, const void *B, int64_t ldb, void *C, int64_t ldc, double alpha, double beta,
-                     int num_iter, cudaStream_t s)
+                     const void *vals, const void *B, int64_t ldb, bool b_nk, void *C, int64_t ldc, double alpha,
+                     double beta, int num_iter, cudaStream_t s)
 {
     if (N < 1 || N > 512 || mb < 1 || kb < 1 || (reinterpret_cast<uintptr_t>(B) & 15) || (ldb & 7) ||
         (reinterpret_cast<uintptr_t>(vals) & 15) || (int64_t)kb * 16 > 0x7fffffff)
@@ -383,13 +400,17 @@ int spmm_tc05_launch(bool bf16, int out_type, int mb, int kb, int N, const int *
         return KAMI_ERR_UNSUPPORTED;
     CUtensorMap map;
     const int64_t K = (int64_t)kb * 16;
-    cuuint64_t dims[3] = {(cuuint64_t)N, (cuuint64_t)K, 1};
-    cuuint64_t strides[2] = {(cuuint64_t)(ldb * 2), (cuuint64_t)(ldb * 2 * K)};
-    cuuint32_t box[3] = {64, 16, 1};
+    // K x N: boxes of 64 columns x 16 rows, 128-byte swizzle; N x K: boxes of
+    // 16 K values (32 bytes) x 128 rows, 32-byte swizzle
+    const int64_t rows = b_nk ? N : K;
+    cuuint64_t dims[3] = {(cuuint64_t)(b_nk ? K : N), (cuuint64_t)rows, 1};
+    cuuint64_t strides[2] = {(cuuint64_t)(ldb * 2), (cuuint64_t)(ldb * 2 * rows)};
+    cuuint32_t box[3] = {b_nk ? 16u : 64u, b_nk ? 128u : 16u, 1};
     cuuint32_t estr[3] = {1, 1, 1};
     if (fn(&map, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3, const_cast<void *>(B),
-           dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+           dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+           b_nk ? CU_TENSOR_MAP_SWIZZLE_32B : CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return KAMI_ERR_UNSUPPORTED;
     SpTcParams p{};
     p.mb = mb;
@@ -415,13 +436,17 @@ int spmm_tc05_launch(bool bf16, int out_type, int mb, int kb, int N, const int *
     p.alpha = (float)alpha;
     p.beta = (float)beta;
     p.num_iter = num_iter;
-    p.idesc = tc::idesc_f16(bf16, 128, 16, 1, 0); // A (B's slice) MN-major, B (the tile) K-major
+    // A (B's slice) MN-major for K x N, K-major for N x K; B (the tile) K-major
+    p.idesc = tc::idesc_f16(bf16, 128, 16, b_nk ? 0 : 1, 0);
     p.timeout_ns = (uint64_t)(2e9 + (double)num_iter * 1e6);
     const size_t smem = (size_t)p.slots * p.slot_bytes + (2 * p.slots + 2 * kAccs + 1) * 8 + 16 + 1024;
-    const void *kfn = bf16 ? (const void *)&spmm_tc05_kernel<true> : (const void *)&spmm_tc05_kernel<false>;
-    static std::once_flag once[2];
+    const void *kfn = b_nk ? (bf16 ? (const void *)&spmm_tc05_kernel<true, true>
+                                   : (const void *)&spmm_tc05_kernel<false, true>)
+                           : (bf16 ? (const void *)&spmm_tc05_kernel<true, false>
+                                   : (const void *)&spmm_tc05_kernel<false, false>);
+    static std::once_flag once[4];
     cudaError_t e = cudaSuccess;
-    std::call_once(once[bf16 ? 1 : 0],
+    std::call_once(once[(bf16 ? 1 : 0) + (b_nk ? 2 : 0)],
                    [&] { e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024); });
     if (e != cudaSuccess)
         return cuda_fail(e, "cudaFuncSetAttribute(spmm_tc05_kernel)");

@@ -171,10 +171,10 @@ def _int_bsr(mb, kb, density, seed):
 @pytest.mark.parametrize("dtype", [torch.float16, torch.bfloat16])
 @pytest.mark.parametrize("b_layout", ["row_kn", "ref_nk"])
 def test_tcgen05_form_exact(cuda, N, dtype, b_layout):
-    """One problem with K beyond the staged panel: the tcgen05 kernel for B
-    K x N (C^T = B^T A^T per block-row) with N up to 512, the mma.sync
-    streamed form for N = 600 and for the reference's N x K; rows without
-    entries included."""
+    """One problem with K beyond the staged panel: the tcgen05 kernel
+    (C^T = B^T A^T per block-row) with N up to 512, for B K x N (its slices
+    MN-major) and the reference's N x K (K-major); the mma.sync streamed form
+    for N = 600; rows without entries included."""
     mb, kb = 40, 24
     rp, ci, vals = _int_bsr(mb, kb, 0.15, N)
     Bk = np.random.default_rng(N + 1).integers(-2, 3, (kb * 16, N)).astype(np.float64)
