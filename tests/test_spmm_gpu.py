@@ -185,6 +185,31 @@ def test_tcgen05_form_exact(cuda, N, dtype, b_layout):
     assert np.array_equal(C.double().cpu().numpy(), oracle.spmm(rp, ci, vals, kb, B, b_layout))
 
 
+def test_tcgen05_both_layouts_full_size(cuda):
+    """n = 16384 with 1 % of its 16 x 16 tiles, 256 dense columns (the
+    bench's large SpMM): B as K x N and the same B transposed as N x K run
+    the same MMAs in the same order (only the slice's shared-memory layout
+    differs), so the two results are identical; the first 64 block-rows
+    against the oracle within the FP32-accumulation bound."""
+    nb, N = 1024, 256
+    rp, ci = oracle.bsr_pattern(nb, nb, 0.01, 1)
+    rng = np.random.default_rng(11)
+    vals = rng.uniform(-1, 1, (ci.size, 16, 16)).astype(np.float16)
+    Bk = rng.uniform(-1, 1, (nb * 16, N)).astype(np.float16)
+    A = api.BSR(torch.tensor(rp, device="cuda"), torch.tensor(ci, device="cuda"),
+                torch.tensor(vals, device="cuda"), nb)
+    C_kn = api.spmm(A, torch.tensor(Bk, device="cuda"), b_layout="row_kn")
+    C_nk = api.spmm(A, torch.tensor(np.ascontiguousarray(Bk.T), device="cuda"), b_layout="ref_nk")
+    assert torch.equal(C_kn, C_nk)
+    ref = oracle.spmm(rp[:65], ci[: rp[64]], vals[: rp[64]].astype(np.float64), nb, Bk.astype(np.float64), "row_kn")
+    absref = oracle.spmm(rp[:65], ci[: rp[64]], np.abs(vals[: rp[64]].astype(np.float64)), nb,
+                         np.abs(Bk.astype(np.float64)), "row_kn")
+    got = C_kn[: 64 * 16].double().cpu().numpy()
+    # FP32 accumulation over at most 16 * (tiles in a row) products per element
+    kmax = 16 * int(np.diff(rp[:65]).max())
+    assert np.all(np.abs(got - ref) <= (kmax + 2) * 2.0 ** -24 * absref + 1e-30)
+
+
 @pytest.mark.parametrize("out_dtype", [torch.float32, torch.float16, torch.bfloat16])
 def test_tcgen05_form_alpha_beta_repeats(cuda, out_dtype):
     mb, kb, N = 30, 20, 200
