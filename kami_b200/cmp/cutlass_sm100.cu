@@ -1,8 +1,9 @@
 // cutlass_sm100.cu -- comparator only (not part of libkami_b200.so): the
 // batched GEMM of the CUTLASS library built for sm_100a from its 5th-
 // generation tensor-core collectives (TMA loads, tcgen05.mma, TMEM
-// accumulators; warp-specialised persistent kernel, cluster 1 x 1 x 1, so no
-// TMA multicast), on the same buffers and layouts as kami_gemm_batched:
+// accumulators; warp-specialised persistent kernel, cluster 1 x 1 x 1, so
+// every CTA loads its own tiles), on the same buffers and layouts as
+// kami_gemm_batched:
 // A batch x M x K row-major, B the reference's batch x N x K row-major
 // operand (K x N column-major for CUTLASS), C batch x M x N row-major.
 // The benchmark times it beside this library's kernels.
