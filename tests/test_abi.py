@@ -183,6 +183,26 @@ def test_host_buffer_gemm_validation(kw, status):
     assert st == status
 
 
+@pytest.mark.parametrize("batch,expect", [
+    # 16 chunks of 37 problems, one buffer each: the whole batch's A, B, C
+    (592, 592 * (128 * 128 * 2 * 2 + 128 * 128 * 4)),
+    # one chunk
+    (1, 128 * 128 * 2 * 2 + 128 * 128 * 4),
+    # 16 chunks of 6250 problems would need 13 GB: a ring of two buffers
+    (100000, 2 * 6250 * (128 * 128 * 2 * 2 + 128 * 128 * 4)),
+])
+def test_host_buffer_gemm_workspace_size(batch, expect):
+    """The host-buffer GEMM's chunking, through the size it reports (no GPU
+    needed; 148 SMs assumed when none answers, as on a B200): chunks of about
+    one problem per four SMs, at most 16, each with its own device buffer
+    unless all of them would exceed 1 GiB."""
+    need = ctypes.c_size_t(0)
+    L = _lib.load()
+    assert L.kami_gemm_batched_host_workspace_size(_lib.F16, _lib.F32, 128, 128, 128, batch, ctypes.byref(need)) == 0
+    assert need.value == expect
+    assert L.kami_gemm_batched_host_workspace_size(_lib.F16, _lib.F32, 0, 128, 128, batch, ctypes.byref(need)) != 0
+
+
 class _FakeCuda:
     """Stands for a CUDA tensor on a given device (no GPU needed)."""
 
